@@ -1,0 +1,128 @@
+/*
+ * simd2.h -- C ABI of libsimd2, a B200 (sm_100a) semiring-GEMM engine.
+ *
+ * Drop-in for the srgemm operator surface of escalab/SIMD2.  Every entry
+ * point returns a simd2_status (0 = success).  All calls are asynchronous on
+ * `stream` unless stated otherwise; callers own every buffer they pass.
+ *
+ * Semantics (row-major, matching mmo::host_srgemm, kernel/host_srgemm.h:17-49):
+ *   D[i,j] = id (+) A[i,0](x)B[0,j] (+) ... (+) A[i,K-1](x)B[K-1,j]   then,
+ *   if do_epilogue, D[i,j] = D[i,j] (+) C[i,j]
+ * where id is the add-identity of the semiring (+inf for min, -inf for max,
+ * 0 for plus and or).  This is host_srgemm with D pre-filled with id, and it
+ * is the cuASR device contract D = (A(x)B) (+) C of kernel/srgemm.cuh:66-81.
+ * D may alias C (in-place accumulation); D must not overlap A or B.
+ *
+ * Exactness: the six min/max semirings and or_and are bit-exact against
+ * host_srgemm.  Preconditions for that: operands hold no NaN and no -0.0.
+ * plus_mul and minus_square are dense contractions computed on the tensor
+ * cores (BF16 hi/lo split, FP32 accumulate); their error bound is stated in
+ * the library documentation and checked against an FP64 oracle.
+ */
+#ifndef SIMD2_H
+#define SIMD2_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The nine (add, mul) pairs, numbered as escalab/SIMD2's `enum op`
+ * (kernel/tensor_srgemm.cuh:18-26) so the two enums convert one-to-one. */
+typedef enum simd2_op {
+  SIMD2_MIN_PLUS = 0,
+  SIMD2_PLUS_MUL = 1,
+  SIMD2_MAX_PLUS = 2,
+  SIMD2_MAX_MIN = 3,
+  SIMD2_MAX_MUL = 4,
+  SIMD2_MIN_MUL = 5,
+  SIMD2_MIN_MAX = 6,
+  SIMD2_OR_AND = 7,
+  SIMD2_MINUS_SQUARE = 8
+} simd2_op;
+
+typedef enum simd2_status {
+  SIMD2_OK = 0,
+  SIMD2_ERR_INVALID_ARG = 1,   /* bad size, stride, op or pointer */
+  SIMD2_ERR_UNSUPPORTED = 2,   /* op/type combination without a kernel */
+  SIMD2_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+  SIMD2_ERR_ALLOC = 4,         /* workspace allocation failed */
+  SIMD2_ERR_TIMEOUT = 5,       /* a bounded device-side wait ran out */
+  SIMD2_ERR_NOT_CONVERGED = 6, /* closure hit max_iter while still changing */
+  SIMD2_ERR_NO_DEVICE = 7      /* no sm_100 device visible */
+} simd2_status;
+
+/* Convergence test used by the closure entry points. */
+typedef enum simd2_conv {
+  SIMD2_CONV_EXACT = 0,   /* stop when the new matrix is bitwise unchanged */
+  SIMD2_CONV_TOL = 1,     /* reference float test: |old-new| > 1e-4 is a change
+                             (kernel/converge.cuh:6-14; inf-inf counts as unchanged) */
+  SIMD2_CONV_APLP = 2     /* APLP test: new values in (-1,1) become -FLT_MAX,
+                             then any difference is a change (converge.cuh:32-43) */
+} simd2_conv;
+
+const char* simd2_status_string(int status);
+
+/* Library version and build target, e.g. "simd2-b200 0.1 sm_100a". */
+const char* simd2_version(void);
+
+/* Float srgemm for every semiring except or_and.
+ * Replaces cuasr_<op>_srsgemm (kernel/srgemm.cuh:28-626, column-major; see
+ * simd2_cuasr.h for the exact-signature shims) and, for FP32 inputs, the
+ * FP16 emulation entry tensor_srgemm (kernel/tensor_srgemm.cuh:197-218).
+ * Row-major; lda >= K, ldb >= N, ldc >= N, ldd >= N (elements).
+ * Any M, N, K >= 0.  Uses a per-(device, stream) workspace that the library
+ * allocates on first use and grows as needed (see simd2_reserve_workspace). */
+int simd2_srgemm(simd2_op op, int M, int N, int K,
+                 const float* A, int lda, const float* B, int ldb,
+                 const float* C, int ldc, float* D, int ldd,
+                 int do_epilogue, cudaStream_t stream);
+
+/* or_and on int32 0/1 (any nonzero is true), the cuASR or_and surface
+ * (kernel/srgemm.cuh:442-494).  D is written as 0/1. */
+int simd2_srgemm_orand_i32(int M, int N, int K,
+                           const int32_t* A, int lda, const int32_t* B, int ldb,
+                           const int32_t* C, int ldc, int32_t* D, int ldd,
+                           int do_epilogue, cudaStream_t stream);
+
+/* or_and on uint8 0/1 (any nonzero is true); D is written as 0/1. */
+int simd2_srgemm_orand_u8(int M, int N, int K,
+                          const uint8_t* A, int lda, const uint8_t* B, int ldb,
+                          const uint8_t* C, int ldc, uint8_t* D, int ldd,
+                          int do_epilogue, cudaStream_t stream);
+
+/* Repeated-squaring closure X <- X (+) X(x)X on an n x n matrix, in place,
+ * until the convergence test reports no change or max_iter steps ran.
+ * Replaces the closure loops of apps/{apsp,aplp,mcp,maxrp,minrp,mst}
+ * (e.g. apps/apsp/cuASR/apsp_cuASR.cu:37-54) together with comp_update /
+ * comp_update2 (kernel/converge.cuh:16-84).  *iters_out receives the number
+ * of srgemm steps, counting the final unchanged one as the reference does.
+ * Synchronous: returns after the result is in X.  Returns
+ * SIMD2_ERR_NOT_CONVERGED if max_iter steps ran and the last still changed. */
+int simd2_closure(simd2_op op, int n, float* X, int ldx, int max_iter,
+                  simd2_conv conv, int* iters_out, cudaStream_t stream);
+
+/* or_and transitive closure on uint8 0/1 (apps/gtc/cuASR), synchronous. */
+int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter,
+                           int* iters_out, cudaStream_t stream);
+
+/* Reserve the per-(device, stream) workspace for srgemm calls up to
+ * M x N x K so that later calls (e.g. inside stream capture) allocate
+ * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */
+int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t stream,
+                            size_t* bytes_out);
+
+/* Free every workspace the library holds on the current device. */
+int simd2_release_workspaces(void);
+
+/* Read and clear the device-side error word that kernels set when a bounded
+ * wait runs out (SIMD2_ERR_TIMEOUT).  Synchronizes the current device. */
+int simd2_device_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIMD2_H */

@@ -1,0 +1,163 @@
+"""simd2_b200 -- B200-native semiring GEMM (srgemm) engine.
+
+Host-side Python mirror of the escalab/SIMD2 srgemm operator surface.  Every
+call goes through the C ABI of ``libsimd2.so`` (``include/simd2.h``), which
+launches hand-written sm_100a kernels; there is no CPU or PyTorch fallback.
+If the library is missing or the device is not sm_100, calls raise.
+
+Tensors are torch CUDA tensors (plumbing only: device memory and streams).
+Row-major semantics follow ``mmo::host_srgemm`` (kernel/host_srgemm.h:17-49):
+``D = id (+) A(x)B`` and, with ``do_epilogue``, ``D = D (+) C``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+from .build import LIB as _LIB_PATH
+
+OPS = ("min_plus", "plus_mul", "max_plus", "max_min", "max_mul", "min_mul", "min_max", "or_and",
+       "minus_square")
+OP_ID = {name: i for i, name in enumerate(OPS)}
+CONV = {"exact": 0, "tol": 1, "aplp": 2}
+
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "unsupported operation", 3: "CUDA runtime error",
+    4: "workspace allocation failed", 5: "device-side wait timed out",
+    6: "closure did not converge within max_iter", 7: "no sm_100 device",
+}
+
+
+class Simd2Error(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: simd2 status {status} ({STATUS.get(status, 'unknown')})")
+
+
+class NotConverged(Simd2Error):
+    pass
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libsimd2.so (raises if it was never built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError(f"libsimd2.so not built at {_LIB_PATH}; run `python -m simd2_b200.build`")
+        L = ctypes.CDLL(_LIB_PATH)
+        P, I = ctypes.c_void_p, ctypes.c_int
+        L.simd2_srgemm.argtypes = [I, I, I, I, P, I, P, I, P, I, P, I, I, P]
+        L.simd2_srgemm_orand_i32.argtypes = [I, I, I, P, I, P, I, P, I, P, I, I, P]
+        L.simd2_srgemm_orand_u8.argtypes = [I, I, I, P, I, P, I, P, I, P, I, I, P]
+        L.simd2_closure.argtypes = [I, I, P, I, I, I, ctypes.POINTER(I), P]
+        L.simd2_closure_orand_u8.argtypes = [I, P, I, I, ctypes.POINTER(I), P]
+        L.simd2_reserve_workspace.argtypes = [I, I, I, I, P, ctypes.POINTER(ctypes.c_size_t)]
+        L.simd2_release_workspaces.argtypes = []
+        L.simd2_device_status.argtypes = []
+        L.simd2_status_string.argtypes = [I]
+        L.simd2_status_string.restype = ctypes.c_char_p
+        L.simd2_version.restype = ctypes.c_char_p
+        for name in ("simd2_srgemm", "simd2_srgemm_orand_i32", "simd2_srgemm_orand_u8", "simd2_closure",
+                     "simd2_closure_orand_u8", "simd2_reserve_workspace", "simd2_release_workspaces",
+                     "simd2_device_status"):
+            getattr(L, name).restype = I
+        _lib = L
+    return _lib
+
+
+def _stream(stream) -> ctypes.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def _check(rc: int, what: str):
+    if rc == 6:
+        raise NotConverged(rc, what)
+    if rc != 0:
+        raise Simd2Error(rc, what)
+
+
+def _mat(t: torch.Tensor, name: str) -> int:
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if t.dim() != 2:
+        raise ValueError(f"{name} must be 2-D")
+    if t.numel() == 0:
+        return max(t.size(1), 1)
+    if t.stride(1) != 1 and t.size(1) > 1:
+        raise ValueError(f"{name} must be a 2-D row-major tensor with unit column stride")
+    return t.stride(0) if t.size(0) > 1 else max(t.size(1), 1)
+
+
+def srgemm(op: str, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, do_epilogue: bool = False,
+           D: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """D = id (+) A(x)B [(+) C] on the GPU; returns D (allocated if not given).
+
+    float32 tensors for the eight float semirings; int32 or uint8 for or_and.
+    """
+    M, K = A.shape
+    K2, N = B.shape
+    if K != K2:
+        raise ValueError("inner dimensions differ")
+    if D is None:
+        D = torch.empty((M, N), dtype=A.dtype, device=A.device)
+    lda, ldb, ldd = _mat(A, "A"), _mat(B, "B"), _mat(D, "D")
+    if do_epilogue:
+        if C is None:
+            raise ValueError("do_epilogue needs C")
+        ldc = _mat(C, "C")
+        cptr = C.data_ptr()
+    else:
+        ldc, cptr = N, None
+    s = _stream(stream)
+    if op == "or_and":
+        fn = {torch.int32: lib().simd2_srgemm_orand_i32, torch.uint8: lib().simd2_srgemm_orand_u8}.get(A.dtype)
+        if fn is None:
+            raise TypeError("or_and takes int32 or uint8 tensors")
+        rc = fn(M, N, K, A.data_ptr(), lda, B.data_ptr(), ldb, cptr, ldc, D.data_ptr(), ldd, int(do_epilogue), s)
+    else:
+        for t, nm in ((A, "A"), (B, "B"), (D, "D")):
+            if t.dtype != torch.float32:
+                raise TypeError(f"{nm} must be float32 for {op}")
+        rc = lib().simd2_srgemm(OP_ID[op], M, N, K, A.data_ptr(), lda, B.data_ptr(), ldb, cptr, ldc, D.data_ptr(),
+                                ldd, int(do_epilogue), s)
+    _check(rc, f"srgemm({op})")
+    return D
+
+
+def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", stream=None,
+            raise_not_converged: bool = True) -> int:
+    """Repeated squaring X <- X (+) X(x)X in place until unchanged; returns the step count."""
+    n = X.shape[0]
+    if X.shape != (n, n):
+        raise ValueError("closure needs a square matrix")
+    ldx = _mat(X, "X")
+    it = ctypes.c_int(0)
+    s = _stream(stream)
+    if op == "or_and":
+        if X.dtype != torch.uint8:
+            raise TypeError("or_and closure takes a uint8 tensor")
+        rc = lib().simd2_closure_orand_u8(n, X.data_ptr(), ldx, max_iter, ctypes.byref(it), s)
+    else:
+        if X.dtype != torch.float32:
+            raise TypeError("closure takes a float32 tensor")
+        rc = lib().simd2_closure(OP_ID[op], n, X.data_ptr(), ldx, max_iter, CONV[conv], ctypes.byref(it), s)
+    if rc == 6 and not raise_not_converged:
+        return it.value
+    _check(rc, f"closure({op})")
+    return it.value
+
+
+def device_status() -> int:
+    """Read and clear the device-side error word (0 = no kernel reported an error)."""
+    return lib().simd2_device_status()
+
+
+def version() -> str:
+    return lib().simd2_version().decode()

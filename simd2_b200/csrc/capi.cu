@@ -1,0 +1,467 @@
+// capi.cu -- C ABI entry points of libsimd2 (see include/simd2.h).
+//
+// Host side of the engine: argument checks, per-(device, stream) workspace,
+// TMA descriptor encoding, kernel dispatch and the closure driver loop.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "common.cuh"
+#include "prep.cuh"
+#include "srgemm_simt.cuh"
+
+namespace simd2 {
+namespace {
+
+#define SIMD2_CUDA_TRY(expr)                       \
+  do {                                             \
+    cudaError_t err__ = (expr);                    \
+    if (err__ != cudaSuccess) return SIMD2_ERR_CUDA; \
+  } while (0)
+
+constexpr size_t kAlign = 1024;
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+inline int round_up(int x, int a) { return (x + a - 1) / a * a; }
+
+// ---------------------------------------------------------------------------
+// device capability check (once per device)
+// ---------------------------------------------------------------------------
+int check_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return SIMD2_ERR_NO_DEVICE;
+  static std::mutex mu;
+  static std::map<int, int> verdict;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = verdict.find(dev);
+  if (it != verdict.end()) return it->second;
+  int major = 0, minor = 0;
+  int rc = SIMD2_OK;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess || major != 10 ||
+      minor != 0)
+    rc = SIMD2_ERR_NO_DEVICE;
+  verdict[dev] = rc;
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// workspace: one growable device buffer per (device, stream)
+// ---------------------------------------------------------------------------
+std::mutex g_ws_mu;
+std::map<std::pair<int, cudaStream_t>, std::pair<void*, size_t>> g_ws;
+
+int get_workspace(cudaStream_t stream, size_t bytes, void** out) {
+  int dev = 0;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  auto& e = g_ws[{dev, stream}];
+  if (e.second < bytes) {
+    if (e.first) {
+      cudaStreamSynchronize(stream);
+      cudaFree(e.first);
+      e = {nullptr, 0};
+    }
+    const size_t nb = align_up(std::max(bytes, (size_t)1 << 20), (size_t)2 << 20);
+    void* p = nullptr;
+    if (cudaMalloc(&p, nb) != cudaSuccess) {
+      cudaGetLastError();
+      return SIMD2_ERR_ALLOC;
+    }
+    e = {p, nb};
+  }
+  *out = e.first;
+  return SIMD2_OK;
+}
+
+// ---------------------------------------------------------------------------
+// TMA descriptors
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Row-major float matrix [rows][cols] with row pitch `pitch` elements.
+int make_map_f32(CUtensorMap* map, const void* base, long long rows, long long cols, long long pitch, int box_cols,
+                 int box_rows, CUtensorMapSwizzle swz, bool nan_fill) {
+  auto fn = encode_fn();
+  if (!fn) return SIMD2_ERR_CUDA;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  nan_fill ? CU_TENSOR_MAP_FLOAT_OOB_FILL_NAN_REQUEST_ZERO_FMA : CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SIMD2_OK : SIMD2_ERR_CUDA;
+}
+
+inline int grid_for(long long items, int threads = 256) {
+  long long b = (items + threads - 1) / threads;
+  return (int)std::max(1LL, std::min(b, 148LL * 16));
+}
+
+bool is_float_op(int op) { return op >= 0 && op <= 8 && op != SIMD2_OR_AND; }
+bool is_sum_op(int op) { return op == SIMD2_PLUS_MUL || op == SIMD2_MINUS_SQUARE; }
+
+float add_identity(int op) {
+  switch (op) {
+    case SIMD2_MIN_PLUS: case SIMD2_MIN_MUL: case SIMD2_MIN_MAX: return __builtin_inff();
+    case SIMD2_MAX_PLUS: case SIMD2_MAX_MIN: case SIMD2_MAX_MUL: return -__builtin_inff();
+    default: return 0.0f;
+  }
+}
+
+// Padding value for out-of-range k: NaN products vanish under min/max.
+float pad_value(int op) { return is_sum_op(op) ? 0.0f : __builtin_nanf(""); }
+
+// ---------------------------------------------------------------------------
+// srgemm plan: workspace layout for one call
+// ---------------------------------------------------------------------------
+struct Plan {
+  int Kp, Np;
+  size_t bp_off, bp_bytes;  // interleaved B'
+  size_t ap_off, ap_bytes;  // packed A (0 when TMA reads A in place)
+  size_t total;
+};
+
+Plan make_plan(int M, int N, int K, bool pack_a) {
+  Plan p{};
+  p.Kp = round_up(std::max(K, 1), kBK);
+  p.Np = round_up(std::max(N, 1), kBN);
+  p.bp_off = 0;
+  p.bp_bytes = align_up((size_t)p.Kp * p.Np * 4, kAlign);
+  p.ap_off = p.bp_bytes;
+  p.ap_bytes = pack_a ? align_up((size_t)M * p.Kp * 4, kAlign) : 0;
+  p.total = p.ap_off + p.ap_bytes;
+  return p;
+}
+
+bool a_tma_ok(const void* A, long long lda) {
+  return (reinterpret_cast<uintptr_t>(A) % 16 == 0) && ((lda * 4) % 16 == 0);
+}
+
+template <int OP>
+int launch_simt(int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& mB, const EpilogueArgs& ep,
+                cudaStream_t stream) {
+  constexpr int STAGES = kSimtStages;
+  auto kern = srgemm_simt_kernel<OP, STAGES>;
+  const size_t smem = simt_smem_bytes(STAGES);
+  static bool configured[64] = {};  // per instantiation and device
+  int dev = 0;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
+  if (!configured[dev]) {
+    SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured[dev] = true;
+  }
+  const int tiles_m = (M + kBM - 1) / kBM;
+  const int tiles_n = (N + kBN - 1) / kBN;
+  kern<<<tiles_m * tiles_n, kSimtThreads, smem, stream>>>(mA, mB, M, N, K, ep, tiles_m, tiles_n);
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+int dispatch_simt(int op, int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& mB, const EpilogueArgs& ep,
+                  cudaStream_t stream) {
+  switch (op) {
+    case SIMD2_MIN_PLUS: return launch_simt<SIMD2_MIN_PLUS>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_PLUS_MUL: return launch_simt<SIMD2_PLUS_MUL>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_MAX_PLUS: return launch_simt<SIMD2_MAX_PLUS>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_MAX_MIN: return launch_simt<SIMD2_MAX_MIN>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_MAX_MUL: return launch_simt<SIMD2_MAX_MUL>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_MIN_MUL: return launch_simt<SIMD2_MIN_MUL>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_MIN_MAX: return launch_simt<SIMD2_MIN_MAX>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_MINUS_SQUARE: return launch_simt<SIMD2_MINUS_SQUARE>(M, N, K, mA, mB, ep, stream);
+    default: return SIMD2_ERR_UNSUPPORTED;
+  }
+}
+
+// Core float srgemm with an explicit workspace.  T/MODE describe how A and B
+// are read (float as-is, or any type normalised to {0,1}).
+template <typename T, int MODE>
+int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T* B, long long ldb,
+                const EpilogueArgs& ep, uint8_t* ws, const Plan& plan, bool pack_a, cudaStream_t stream) {
+  const float pad = pad_value(op);
+  float* Bp = reinterpret_cast<float*>(ws + plan.bp_off);
+  interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 2), 256, 0, stream>>>(
+      B, ldb, K, N, Bp, plan.Kp, plan.Np, pad);
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  const void* a_base = A;
+  long long a_pitch = lda;
+  if (pack_a) {
+    float* Ap = reinterpret_cast<float*>(ws + plan.ap_off);
+    pack_rows_kernel<T, MODE><<<grid_for((long long)M * plan.Kp), 256, 0, stream>>>(A, lda, M, K, Ap, plan.Kp, pad);
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    a_base = Ap;
+    a_pitch = plan.Kp;
+  }
+  CUtensorMap mA, mB;
+  int rc = make_map_f32(&mA, a_base, M, pack_a ? plan.Kp : K, a_pitch, kBK, kBM, CU_TENSOR_MAP_SWIZZLE_128B,
+                        !is_sum_op(op));
+  if (rc) return rc;
+  rc = make_map_f32(&mB, Bp, plan.Kp / 2, 2LL * plan.Np, 2LL * plan.Np, 2 * kBN, kBK / 2, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    false);
+  if (rc) return rc;
+  return dispatch_simt(op, M, N, K, mA, mB, ep, stream);
+}
+
+int check_dims(int M, int N, int K, long long lda, long long ldb, long long ldc, long long ldd, const void* A,
+               const void* B, const void* C, const void* D, int do_epilogue) {
+  if (M < 0 || N < 0 || K < 0) return SIMD2_ERR_INVALID_ARG;
+  if (M == 0 || N == 0) return SIMD2_OK;
+  if (!D || ldd < N) return SIMD2_ERR_INVALID_ARG;
+  if (K > 0 && (!A || !B || lda < K || ldb < N)) return SIMD2_ERR_INVALID_ARG;
+  if (do_epilogue && (!C || ldc < N)) return SIMD2_ERR_INVALID_ARG;
+  return SIMD2_OK;
+}
+
+// D = id (+) C for K == 0 (a copy of C for every semiring, id otherwise).
+int srgemm_k0(int op, int M, int N, const float* C, long long ldc, float* D, long long ldd, int do_epilogue,
+              cudaStream_t stream) {
+  if (do_epilogue) {
+    SIMD2_CUDA_TRY(cudaMemcpy2DAsync(D, ldd * 4, C, ldc * 4, (size_t)N * 4, M, cudaMemcpyDeviceToDevice, stream));
+  } else {
+    fill_kernel<float><<<grid_for((long long)M * N), 256, 0, stream>>>(D, ldd, M, N, add_identity(op));
+    SIMD2_CUDA_TRY(cudaGetLastError());
+  }
+  return SIMD2_OK;
+}
+
+EpilogueArgs make_epilogue(const float* C, long long ldc, float* D, long long ldd, int do_epilogue, int* changed,
+                           int conv) {
+  EpilogueArgs ep{};
+  ep.C = do_epilogue ? C : D;
+  ep.ldc = do_epilogue ? ldc : ldd;
+  ep.D = D;
+  ep.ldd = ldd;
+  ep.do_epilogue = do_epilogue;
+  ep.vec2 = (reinterpret_cast<uintptr_t>(D) % 8 == 0) && (ldd % 2 == 0) &&
+            (!do_epilogue || ((reinterpret_cast<uintptr_t>(C) % 8 == 0) && (ldc % 2 == 0)));
+  ep.changed = changed;
+  ep.conv_mode = conv;
+  return ep;
+}
+
+int srgemm_f32_ws(int op, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb,
+                  const float* C, long long ldc, float* D, long long ldd, int do_epilogue, int* changed, int conv,
+                  uint8_t* ws_or_null, cudaStream_t stream) {
+  if (K == 0) return srgemm_k0(op, M, N, C, ldc, D, ldd, do_epilogue, stream);
+  const bool pack_a = !a_tma_ok(A, lda);
+  const Plan plan = make_plan(M, N, K, pack_a);
+  uint8_t* ws = ws_or_null;
+  if (!ws) {
+    void* p = nullptr;
+    int rc = get_workspace(stream, plan.total, &p);
+    if (rc) return rc;
+    ws = static_cast<uint8_t*>(p);
+  }
+  const EpilogueArgs ep = make_epilogue(C, ldc, D, ldd, do_epilogue, changed, conv);
+  return srgemm_core<float, 0>(op, M, N, K, A, lda, B, ldb, ep, ws, plan, pack_a, stream);
+}
+
+// or_and through the max_min kernel on {0,1}: AND of booleans is min, OR is
+// max, so the result (converted back to 0/1) is exact.
+template <typename T>
+int srgemm_orand(int M, int N, int K, const T* A, long long lda, const T* B, long long ldb, const T* C, long long ldc,
+                 T* D, long long ldd, int do_epilogue, cudaStream_t stream) {
+  int rc = check_dims(M, N, K, lda, ldb, ldc, ldd, A, B, C, D, do_epilogue);
+  if (rc || M == 0 || N == 0) return rc;
+  if ((rc = check_device())) return rc;
+  const Plan plan = make_plan(M, N, K, true);
+  const size_t c_off = plan.total;
+  const size_t c_bytes = align_up((size_t)M * N * 4, kAlign);
+  const size_t d_off = c_off + c_bytes;
+  const size_t total = d_off + c_bytes;
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, total, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  float* Cf = reinterpret_cast<float*>(ws + c_off);
+  float* Df = reinterpret_cast<float*>(ws + d_off);
+  if (do_epilogue) {
+    pack_rows_kernel<T, 1><<<grid_for((long long)M * N), 256, 0, stream>>>(C, ldc, M, N, Cf, N, 0.0f);
+    SIMD2_CUDA_TRY(cudaGetLastError());
+  }
+  if (K == 0) {
+    rc = srgemm_k0(SIMD2_MAX_MIN, M, N, Cf, N, Df, N, do_epilogue, stream);
+  } else {
+    const EpilogueArgs ep = make_epilogue(Cf, N, Df, N, do_epilogue, nullptr, 0);
+    rc = srgemm_core<T, 1>(SIMD2_MAX_MIN, M, N, K, A, lda, B, ldb, ep, ws, plan, true, stream);
+  }
+  if (rc) return rc;
+  bool_out_kernel<T><<<grid_for((long long)M * N), 256, 0, stream>>>(Df, N, D, ldd, M, N);
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// closure driver
+// ---------------------------------------------------------------------------
+namespace {
+
+int closure_f32(int op, int n, float* X, long long ldx, int max_iter, int conv, int* iters_out,
+                cudaStream_t stream) {
+  if (iters_out) *iters_out = 0;
+  if (n < 0 || max_iter < 0 || !is_float_op(op) || (n > 0 && (!X || ldx < n))) return SIMD2_ERR_INVALID_ARG;
+  if (n == 0 || max_iter == 0) return SIMD2_OK;
+  int rc = check_device();
+  if (rc) return rc;
+  // Workspace: [srgemm plan][Xnew n x n][change flag]
+  const bool pack_a = !a_tma_ok(X, ldx) || (n % 4 != 0);
+  const Plan plan = make_plan(n, n, n, pack_a);
+  const size_t x_off = align_up(plan.total, kAlign);
+  const size_t x_bytes = align_up((size_t)n * n * 4, kAlign);
+  const size_t f_off = x_off + x_bytes;
+  const size_t total = f_off + kAlign;
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, total, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  float* Xn = reinterpret_cast<float*>(ws + x_off);
+  int* flag = reinterpret_cast<int*>(ws + f_off);
+
+  float* cur = X;
+  long long ldcur = ldx;
+  float* nxt = Xn;
+  long long ldnxt = n;
+  int it = 0;
+  int changed = 1;
+  while (changed && it < max_iter) {
+    it++;
+    SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), stream));
+    const bool pk = !a_tma_ok(cur, ldcur);
+    const Plan pl = make_plan(n, n, n, pk);
+    const EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, flag, conv);
+    rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream);
+    if (rc) return rc;
+    int h = 0;
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+    changed = h != 0;
+    std::swap(cur, nxt);
+    std::swap(ldcur, ldnxt);
+  }
+  if (cur != X) {
+    SIMD2_CUDA_TRY(cudaMemcpy2DAsync(X, ldx * 4, cur, ldcur * 4, (size_t)n * 4, n, cudaMemcpyDeviceToDevice, stream));
+  }
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (iters_out) *iters_out = it;
+  return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
+}
+
+}  // namespace
+}  // namespace simd2
+
+using namespace simd2;
+
+extern "C" {
+
+const char* simd2_status_string(int status) {
+  switch (status) {
+    case SIMD2_OK: return "ok";
+    case SIMD2_ERR_INVALID_ARG: return "invalid argument";
+    case SIMD2_ERR_UNSUPPORTED: return "unsupported operation";
+    case SIMD2_ERR_CUDA: return "CUDA runtime error";
+    case SIMD2_ERR_ALLOC: return "workspace allocation failed";
+    case SIMD2_ERR_TIMEOUT: return "device-side wait timed out";
+    case SIMD2_ERR_NOT_CONVERGED: return "closure did not converge within max_iter";
+    case SIMD2_ERR_NO_DEVICE: return "no sm_100 device";
+    default: return "unknown status";
+  }
+}
+
+const char* simd2_version(void) { return "simd2-b200 0.1 sm_100a"; }
+
+int simd2_srgemm(simd2_op op, int M, int N, int K, const float* A, int lda, const float* B, int ldb, const float* C,
+                 int ldc, float* D, int ldd, int do_epilogue, cudaStream_t stream) {
+  if (!is_float_op(op)) return op == SIMD2_OR_AND ? SIMD2_ERR_UNSUPPORTED : SIMD2_ERR_INVALID_ARG;
+  int rc = check_dims(M, N, K, lda, ldb, ldc, ldd, A, B, C, D, do_epilogue);
+  if (rc || M == 0 || N == 0) return rc;
+  if ((rc = check_device())) return rc;
+  return srgemm_f32_ws(op, M, N, K, A, lda, B, ldb, C, ldc, D, ldd, do_epilogue, nullptr, 0, nullptr, stream);
+}
+
+int simd2_srgemm_orand_i32(int M, int N, int K, const int32_t* A, int lda, const int32_t* B, int ldb, const int32_t* C,
+                           int ldc, int32_t* D, int ldd, int do_epilogue, cudaStream_t stream) {
+  return srgemm_orand<int32_t>(M, N, K, A, lda, B, ldb, C, ldc, D, ldd, do_epilogue, stream);
+}
+
+int simd2_srgemm_orand_u8(int M, int N, int K, const uint8_t* A, int lda, const uint8_t* B, int ldb, const uint8_t* C,
+                          int ldc, uint8_t* D, int ldd, int do_epilogue, cudaStream_t stream) {
+  return srgemm_orand<uint8_t>(M, N, K, A, lda, B, ldb, C, ldc, D, ldd, do_epilogue, stream);
+}
+
+int simd2_closure(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_conv conv, int* iters_out,
+                  cudaStream_t stream) {
+  if (conv < SIMD2_CONV_EXACT || conv > SIMD2_CONV_APLP) return SIMD2_ERR_INVALID_ARG;
+  return closure_f32(op, n, X, ldx, max_iter, conv, iters_out, stream);
+}
+
+int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_out, cudaStream_t stream) {
+  if (iters_out) *iters_out = 0;
+  if (n < 0 || max_iter < 0 || (n > 0 && (!X || ldx < n))) return SIMD2_ERR_INVALID_ARG;
+  if (n == 0 || max_iter == 0) return SIMD2_OK;
+  int rc = check_device();
+  if (rc) return rc;
+  // Boolean closure as max_min on a {0,1} float copy (exact), then back to bytes.
+  float* Xf = nullptr;
+  SIMD2_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&Xf), (size_t)n * n * 4, stream));
+  pack_rows_kernel<uint8_t, 1><<<grid_for((long long)n * n), 256, 0, stream>>>(X, ldx, n, n, Xf, n, 0.0f);
+  rc = closure_f32(SIMD2_MAX_MIN, n, Xf, n, max_iter, SIMD2_CONV_EXACT, iters_out, stream);
+  if (rc == SIMD2_OK || rc == SIMD2_ERR_NOT_CONVERGED) {
+    bool_out_kernel<uint8_t><<<grid_for((long long)n * n), 256, 0, stream>>>(Xf, n, X, ldx, n, n);
+  }
+  cudaFreeAsync(Xf, stream);
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return SIMD2_ERR_CUDA;
+  return rc;
+}
+
+int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t stream, size_t* bytes_out) {
+  if (M < 0 || N < 0 || K < 0 || (int)op < 0 || (int)op > 8) return SIMD2_ERR_INVALID_ARG;
+  const Plan plan = make_plan(M, N, K, true);
+  size_t total = plan.total + 2 * align_up((size_t)M * N * 4, kAlign) + kAlign;
+  void* p = nullptr;
+  int rc = get_workspace(stream, total, &p);
+  if (bytes_out) *bytes_out = rc ? 0 : total;
+  return rc;
+}
+
+int simd2_release_workspaces(void) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return SIMD2_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  cudaDeviceSynchronize();
+  for (auto it = g_ws.begin(); it != g_ws.end();) {
+    if (it->first.first == dev) {
+      cudaFree(it->second.first);
+      it = g_ws.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  return SIMD2_OK;
+}
+
+int simd2_device_status(void) {
+  if (cudaDeviceSynchronize() != cudaSuccess) return SIMD2_ERR_CUDA;
+  int h = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&h, g_device_status, sizeof(int)) != cudaSuccess) return SIMD2_ERR_CUDA;
+  if (cudaMemcpyToSymbol(g_device_status, &zero, sizeof(int)) != cudaSuccess) return SIMD2_ERR_CUDA;
+  return h;
+}
+
+}  // extern "C"

@@ -1,0 +1,241 @@
+// srgemm_simt.cuh -- FP32 CUDA-core semiring GEMM for sm_100a.
+//
+// Computes one BM x BN tile of D = id (+) A(x)B [(+) C] per CTA, the
+// row-major contract of mmo::host_srgemm (escalab/SIMD2 kernel/host_srgemm.h:17-49).
+//
+//   * 1 producer warp issues 2D TMA loads (no multicast) of an A tile
+//     [BM rows][BK k] (128-byte swizzle) and a B' tile into a STAGES-deep ring
+//     in shared memory, with full/empty mbarriers per stage.
+//   * B' is B with consecutive k rows interleaved in pairs,
+//     B'[p][2j+e] = B[2p+e][j], written once per call by interleave_pairs
+//     (prep.cu).  A thread then holds (A[i][2p], A[i][2p+1]) and
+//     (B[2p][j], B[2p+1][j]) as register pairs, forms both products with one
+//     packed f32x2 add/mul (each element rounded exactly like the scalar op),
+//     and folds both into the accumulator with one three-operand min/max.
+//   * 8 consumer warps each own a 16 x 128 slab; each thread holds an
+//     8 x 8 register tile (rows ty+16i, columns 32c+2tx+e).
+//   * The epilogue applies (+) C, writes D with coalesced 8-byte stores and,
+//     for the closure, sets one change flag per warp (warp vote + atomicOr).
+//
+// Out-of-range k is filled with NaN for the min/max semirings (TMA OOB fill
+// for A, explicit padding for B'): a NaN product is dropped by min/max, so the
+// tail adds nothing.  The summing semirings use zero fill.
+#pragma once
+#include "common.cuh"
+
+namespace simd2 {
+
+constexpr int kBM = 128;
+constexpr int kBN = 128;
+constexpr int kBK = 32;
+constexpr int kConsumerWarps = 8;
+constexpr int kSimtThreads = (kConsumerWarps + 1) * 32;
+constexpr int kATileBytes = kBM * kBK * 4;  // 16 KiB
+constexpr int kBTileBytes = kBK * kBN * 4;  // 16 KiB
+constexpr int kStageBytes = kATileBytes + kBTileBytes;
+constexpr int kSimtStages = 4;
+
+constexpr size_t simt_smem_bytes(int stages) {
+  return (size_t)stages * kStageBytes + 1024 /* alignment slack */ + 2 * stages * sizeof(uint64_t);
+}
+
+// Fused multiply-accumulate of two k terms into one output.
+template <int OP>
+struct Mac {
+  __device__ static float mac2(float acc, float2 a, float2 b) {
+    const float2 p = Semiring<OP>::mul2(a, b);
+    return Semiring<OP>::add3(acc, p.x, p.y);
+  }
+  __device__ static float identity() { return Semiring<OP>::identity(); }
+  __device__ static float add(float acc, float p) { return Semiring<OP>::add(acc, p); }
+};
+
+// plus_mul on CUDA cores (reference-precision FP32 path).
+template <>
+struct Mac<SIMD2_PLUS_MUL> {
+  __device__ static float mac2(float acc, float2 a, float2 b) { return fmaf(a.y, b.y, fmaf(a.x, b.x, acc)); }
+  __device__ static float identity() { return 0.0f; }
+  __device__ static float add(float acc, float p) { return __fadd_rn(acc, p); }
+};
+
+// minus_square on CUDA cores: sum_k (a-b)^2.
+template <>
+struct Mac<SIMD2_MINUS_SQUARE> {
+  __device__ static float mac2(float acc, float2 a, float2 b) {
+    const float2 d = __fadd2_rn(a, make_float2(-b.x, -b.y));
+    return fmaf(d.y, d.y, fmaf(d.x, d.x, acc));
+  }
+  __device__ static float identity() { return 0.0f; }
+  __device__ static float add(float acc, float p) { return __fadd_rn(acc, p); }
+};
+
+struct EpilogueArgs {
+  const float* C;
+  long long ldc;
+  float* D;
+  long long ldd;
+  int do_epilogue;
+  int vec2;       // C/D rows are 8-byte aligned: use float2 accesses
+  int* changed;   // nullable: set to 1 when any D element differs from C
+  int conv_mode;  // simd2_conv, used with `changed`
+};
+
+__device__ __forceinline__ bool conv_changed(int mode, float old_v, float new_v) {
+  if (mode == SIMD2_CONV_TOL) return fabsf(old_v - new_v) > 0.0001f;
+  return __float_as_uint(old_v) != __float_as_uint(new_v);
+}
+
+template <int OP>
+__device__ __forceinline__ float epilogue_value(const EpilogueArgs& ep, float v, float c, int& changed) {
+  if (ep.do_epilogue) v = Mac<OP>::add(v, c);
+  if (ep.conv_mode == SIMD2_CONV_APLP && v > -1.0f && v < 1.0f) v = -3.402823466e+38f;
+  if (ep.changed && conv_changed(ep.conv_mode, c, v)) changed = 1;
+  return v;
+}
+
+template <int OP, int STAGES>
+__global__ void __launch_bounds__(kSimtThreads, 1)
+    srgemm_simt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M,
+                       int N, int K, EpilogueArgs ep, int tiles_m, int tiles_n) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
+  uint64_t* empty = full + STAGES;
+
+  // Grouped raster: 8 consecutive tile rows share each B' column panel in L2.
+  const int group = 8;
+  const int per_group = group * tiles_n;
+  const int g = blockIdx.x / per_group;
+  const int first_m = g * group;
+  const int gsize = min(tiles_m - first_m, group);
+  const int local = blockIdx.x - g * per_group;
+  const int tm = first_m + local % gsize;
+  const int tn = local / gsize;
+  const int m0 = tm * kBM;
+  const int n0 = tn * kBN;
+  const int ktiles = (K + kBK - 1) / kBK;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == kConsumerWarps) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      prefetch_tensormap(&tmA);
+      prefetch_tensormap(&tmB);
+      int issued = 0;
+      for (int kt = 0; kt < ktiles; kt++) {
+        const int s = kt % STAGES;
+        const uint32_t round = kt / STAGES;
+        if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
+          report_error(SIMD2_ERR_TIMEOUT);
+          break;
+        }
+        uint8_t* sa = smem + s * kStageBytes;
+        mbar_arrive_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(sa, &tmA, &full[s], kt * kBK, m0);
+        tma_load_2d(sa + kATileBytes, &tmB, &full[s], 2 * n0, kt * (kBK / 2));
+        issued = kt + 1;
+      }
+      // Every issued copy must land before this CTA's shared memory is released.
+      for (int kt = max(0, issued - STAGES); kt < issued; kt++) {
+        if (!mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1)) report_error(SIMD2_ERR_TIMEOUT);
+      }
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const int tx = lane & 15;
+  const int ty = warp * 2 + (lane >> 4);
+  const int swz = ty & 7;  // row & 7 for every row this thread reads (rows ty + 16 i)
+
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = Mac<OP>::identity();
+
+  bool ok = true;
+  for (int kt = 0; kt < ktiles; kt++) {
+    const int s = kt % STAGES;
+    if (!mbar_wait(&full[s], (kt / STAGES) & 1)) {
+      report_error(SIMD2_ERR_TIMEOUT);
+      ok = false;
+      break;
+    }
+    const float* As = reinterpret_cast<const float*>(smem + s * kStageBytes);
+    const float* Bs = reinterpret_cast<const float*>(smem + s * kStageBytes + kATileBytes);
+#pragma unroll 2
+    for (int q = 0; q < kBK / 4; q++) {
+      float4 a[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        a[i] = *reinterpret_cast<const float4*>(As + (ty + 16 * i) * kBK + ((q ^ swz) << 2));
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        float4 b[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+          b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (32 * c + 2 * tx) * 2);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const float2 ap = h == 0 ? make_float2(a[i].x, a[i].y) : make_float2(a[i].z, a[i].w);
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            acc[i][2 * c] = Mac<OP>::mac2(acc[i][2 * c], ap, make_float2(b[c].x, b[c].y));
+            acc[i][2 * c + 1] = Mac<OP>::mac2(acc[i][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (!ok) return;
+
+  // ---------------- epilogue ----------------
+  int changed = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int row = m0 + ty + 16 * i;
+    if (row < M) {
+      const float* crow = ep.C + (long long)row * ep.ldc;
+      float* drow = ep.D + (long long)row * ep.ldd;
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const int col = n0 + 32 * c + 2 * tx;
+        if (ep.vec2 && col + 1 < N) {
+          float2 cv = make_float2(0.f, 0.f);
+          if (ep.do_epilogue) cv = *reinterpret_cast<const float2*>(crow + col);
+          float2 v;
+          v.x = epilogue_value<OP>(ep, acc[i][2 * c], cv.x, changed);
+          v.y = epilogue_value<OP>(ep, acc[i][2 * c + 1], cv.y, changed);
+          *reinterpret_cast<float2*>(drow + col) = v;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            if (col + e < N) {
+              const float cv = ep.do_epilogue ? crow[col + e] : 0.0f;
+              drow[col + e] = epilogue_value<OP>(ep, acc[i][2 * c + e], cv, changed);
+            }
+          }
+        }
+      }
+    }
+  }
+  if (ep.changed) {
+    if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
+  }
+}
+
+}  // namespace simd2

@@ -1,0 +1,154 @@
+"""GPU parity: libsimd2 srgemm (through the C ABI) against the CPU oracle.
+
+Min/max semirings and or_and must be bit-exact against host_srgemm semantics.
+plus_mul and minus_square are compared with the FP64 oracle under the
+forward-error bound |D - D64| <= TOL_K * K * 2^-24 * S, where
+S = sum_k |a_ik (x) b_kj| + |c_ij| is the absolute-value sum of the terms.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import simd2_b200 as s2
+from simd2_b200 import datagen
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+MINMAX = ["min_plus", "max_plus", "max_min", "max_mul", "min_mul", "min_max"]
+SUMS = ["plus_mul", "minus_square"]
+EPS32 = 2.0 ** -24
+TOL_K = 2.0  # bound constant for the summing semirings (FP32 accumulate)
+
+SHAPES = [(1, 1, 1), (17, 23, 13), (128, 128, 32), (129, 130, 33), (64, 256, 100), (300, 517, 257), (7, 5, 700)]
+
+
+def bits(x):
+    x = np.ascontiguousarray(x)
+    return x.view(np.uint32) if x.dtype == np.float32 else x
+
+
+def run_gpu(op, a, b, c, epi, dev):
+    A = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    B = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+    C = torch.from_numpy(np.ascontiguousarray(c)).to(dev)
+    D = s2.srgemm(op, A, B, C, do_epilogue=epi)
+    torch.cuda.synchronize()
+    return D.cpu().numpy()
+
+
+def abs_sum(op, a, b, c, epi):
+    a64, b64 = np.abs(a.astype(np.float64)), np.abs(b.astype(np.float64))
+    if op == "plus_mul":
+        s = a64 @ b64
+    else:  # (a-b)^2 <= 2a^2 + 2b^2
+        s = 2 * (a64 ** 2).sum(1)[:, None] + 2 * (b64 ** 2).sum(0)[None, :]
+    if epi:
+        s = s + np.abs(c.astype(np.float64))
+    return s
+
+
+def check_sum_op(op, a, b, c, epi, got):
+    want = oracle.srgemm_f64(op, a, b, c, do_epilogue=epi)
+    k = a.shape[1]
+    bound = TOL_K * max(k, 1) * EPS32 * abs_sum(op, a, b, c, epi) + 1e-30
+    err = np.abs(got.astype(np.float64) - want)
+    assert np.all(err <= bound), f"{op}: max err {err.max():.3e}, worst ratio {(err / bound).max():.3f}"
+
+
+@pytest.mark.parametrize("op", MINMAX + SUMS)
+@pytest.mark.parametrize("shape", SHAPES)
+def test_srgemm_random_shapes(cuda, op, shape):
+    m, n, k = shape
+    a, b, c = datagen.semiring_operands(op, m, n, k, seed=m * 131 + n * 7 + k)
+    for epi in (False, True):
+        got = run_gpu(op, a, b, c, epi, cuda)
+        if op in MINMAX:
+            want = oracle.srgemm(op, a, b, c, do_epilogue=epi)
+            np.testing.assert_array_equal(bits(got), bits(want), err_msg=f"{op} {shape} epi={epi}")
+        else:
+            check_sum_op(op, a, b, c, epi, got)
+
+
+@pytest.mark.parametrize("op", oracle.OPS)
+def test_srgemm_golden(cuda, op):
+    g = np.load(os.path.join(GOLDEN, f"srgemm_{op}.npz"))
+    for s in sorted({k.split("_")[0] for k in g.files}):
+        a, b, c = g[f"{s}_A"], g[f"{s}_B"], g[f"{s}_C"]
+        for epi in (0, 1):
+            got = run_gpu(op, a, b, c, bool(epi), cuda)
+            if op in SUMS:
+                check_sum_op(op, a, b, c, bool(epi), got)
+            else:
+                np.testing.assert_array_equal(bits(got), bits(g[f"{s}_e{epi}_D"]), err_msg=f"{op} {s} e{epi}")
+
+
+@pytest.mark.parametrize("dtype", [np.int32, np.uint8])
+def test_or_and(cuda, dtype):
+    for (m, n, k) in [(1, 1, 1), (33, 65, 17), (200, 130, 300)]:
+        a, b, c = datagen.semiring_operands("or_and", m, n, k, seed=k)
+        a = (np.random.default_rng(1).random((m, k)) < 0.2).astype(dtype) * 3  # nonzero != 1 is true too
+        a, b, c = a.astype(dtype), b.astype(dtype), c.astype(dtype)
+        for epi in (False, True):
+            got = run_gpu("or_and", a, b, c, epi, cuda)
+            want = oracle.srgemm("or_and", a.astype(np.int32), b.astype(np.int32), c.astype(np.int32),
+                                 do_epilogue=epi)
+            np.testing.assert_array_equal(got.astype(np.int32), want)
+
+
+def test_k_zero_and_empty(cuda):
+    for op in MINMAX + SUMS:
+        a, b, c = datagen.semiring_operands(op, 9, 11, 0, seed=1)
+        got = run_gpu(op, a, b, c, False, cuda)
+        want = oracle.srgemm(op, a, b, c, do_epilogue=False)
+        np.testing.assert_array_equal(bits(got), bits(want))
+        got = run_gpu(op, a, b, c, True, cuda)
+        np.testing.assert_array_equal(bits(got), bits(c))
+    A = torch.zeros((0, 5), device=cuda)
+    B = torch.zeros((5, 3), device=cuda)
+    assert s2.srgemm("min_plus", A, B).shape == (0, 3)
+
+
+def test_strided_and_unaligned_operands(cuda):
+    """Row pitches that are not multiples of 4 floats take the packing path."""
+    op = "min_plus"
+    m, n, k = 70, 90, 45
+    a, b, c = datagen.semiring_operands(op, m, n, k, seed=9)
+    Abig = torch.full((m, k + 3), 5.0, device=cuda)
+    Abig[:, :k] = torch.from_numpy(a).to(cuda)
+    Bbig = torch.full((k, n + 1), 5.0, device=cuda)
+    Bbig[:, :n] = torch.from_numpy(b).to(cuda)
+    Cbig = torch.full((m, n + 5), 5.0, device=cuda)
+    Cbig[:, :n] = torch.from_numpy(c).to(cuda)
+    Dbig = torch.full((m, n + 7), -1.0, device=cuda)
+    s2.srgemm(op, Abig[:, :k], Bbig[:, :n], Cbig[:, :n], do_epilogue=True, D=Dbig[:, :n])
+    torch.cuda.synchronize()
+    want = oracle.srgemm(op, a, b, c, do_epilogue=True)
+    np.testing.assert_array_equal(bits(Dbig[:, :n].cpu().numpy()), bits(want))
+    assert torch.all(Dbig[:, n:] == -1.0)  # nothing written past N
+
+
+def test_in_place_epilogue(cuda):
+    """D aliasing C accumulates in place (host_srgemm's D += semantics)."""
+    op = "max_plus"
+    a, b, c = datagen.semiring_operands(op, 100, 120, 64, seed=4)
+    A, B = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+    C = torch.from_numpy(c).to(cuda)
+    s2.srgemm(op, A, B, C, do_epilogue=True, D=C)
+    torch.cuda.synchronize()
+    want = oracle.srgemm(op, a, b, c, do_epilogue=True)
+    np.testing.assert_array_equal(bits(C.cpu().numpy()), bits(want))
+
+
+@pytest.mark.parametrize("op", MINMAX)
+def test_full_size_row_sample(cuda, op):
+    """4096^3 (the nine-semiring sweep size): bit-exact on a sample of rows."""
+    n = 4096
+    a, b, c = datagen.semiring_operands(op, n, n, n, seed=77)
+    got = run_gpu(op, a, b, c, True, cuda)
+    rows = np.random.default_rng(0).choice(n, size=24, replace=False)
+    want = oracle.srgemm(op, a[rows], b, c[rows], do_epilogue=True)
+    np.testing.assert_array_equal(bits(got[rows]), bits(want))
+    assert s2.device_status() == 0
