@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""bench.py -- srgemm throughput on B200 through libsimd2.
+
+Default workload: the nine-semiring srgemm sweep at M = N = K = 4096
+(min_plus, plus_mul, max_plus, max_min, max_mul, min_mul, min_max, or_and,
+minus_square).  One step runs all nine once.  Inputs are seeded synthetic
+matrices with the sweep's value distributions (integer-valued FP32 in
+[1,1000] with 20% +-inf add-identities for the min/max semirings, U(0,1] for
+the *_mul ones, N(0,1) for plus_mul / minus_square, uint8 Bernoulli(0.01)
+for or_and).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl simd2|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs the sweep on its
+own inputs (independent problems, no collective in the data path): weak
+scaling, value = all ranks' operations / max-over-ranks time.
+
+``--impl reference`` times the reference's own CPU srgemm
+(escalab/SIMD2 kernel/host_srgemm.h, compiled unchanged into
+oracle/_ref/libref.so; the C restatement in oracle/ if that library is
+absent) on every host core, on a bounded row sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SWEEP_OPS = ("min_plus", "plus_mul", "max_plus", "max_min", "max_mul", "min_mul", "min_max", "or_and",
+             "minus_square")
+METRIC = "srgemm Gop/s & % CUDA-core/tensor peak; batched APSP graphs/s vs plain path"
+SMS = 148
+LANES = 128
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("simd2", "reference"), default="simd2")
+    p.add_argument("--n", type=int, default=4096, help="M = N = K of the sweep")
+    p.add_argument("--ref-rows", type=int, default=max(8, os.cpu_count() or 1),
+                   help="rows per semiring in the CPU sample (one per host core)")
+    p.add_argument("--ops", default=",".join(SWEEP_OPS),
+                   help="comma-separated subset of the sweep (profiling runs use one semiring)")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm.append(float(parts[1]))
+                        mx.append(float(parts[2]))
+                    except ValueError:
+                        continue
+                    for nm, v in zip(names, parts[5:9]):
+                        if v.lower() == "active":
+                            reasons.add(nm)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the reference's host_srgemm on a bounded row sample
+# --------------------------------------------------------------------------
+def cpu_sample_inputs(n, rows, seed=11):
+    from simd2_b200 import datagen
+    out = {}
+    for i, op in enumerate(SWEEP_OPS):
+        # rows x n slice of A, full B, rows x n slice of C, same distributions
+        a, _, c = datagen.semiring_operands(op, rows, n, n, seed=seed + i)
+        _, b, _ = datagen.semiring_operands(op, 1, n, n, seed=seed + 100 + i)
+        out[op] = (a, b, c)
+    return out
+
+
+def cpu_sweep(inputs, threads):
+    """Runs one sampled sweep on the CPU; returns (ops, seconds, kind)."""
+    import oracle
+    use_ref = oracle.ref_lib() is not None
+    kind = "reference" if use_ref else "port"
+    ops = 0.0
+    t0 = time.perf_counter()
+    for op, (a, b, c) in inputs.items():
+        if op == "or_and" and use_ref:
+            oracle.srgemm(op, a.astype(np.int32), b.astype(np.int32), c.astype(np.int32), do_epilogue=True,
+                          threads=threads, use_ref=True)
+        else:
+            oracle.srgemm(op, a, b, c, do_epilogue=True, threads=threads, use_ref=use_ref)
+        ops += 2.0 * a.shape[0] * b.shape[1] * a.shape[1]
+    return ops, time.perf_counter() - t0, kind
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    inputs = cpu_sample_inputs(args.n, args.ref_rows)
+    for _ in range(max(args.warmup, 0)):
+        cpu_sweep(inputs, threads)
+    tot_ops, tot_s, kind = 0.0, 0.0, "port"
+    for _ in range(args.steps):
+        o, s, kind = cpu_sweep(inputs, threads)
+        tot_ops += o
+        tot_s += s
+    gops = tot_ops / tot_s / 1e9
+    sample = (f"{args.ref_rows} rows x {args.n} x {args.n} per semiring, all nine semirings per step "
+              f"(host_srgemm on row panels, one thread per core)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gops, "unit": "Gop/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_s / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"nine-semiring srgemm sweep M=N=K={args.n} (or_and uint8, int32 for host_srgemm)",
+                   "sample": sample},
+        "cpu_baseline": {"value": gops, "unit": "Gop/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": gops, "unit": "Gop/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+def traffic_from_profile():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "srgemm_simt_kernel_min_plus_4096.md")
+    try:
+        with open(path) as f:
+            m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
+            return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def main():
+    global SWEEP_OPS
+    args = parse_args()
+    SWEEP_OPS = tuple(op for op in args.ops.split(",") if op)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import simd2_b200 as s2
+    from simd2_b200 import datagen
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    n = args.n
+    s2.lib()
+    # inputs: resident in HBM for `value`, pinned on the host for `e2e`
+    host, devb = {}, {}
+    for i, op in enumerate(SWEEP_OPS):
+        a, b, c = datagen.semiring_operands(op, n, n, n, seed=1000 * rank + i)
+        host[op] = tuple(torch.from_numpy(x).pin_memory() for x in (a, b, c))
+        devb[op] = tuple(x.to(dev, non_blocking=True) for x in host[op])
+    outs = {op: torch.empty((n, n), dtype=devb[op][2].dtype, device=dev) for op in SWEEP_OPS}
+    torch.cuda.synchronize()
+
+    def step():
+        for op in SWEEP_OPS:
+            A, B, C = devb[op]
+            s2.srgemm(op, A, B, C, do_epilogue=True, D=outs[op])
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = s2.launch_count()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        with s2.KernelTimer() as kt:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+    launches = s2.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    ops_per_step = 2.0 * n ** 3 * len(SWEEP_OPS)
+    value = ops_per_step * args.steps * world / (ms_max / 1e3) / 1e9
+    assert s2.device_status() == 0, "a kernel reported a device-side error"
+
+    # per-semiring kernel throughput (one timed launch each, after the sweep)
+    per_op = {}
+    for op in SWEEP_OPS:
+        A, B, C = devb[op]
+        with s2.KernelTimer() as t1:
+            for _ in range(3):
+                s2.srgemm(op, A, B, C, do_epilogue=True, D=outs[op])
+        per_op[op] = t1.ops / (t1.kernel_ms / 1e3) / 1e9
+
+    # e2e through the public API with host buffers: H2D inputs, srgemm, D2H result,
+    # pipelined over two buffer sets and three streams.
+    e2e = None
+    if not args.no_e2e:
+        s_in, s_cmp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+        slots = [{op: (torch.empty_like(devb[op][0]), torch.empty_like(devb[op][1]), torch.empty_like(devb[op][2]),
+                       torch.empty_like(outs[op])) for op in SWEEP_OPS} for _ in range(2)]
+        host_out = {op: torch.empty((n, n), dtype=outs[op].dtype).pin_memory() for op in SWEEP_OPS}
+        bi = sum(sum(x.numel() * x.element_size() for x in host[op]) for op in SWEEP_OPS)
+        bo = sum(host_out[op].numel() * host_out[op].element_size() for op in SWEEP_OPS)
+
+        def e2e_step(free_ev):
+            for j, op in enumerate(SWEEP_OPS):
+                slot = slots[j % 2][op]
+                with torch.cuda.stream(s_in):
+                    if free_ev[j % 2] is not None:
+                        s_in.wait_event(free_ev[j % 2])
+                    for hx, dx in zip(host[op], slot[:3]):
+                        dx.copy_(hx, non_blocking=True)
+                    in_ev = torch.cuda.Event()
+                    in_ev.record(s_in)
+                with torch.cuda.stream(s_cmp):
+                    s_cmp.wait_event(in_ev)
+                    s2.srgemm(op, slot[0], slot[1], slot[2], do_epilogue=True, D=slot[3], stream=s_cmp)
+                    c_ev = torch.cuda.Event()
+                    c_ev.record(s_cmp)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(c_ev)
+                    host_out[op].copy_(slot[3], non_blocking=True)
+                    f_ev = torch.cuda.Event()
+                    f_ev.record(s_out)
+                free_ev[j % 2] = f_ev
+
+        free = [None, None]
+        for _ in range(2):
+            e2e_step(free)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.steps // 3)):
+            e2e_step(free)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        e2e_steps = max(1, args.steps // 3)
+        et = torch.tensor([e2e_s], device=dev)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": ops_per_step * e2e_steps * world / float(et.item()) / 1e9, "unit": "Gop/s",
+               "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+               "how": "pinned host buffers; per semiring H2D(A,B,C) -> srgemm -> D2H(D), two buffer sets on "
+                      "three streams; wall clock around synchronize"}
+
+    clocks = clk.summary()
+    peaks, peak_kind = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    issue_peak_gops = SMS * LANES * sm_max * 1e6 / 1e9  # 2 ops/MAC == 2 lane-instructions/MAC
+    achieved = kt.ops / (kt.kernel_ms / 1e3) / 1e9 if kt.kernel_ms > 0 else None
+    traffic = traffic_from_profile()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        inputs = cpu_sample_inputs(n, args.ref_rows)
+        o, s_, kind = cpu_sweep(inputs, threads)
+        cpu = {"value": o / s_ / 1e9, "unit": "Gop/s", "cores": threads, "kind": kind,
+               "sample": f"{args.ref_rows} rows x {n} x {n} per semiring, all nine semirings, one sweep"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gop/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"nine-semiring srgemm sweep M=N=K={n} (or_and uint8 0/1 density 0.01)",
+                       "l2": "inputs larger than L2: 9 semirings x (A,B,C) x 64 MiB rotated every step",
+                       "parallelism": f"independent sweep per rank x{world}"},
+            "per_semiring_kernel_gops": per_op,
+            "roofline": {"bound": "cuda_core_issue", "kernel": "srgemm_simt_kernel (all semirings)",
+                         "achieved": achieved, "peak": issue_peak_gops, "unit": "Gop/s",
+                         "frac": achieved / issue_peak_gops if achieved else None, "traffic": traffic,
+                         "peak_source": f"{SMS} SMs x {LANES} lanes x {sm_max:.0f} MHz ({peak_kind} sm_max_mhz); "
+                                        "2 ops per (x),(+) pair = 2 lane-instructions",
+                         "timed_launches": kt.launches},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -118,6 +118,16 @@ int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t strea
 /* Free every workspace the library holds on the current device. */
 int simd2_release_workspaces(void);
 
+/* Running total of kernels this library has launched in this process. */
+long long simd2_launch_count(void);
+
+/* Kernel timing: between begin and end, every main srgemm kernel launch is
+ * bracketed by CUDA events on its own stream.  end() waits for them and
+ * returns the summed kernel time, the number of timed launches and the
+ * algorithmic operation count (2*M*N*K per launch). */
+int simd2_profile_begin(void);
+int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops);
+
 /* Read and clear the device-side error word that kernels set when a bounded
  * wait runs out (SIMD2_ERR_TIMEOUT).  Synchronizes the current device. */
 int simd2_device_status(void);

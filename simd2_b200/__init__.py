@@ -62,9 +62,14 @@ def lib() -> ctypes.CDLL:
         L.simd2_status_string.argtypes = [I]
         L.simd2_status_string.restype = ctypes.c_char_p
         L.simd2_version.restype = ctypes.c_char_p
+        L.simd2_launch_count.argtypes = []
+        L.simd2_launch_count.restype = ctypes.c_longlong
+        L.simd2_profile_begin.argtypes = []
+        L.simd2_profile_end.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_longlong)]
         for name in ("simd2_srgemm", "simd2_srgemm_orand_i32", "simd2_srgemm_orand_u8", "simd2_closure",
                      "simd2_closure_orand_u8", "simd2_reserve_workspace", "simd2_release_workspaces",
-                     "simd2_device_status"):
+                     "simd2_device_status", "simd2_profile_begin", "simd2_profile_end"):
             getattr(L, name).restype = I
         _lib = L
     return _lib
@@ -157,6 +162,26 @@ def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", 
 def device_status() -> int:
     """Read and clear the device-side error word (0 = no kernel reported an error)."""
     return lib().simd2_device_status()
+
+
+def launch_count() -> int:
+    """Kernels launched by libsimd2 so far in this process."""
+    return int(lib().simd2_launch_count())
+
+
+class KernelTimer:
+    """Times every main srgemm kernel launched inside the ``with`` block with
+    CUDA events recorded on the kernel's own stream."""
+
+    def __enter__(self):
+        _check(lib().simd2_profile_begin(), "profile_begin")
+        return self
+
+    def __exit__(self, *exc):
+        ms, n, ops = ctypes.c_double(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
+        _check(lib().simd2_profile_end(ctypes.byref(ms), ctypes.byref(n), ctypes.byref(ops)), "profile_end")
+        self.kernel_ms, self.launches, self.ops = ms.value, n.value, ops.value
+        return False
 
 
 def version() -> str:

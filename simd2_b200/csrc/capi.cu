@@ -9,7 +9,9 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <atomic>
 #include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "prep.cuh"
@@ -47,6 +49,33 @@ int check_device() {
     rc = SIMD2_ERR_NO_DEVICE;
   verdict[dev] = rc;
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// launch accounting: a running count of every kernel this library launched,
+// and optional CUDA-event timing of the main srgemm kernels (recorded on the
+// stream each kernel is launched on).
+// ---------------------------------------------------------------------------
+std::atomic<long long> g_launches{0};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
+size_t g_prof_used = 0;
+long long g_prof_ops = 0;
+
+inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// Returns the event pair to bracket a main-kernel launch, or nullptr.
+std::pair<cudaEvent_t, cudaEvent_t>* prof_slot(long long ops) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on) return nullptr;
+  if (g_prof_used == g_prof_events.size()) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return nullptr;
+    g_prof_events.push_back({a, b});
+  }
+  g_prof_ops += ops;
+  return &g_prof_events[g_prof_used++];
 }
 
 // ---------------------------------------------------------------------------
@@ -170,7 +199,11 @@ int launch_simt(int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& m
   }
   const int tiles_m = (M + kBM - 1) / kBM;
   const int tiles_n = (N + kBN - 1) / kBN;
+  auto* ev = prof_slot(2LL * M * N * K);
+  if (ev) cudaEventRecord(ev->first, stream);
   kern<<<tiles_m * tiles_n, kSimtThreads, smem, stream>>>(mA, mB, M, N, K, ep, tiles_m, tiles_n);
+  count_launch();
+  if (ev) cudaEventRecord(ev->second, stream);
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
 }
@@ -199,12 +232,14 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   float* Bp = reinterpret_cast<float*>(ws + plan.bp_off);
   interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 2), 256, 0, stream>>>(
       B, ldb, K, N, Bp, plan.Kp, plan.Np, pad);
+  count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   const void* a_base = A;
   long long a_pitch = lda;
   if (pack_a) {
     float* Ap = reinterpret_cast<float*>(ws + plan.ap_off);
     pack_rows_kernel<T, MODE><<<grid_for((long long)M * plan.Kp), 256, 0, stream>>>(A, lda, M, K, Ap, plan.Kp, pad);
+    count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
     a_base = Ap;
     a_pitch = plan.Kp;
@@ -236,6 +271,7 @@ int srgemm_k0(int op, int M, int N, const float* C, long long ldc, float* D, lon
     SIMD2_CUDA_TRY(cudaMemcpy2DAsync(D, ldd * 4, C, ldc * 4, (size_t)N * 4, M, cudaMemcpyDeviceToDevice, stream));
   } else {
     fill_kernel<float><<<grid_for((long long)M * N), 256, 0, stream>>>(D, ldd, M, N, add_identity(op));
+    count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
   }
   return SIMD2_OK;
@@ -293,6 +329,7 @@ int srgemm_orand(int M, int N, int K, const T* A, long long lda, const T* B, lon
   float* Df = reinterpret_cast<float*>(ws + d_off);
   if (do_epilogue) {
     pack_rows_kernel<T, 1><<<grid_for((long long)M * N), 256, 0, stream>>>(C, ldc, M, N, Cf, N, 0.0f);
+    count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
   }
   if (K == 0) {
@@ -303,6 +340,7 @@ int srgemm_orand(int M, int N, int K, const T* A, long long lda, const T* B, lon
   }
   if (rc) return rc;
   bool_out_kernel<T><<<grid_for((long long)M * N), 256, 0, stream>>>(Df, N, D, ldd, M, N);
+  count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
 }
@@ -421,9 +459,11 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
   float* Xf = nullptr;
   SIMD2_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&Xf), (size_t)n * n * 4, stream));
   pack_rows_kernel<uint8_t, 1><<<grid_for((long long)n * n), 256, 0, stream>>>(X, ldx, n, n, Xf, n, 0.0f);
+  count_launch();
   rc = closure_f32(SIMD2_MAX_MIN, n, Xf, n, max_iter, SIMD2_CONV_EXACT, iters_out, stream);
   if (rc == SIMD2_OK || rc == SIMD2_ERR_NOT_CONVERGED) {
     bool_out_kernel<uint8_t><<<grid_for((long long)n * n), 256, 0, stream>>>(Xf, n, X, ldx, n, n);
+    count_launch();
   }
   cudaFreeAsync(Xf, stream);
   if (cudaStreamSynchronize(stream) != cudaSuccess) return SIMD2_ERR_CUDA;
@@ -453,6 +493,33 @@ int simd2_release_workspaces(void) {
       ++it;
     }
   }
+  return SIMD2_OK;
+}
+
+long long simd2_launch_count(void) { return g_launches.load(); }
+
+int simd2_profile_begin(void) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = true;
+  g_prof_used = 0;
+  g_prof_ops = 0;
+  return SIMD2_OK;
+}
+
+int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = false;
+  double total = 0.0;
+  for (size_t i = 0; i < g_prof_used; i++) {
+    if (cudaEventSynchronize(g_prof_events[i].second) != cudaSuccess) return SIMD2_ERR_CUDA;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, g_prof_events[i].first, g_prof_events[i].second) != cudaSuccess)
+      return SIMD2_ERR_CUDA;
+    total += ms;
+  }
+  if (kernel_ms) *kernel_ms = total;
+  if (launches) *launches = (long long)g_prof_used;
+  if (ops) *ops = g_prof_ops;
   return SIMD2_OK;
 }
 
