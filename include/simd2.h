@@ -128,6 +128,10 @@ long long simd2_launch_count(void);
 int simd2_profile_begin(void);
 int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops);
 
+/* Read and clear the id of the last bounded wait that ran out (0 = none);
+ * a diagnostic companion of simd2_device_status(). */
+int simd2_timeout_site(void);
+
 /* Read and clear the device-side error word that kernels set when a bounded
  * wait runs out (SIMD2_ERR_TIMEOUT).  Synchronizes the current device. */
 int simd2_device_status(void);

@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "prep.cuh"
 #include "srgemm_simt.cuh"
+#include "tc_gemm.cuh"
 
 namespace simd2 {
 namespace {
@@ -138,6 +139,20 @@ int make_map_f32(CUtensorMap* map, const void* base, long long rows, long long c
   return r == CUDA_SUCCESS ? SIMD2_OK : SIMD2_ERR_CUDA;
 }
 
+// Row-major matrix [rows][cols] of `esize`-byte elements, pitch in elements.
+int make_map_2d(CUtensorMap* map, CUtensorMapDataType dt, int esize, const void* base, long long rows,
+                long long cols, long long pitch, int box_cols, int box_rows, CUtensorMapSwizzle swz) {
+  auto fn = encode_fn();
+  if (!fn) return SIMD2_ERR_CUDA;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(pitch * esize)};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SIMD2_OK : SIMD2_ERR_CUDA;
+}
+
 inline int grid_for(long long items, int threads = 256) {
   long long b = (items + threads - 1) / threads;
   return (int)std::max(1LL, std::min(b, 148LL * 16));
@@ -254,6 +269,149 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   return dispatch_simt(op, M, N, K, mA, mB, ep, stream);
 }
 
+// ---------------------------------------------------------------------------
+// tensor-core paths
+// ---------------------------------------------------------------------------
+template <int KIND>
+int launch_tc(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
+              const CUtensorMap& b1, const TcEpilogue& ep, cudaStream_t stream) {
+  auto kern = tc_gemm_kernel<KIND>;
+  const size_t smem = tc_smem_bytes<KIND>();
+  static bool configured[64] = {};
+  int dev = 0;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
+  if (!configured[dev]) {
+    SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured[dev] = true;
+  }
+  const int tiles_m = (M + kTcBM - 1) / kTcBM;
+  const int tiles_n = (N + kTcBN - 1) / kTcBN;
+  auto* ev = prof_slot(2LL * M * N * K);
+  if (ev) cudaEventRecord(ev->first, stream);
+  kern<<<tiles_m * tiles_n, kTcThreads, smem, stream>>>(a0, a1, b0, b1, M, N, K, ep, tiles_m, tiles_n);
+  count_launch();
+  if (ev) cudaEventRecord(ev->second, stream);
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+struct TcPlan {
+  int Kp;
+  size_t a0, a1, b0, b1, na, nb, total;
+};
+
+// bf16 hi/lo operands (plus_mul, minus_square)
+TcPlan tc_plan_bf16(int M, int N, int K) {
+  TcPlan p{};
+  p.Kp = round_up(std::max(K, 1), 8);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
+  p.a0 = take((size_t)M * p.Kp * 2);
+  p.a1 = take((size_t)M * p.Kp * 2);
+  p.b0 = take((size_t)N * p.Kp * 2);
+  p.b1 = take((size_t)N * p.Kp * 2);
+  p.na = take((size_t)M * 4);
+  p.nb = take((size_t)N * 4);
+  p.total = off;
+  return p;
+}
+
+// 0/1 byte operands (or_and)
+TcPlan tc_plan_u8(int M, int N, int K) {
+  TcPlan p{};
+  p.Kp = round_up(std::max(K, 1), 16);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
+  p.a0 = take((size_t)M * p.Kp);
+  p.b0 = take((size_t)N * p.Kp);
+  p.a1 = p.a0;
+  p.b1 = p.b0;
+  p.na = p.nb = 0;
+  p.total = off;
+  return p;
+}
+
+// Band of the minus_square exact recompute: distances below 2^-6 of |a|^2+|b|^2.
+constexpr float kMinusSquareBand = 1.0f / 64.0f;
+
+int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb,
+                  const float* C, long long ldc, float* D, long long ldd, int do_epilogue, uint8_t* ws,
+                  const TcPlan& plan, cudaStream_t stream) {
+  const int Kp = plan.Kp;
+  auto* ahi = reinterpret_cast<__nv_bfloat16*>(ws + plan.a0);
+  auto* alo = reinterpret_cast<__nv_bfloat16*>(ws + plan.a1);
+  split_rows_bf16_kernel<<<grid_for((long long)M * Kp), 256, 0, stream>>>(A, lda, M, K, ahi, alo, Kp);
+  count_launch();
+  dim3 tgrid((N + 31) / 32, (Kp + 31) / 32), tblock(32, 8);
+  transpose_prep_kernel<float, 0><<<tgrid, tblock, 0, stream>>>(B, ldb, K, N, ws + plan.b0, ws + plan.b1, Kp);
+  count_launch();
+  float* na = reinterpret_cast<float*>(ws + plan.na);
+  float* nb = reinterpret_cast<float*>(ws + plan.nb);
+  if (op == SIMD2_MINUS_SQUARE) {
+    row_norms_kernel<<<grid_for((long long)M * 32), 256, 0, stream>>>(A, lda, M, K, na);
+    count_launch();
+    col_norms_kernel<<<grid_for(N), 256, 0, stream>>>(B, ldb, K, N, nb);
+    count_launch();
+  }
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  CUtensorMap ma0, ma1, mb0, mb1;
+  const auto BF = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  const auto SW = CU_TENSOR_MAP_SWIZZLE_128B;
+  int rc;
+  if ((rc = make_map_2d(&ma0, BF, 2, ahi, M, Kp, Kp, 64, kTcBM, SW))) return rc;
+  if ((rc = make_map_2d(&ma1, BF, 2, alo, M, Kp, Kp, 64, kTcBM, SW))) return rc;
+  if ((rc = make_map_2d(&mb0, BF, 2, ws + plan.b0, N, Kp, Kp, 64, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&mb1, BF, 2, ws + plan.b1, N, Kp, Kp, 64, kTcBN, SW))) return rc;
+  TcEpilogue ep{};
+  ep.op = op;
+  ep.do_epilogue = do_epilogue;
+  ep.C = do_epilogue ? (const void*)C : (const void*)D;
+  ep.ldc = do_epilogue ? ldc : ldd;
+  ep.D = D;
+  ep.ldd = ldd;
+  ep.norm_a = na;
+  ep.norm_b = nb;
+  ep.A32 = A;
+  ep.lda32 = lda;
+  ep.B32 = B;
+  ep.ldb32 = ldb;
+  ep.K = K;
+  ep.band = kMinusSquareBand;
+  return launch_tc<0>(M, N, K, ma0, ma1, mb0, mb1, ep, stream);
+}
+
+template <typename T>
+int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, long long ldb, const T* C,
+                    long long ldc, T* D, long long ldd, int do_epilogue, int* changed, uint8_t* ws,
+                    const TcPlan& plan, cudaStream_t stream) {
+  const int Kp = plan.Kp;
+  uint8_t* a8 = ws + plan.a0;
+  uint8_t* b8 = ws + plan.b0;
+  bool_rows_u8_kernel<T><<<grid_for((long long)M * Kp), 256, 0, stream>>>(A, lda, M, K, a8, Kp);
+  count_launch();
+  dim3 tgrid((N + 31) / 32, (Kp + 31) / 32), tblock(32, 8);
+  transpose_prep_kernel<T, 1><<<tgrid, tblock, 0, stream>>>(B, ldb, K, N, b8, nullptr, Kp);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  CUtensorMap ma, mb;
+  const auto U8 = CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  const auto SW = CU_TENSOR_MAP_SWIZZLE_128B;
+  int rc;
+  if ((rc = make_map_2d(&ma, U8, 1, a8, M, Kp, Kp, 128, kTcBM, SW))) return rc;
+  if ((rc = make_map_2d(&mb, U8, 1, b8, N, Kp, Kp, 128, kTcBN, SW))) return rc;
+  TcEpilogue ep{};
+  ep.op = SIMD2_OR_AND;
+  ep.do_epilogue = do_epilogue;
+  ep.C = do_epilogue ? (const void*)C : (const void*)D;
+  ep.ldc = do_epilogue ? ldc : ldd;
+  ep.D = D;
+  ep.ldd = ldd;
+  ep.out_u8 = sizeof(T) == 1;
+  ep.changed = changed;
+  return launch_tc<1>(M, N, K, ma, ma, mb, mb, ep, stream);
+}
+
 int check_dims(int M, int N, int K, long long lda, long long ldb, long long ldc, long long ldd, const void* A,
                const void* B, const void* C, const void* D, int do_epilogue) {
   if (M < 0 || N < 0 || K < 0) return SIMD2_ERR_INVALID_ARG;
@@ -296,6 +454,17 @@ int srgemm_f32_ws(int op, int M, int N, int K, const float* A, long long lda, co
                   const float* C, long long ldc, float* D, long long ldd, int do_epilogue, int* changed, int conv,
                   uint8_t* ws_or_null, cudaStream_t stream) {
   if (K == 0) return srgemm_k0(op, M, N, C, ldc, D, ldd, do_epilogue, stream);
+  if (is_sum_op(op)) {
+    const TcPlan tp = tc_plan_bf16(M, N, K);
+    uint8_t* ws = ws_or_null;
+    if (!ws) {
+      void* p = nullptr;
+      int rc = get_workspace(stream, tp.total, &p);
+      if (rc) return rc;
+      ws = static_cast<uint8_t*>(p);
+    }
+    return srgemm_tc_sum(op, M, N, K, A, lda, B, ldb, C, ldc, D, ldd, do_epilogue, ws, tp, stream);
+  }
   const bool pack_a = !a_tma_ok(A, lda);
   const Plan plan = make_plan(M, N, K, pack_a);
   uint8_t* ws = ws_or_null;
@@ -309,40 +478,30 @@ int srgemm_f32_ws(int op, int M, int N, int K, const float* A, long long lda, co
   return srgemm_core<float, 0>(op, M, N, K, A, lda, B, ldb, ep, ws, plan, pack_a, stream);
 }
 
-// or_and through the max_min kernel on {0,1}: AND of booleans is min, OR is
-// max, so the result (converted back to 0/1) is exact.
+// or_and on the INT8 tensor cores (0/1 bytes, S32 counts), exact.
 template <typename T>
 int srgemm_orand(int M, int N, int K, const T* A, long long lda, const T* B, long long ldb, const T* C, long long ldc,
                  T* D, long long ldd, int do_epilogue, cudaStream_t stream) {
   int rc = check_dims(M, N, K, lda, ldb, ldc, ldd, A, B, C, D, do_epilogue);
   if (rc || M == 0 || N == 0) return rc;
   if ((rc = check_device())) return rc;
-  const Plan plan = make_plan(M, N, K, true);
-  const size_t c_off = plan.total;
-  const size_t c_bytes = align_up((size_t)M * N * 4, kAlign);
-  const size_t d_off = c_off + c_bytes;
-  const size_t total = d_off + c_bytes;
-  void* p = nullptr;
-  if ((rc = get_workspace(stream, total, &p))) return rc;
-  uint8_t* ws = static_cast<uint8_t*>(p);
-  float* Cf = reinterpret_cast<float*>(ws + c_off);
-  float* Df = reinterpret_cast<float*>(ws + d_off);
-  if (do_epilogue) {
-    pack_rows_kernel<T, 1><<<grid_for((long long)M * N), 256, 0, stream>>>(C, ldc, M, N, Cf, N, 0.0f);
-    count_launch();
-    SIMD2_CUDA_TRY(cudaGetLastError());
-  }
   if (K == 0) {
-    rc = srgemm_k0(SIMD2_MAX_MIN, M, N, Cf, N, Df, N, do_epilogue, stream);
-  } else {
-    const EpilogueArgs ep = make_epilogue(Cf, N, Df, N, do_epilogue, nullptr, 0);
-    rc = srgemm_core<T, 1>(SIMD2_MAX_MIN, M, N, K, A, lda, B, ldb, ep, ws, plan, true, stream);
+    // D = 0 (+) C
+    if (do_epilogue) {
+      bool_copy_kernel<T><<<grid_for((long long)M * N), 256, 0, stream>>>(C, ldc, D, ldd, M, N);
+      count_launch();
+    } else {
+      fill_kernel<T><<<grid_for((long long)M * N), 256, 0, stream>>>(D, ldd, M, N, T(0));
+      count_launch();
+    }
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    return SIMD2_OK;
   }
-  if (rc) return rc;
-  bool_out_kernel<T><<<grid_for((long long)M * N), 256, 0, stream>>>(Df, N, D, ldd, M, N);
-  count_launch();
-  SIMD2_CUDA_TRY(cudaGetLastError());
-  return SIMD2_OK;
+  const TcPlan plan = tc_plan_u8(M, N, K);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, plan.total, &p))) return rc;
+  return srgemm_tc_orand<T>(M, N, K, A, lda, B, ldb, C, ldc, D, ldd, do_epilogue, nullptr,
+                            static_cast<uint8_t*>(p), plan, stream);
 }
 
 }  // namespace
@@ -455,19 +614,40 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
   if (n == 0 || max_iter == 0) return SIMD2_OK;
   int rc = check_device();
   if (rc) return rc;
-  // Boolean closure as max_min on a {0,1} float copy (exact), then back to bytes.
-  float* Xf = nullptr;
-  SIMD2_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&Xf), (size_t)n * n * 4, stream));
-  pack_rows_kernel<uint8_t, 1><<<grid_for((long long)n * n), 256, 0, stream>>>(X, ldx, n, n, Xf, n, 0.0f);
-  count_launch();
-  rc = closure_f32(SIMD2_MAX_MIN, n, Xf, n, max_iter, SIMD2_CONV_EXACT, iters_out, stream);
-  if (rc == SIMD2_OK || rc == SIMD2_ERR_NOT_CONVERGED) {
-    bool_out_kernel<uint8_t><<<grid_for((long long)n * n), 256, 0, stream>>>(Xf, n, X, ldx, n, n);
-    count_launch();
+  // Workspace: [tensor-core operands][Xnew n x n bytes][change flag]
+  const TcPlan plan = tc_plan_u8(n, n, n);
+  const size_t x_off = align_up(plan.total, kAlign);
+  const size_t f_off = x_off + align_up((size_t)n * n, kAlign);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, f_off + kAlign, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  uint8_t* Xn = ws + x_off;
+  int* flag = reinterpret_cast<int*>(ws + f_off);
+  uint8_t* cur = X;
+  long long ldcur = ldx;
+  uint8_t* nxt = Xn;
+  long long ldnxt = n;
+  int it = 0, changed = 1;
+  while (changed && it < max_iter) {
+    it++;
+    SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), stream));
+    rc = srgemm_tc_orand<uint8_t>(n, n, n, cur, ldcur, cur, ldcur, cur, ldcur, nxt, ldnxt, 1, flag, ws, plan, stream);
+    if (rc) return rc;
+    int h = 0;
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+    changed = h != 0;
+    std::swap(cur, nxt);
+    std::swap(ldcur, ldnxt);
   }
-  cudaFreeAsync(Xf, stream);
-  if (cudaStreamSynchronize(stream) != cudaSuccess) return SIMD2_ERR_CUDA;
-  return rc;
+  if (cur != X) {
+    SIMD2_CUDA_TRY(cudaMemcpy2DAsync(X, ldx, cur, ldcur, (size_t)n, n, cudaMemcpyDeviceToDevice, stream));
+  } else if (it == 0) {
+    // nothing ran
+  }
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (iters_out) *iters_out = it;
+  return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
 int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t stream, size_t* bytes_out) {
@@ -521,6 +701,14 @@ int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops) {
   if (launches) *launches = (long long)g_prof_used;
   if (ops) *ops = g_prof_ops;
   return SIMD2_OK;
+}
+
+int simd2_timeout_site(void) {
+  int h = 0, zero = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+  if (cudaMemcpyFromSymbol(&h, g_timeout_site, sizeof(int)) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(g_timeout_site, &zero, sizeof(int)) != cudaSuccess) return -1;
+  return h;
 }
 
 int simd2_device_status(void) {

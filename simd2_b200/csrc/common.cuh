@@ -16,6 +16,8 @@ namespace simd2 {
 // The library is one translation unit (capi.cu includes every kernel header),
 // so this is the single definition.
 __device__ int g_device_status = 0;
+// Largest wait-site id that timed out (0 = none); sites are numbered per kernel.
+__device__ int g_timeout_site = 0;
 
 // Wall-time limit of one bounded wait, in nanoseconds (2 s).
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
@@ -90,6 +92,10 @@ __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map) {
 }
 
 __device__ __forceinline__ void report_error(int code) { atomicOr(&g_device_status, code); }
+__device__ __forceinline__ void report_timeout(int site) {
+  atomicOr(&g_device_status, SIMD2_ERR_TIMEOUT);
+  atomicMax(&g_timeout_site, site);
+}
 
 // ---------------------------------------------------------------------------
 // Semiring operators.  The add step keeps host_srgemm's accumulator-first

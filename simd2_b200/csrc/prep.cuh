@@ -1,5 +1,7 @@
 // prep.cuh -- operand preparation kernels (HBM-bound, one pass each).
 #pragma once
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace simd2 {
@@ -59,6 +61,19 @@ __global__ void fill_kernel(T* D, long long ldd, int M, int N, T value) {
   }
 }
 
+// D = (C != 0) as 0/1 of type T.
+template <typename T>
+__global__ void bool_copy_kernel(const T* __restrict__ C, long long ldc, T* __restrict__ D, long long ldd, int M,
+                                 int N) {
+  const long long total = (long long)M * N;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / N);
+    const int j = (int)(t - (long long)i * N);
+    D[(long long)i * ldd + j] = C[(long long)i * ldc + j] != T(0) ? T(1) : T(0);
+  }
+}
+
 // float {-inf,0,1} -> 0/1 of type T (or_and result).
 template <typename T>
 __global__ void bool_out_kernel(const float* __restrict__ S, long long lds, T* __restrict__ D, long long ldd, int M,
@@ -69,6 +84,113 @@ __global__ void bool_out_kernel(const float* __restrict__ S, long long lds, T* _
     const int i = (int)(t / N);
     const int j = (int)(t - (long long)i * N);
     D[(long long)i * ldd + j] = S[(long long)i * lds + j] > 0.5f ? T(1) : T(0);
+  }
+}
+
+}  // namespace simd2
+
+namespace simd2 {
+
+// ---------------------------------------------------------------------------
+// Operand preparation for the tensor-core paths.  Outputs are K-major with a
+// row pitch of Kp elements (Kp a multiple of 8 for BF16, 16 for bytes, so the
+// TMA row stride is a multiple of 16 bytes); k in [K, Kp) is zero.
+// ---------------------------------------------------------------------------
+
+// x = hi + lo with hi = bf16(x), lo = bf16(x - hi) (both round-to-nearest).
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(__fsub_rn(x, __bfloat162float(hi)));
+}
+
+// A [M][K] (pitch lda) -> A_hi, A_lo [M][Kp].
+__global__ void split_rows_bf16_kernel(const float* __restrict__ A, long long lda, int M, int K,
+                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int Kp) {
+  const long long total = (long long)M * Kp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / Kp);
+    const int k = (int)(t - (long long)i * Kp);
+    __nv_bfloat16 h = __float2bfloat16_rn(0.f), l = h;
+    if (k < K) split_bf16(A[(long long)i * lda + k], h, l);
+    hi[t] = h;
+    lo[t] = l;
+  }
+}
+
+// A [M][K] of T -> bytes {0,1} [M][Kp].
+template <typename T>
+__global__ void bool_rows_u8_kernel(const T* __restrict__ A, long long lda, int M, int K, uint8_t* __restrict__ out,
+                                    int Kp) {
+  const long long total = (long long)M * Kp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / Kp);
+    const int k = (int)(t - (long long)i * Kp);
+    out[t] = (k < K && A[(long long)i * lda + k] != T(0)) ? 1 : 0;
+  }
+}
+
+// B [K][N] (pitch ldb) -> transposed K-major [N][Kp] through a 32 x 32 shared
+// tile (coalesced reads along n, coalesced writes along k).
+// MODE 0: BF16 hi/lo split (out0 = hi, out1 = lo); MODE 1: bytes {0,1} (out0).
+template <typename T, int MODE>
+__global__ void transpose_prep_kernel(const T* __restrict__ B, long long ldb, int K, int N, void* __restrict__ out0,
+                                      void* __restrict__ out1, int Kp) {
+  __shared__ float tile[32][33];
+  const int k0 = blockIdx.y * 32;
+  const int j0 = blockIdx.x * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int k = k0 + i, j = j0 + threadIdx.x;
+    float v = 0.f;
+    if (k < K && j < N) {
+      const T x = B[(long long)k * ldb + j];
+      if constexpr (MODE == 1) v = (x != T(0)) ? 1.f : 0.f;
+      else v = static_cast<float>(x);
+    }
+    tile[i][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int j = j0 + i, k = k0 + threadIdx.x;
+    if (j < N && k < Kp) {
+      const float v = tile[threadIdx.x][i];
+      const long long o = (long long)j * Kp + k;
+      if constexpr (MODE == 1) {
+        static_cast<uint8_t*>(out0)[o] = (uint8_t)(v != 0.f);
+      } else {
+        __nv_bfloat16 h, l;
+        split_bf16(v, h, l);
+        static_cast<__nv_bfloat16*>(out0)[o] = h;
+        static_cast<__nv_bfloat16*>(out1)[o] = l;
+      }
+    }
+  }
+}
+
+// Squared row norms of A [M][K], accumulated in FP64, rounded to float.
+__global__ void row_norms_kernel(const float* __restrict__ A, long long lda, int M, int K, float* __restrict__ out) {
+  const int warps = blockDim.x / 32;
+  for (int i = blockIdx.x * warps + threadIdx.x / 32; i < M; i += gridDim.x * warps) {
+    double s = 0.0;
+    for (int k = threadIdx.x % 32; k < K; k += 32) {
+      const double v = A[(long long)i * lda + k];
+      s += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x % 32 == 0) out[i] = (float)s;
+  }
+}
+
+// Squared column norms of B [K][N], accumulated in FP64, rounded to float.
+__global__ void col_norms_kernel(const float* __restrict__ B, long long ldb, int K, int N, float* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < K; k++) {
+      const double v = B[(long long)k * ldb + j];
+      s += v * v;
+    }
+    out[j] = (float)s;
   }
 }
 

@@ -3,17 +3,23 @@
 // Computes one BM x BN tile of D = id (+) A(x)B [(+) C] per CTA, the
 // row-major contract of mmo::host_srgemm (escalab/SIMD2 kernel/host_srgemm.h:17-49).
 //
-//   * 1 producer warp issues 2D TMA loads (no multicast) of an A tile
-//     [BM rows][BK k] (128-byte swizzle) and a B' tile into a STAGES-deep ring
-//     in shared memory, with full/empty mbarriers per stage.
+//   * Thread 0 issues 2D TMA loads (no multicast) of an A tile [BM rows][BK k]
+//     (128-byte swizzle) and a B' tile into a STAGES-deep ring in shared
+//     memory, with full/empty mbarriers per stage: the first STAGES tiles up
+//     front, then each refill one tile after its stage is released.  (A
+//     dedicated producer warp would put three warps on one SM sub-partition
+//     and cap every thread at 168 registers.)
 //   * B' is B with consecutive k rows interleaved in pairs,
 //     B'[p][2j+e] = B[2p+e][j], written once per call by interleave_pairs
 //     (prep.cu).  A thread then holds (A[i][2p], A[i][2p+1]) and
 //     (B[2p][j], B[2p+1][j]) as register pairs, forms both products with one
 //     packed f32x2 add/mul (each element rounded exactly like the scalar op),
 //     and folds both into the accumulator with one three-operand min/max.
-//   * 8 consumer warps each own a 16 x 128 slab; each thread holds an
-//     8 x 8 register tile (rows ty+16i, columns 32c+2tx+e).
+//   * 16 warps (4 per SM sub-partition); warp w owns rows {ty+16i} of the
+//     column half 64*(w/8); each thread holds an 8 x 4 register tile (rows
+//     ty+16i, columns 64*(w/8) + 32c + 2tx + e).  The tile is dispatch-bound:
+//     the packed add and the three-operand min each occupy a 16-lane pipe for
+//     two cycles per warp, i.e. one (x),(+) pair per lane per cycle.
 //   * The epilogue applies (+) C, writes D with coalesced 8-byte stores and,
 //     for the closure, sets one change flag per warp (warp vote + atomicOr).
 //
@@ -28,8 +34,8 @@ namespace simd2 {
 constexpr int kBM = 128;
 constexpr int kBN = 128;
 constexpr int kBK = 32;
-constexpr int kConsumerWarps = 8;
-constexpr int kSimtThreads = (kConsumerWarps + 1) * 32;
+constexpr int kSimtWarps = 16;
+constexpr int kSimtThreads = kSimtWarps * 32;
 constexpr int kATileBytes = kBM * kBK * 4;  // 16 KiB
 constexpr int kBTileBytes = kBK * kBN * 4;  // 16 KiB
 constexpr int kStageBytes = kATileBytes + kBTileBytes;
@@ -86,10 +92,11 @@ __device__ __forceinline__ bool conv_changed(int mode, float old_v, float new_v)
 }
 
 template <int OP>
-__device__ __forceinline__ float epilogue_value(const EpilogueArgs& ep, float v, float c, int& changed) {
-  if (ep.do_epilogue) v = Mac<OP>::add(v, c);
-  if (ep.conv_mode == SIMD2_CONV_APLP && v > -1.0f && v < 1.0f) v = -3.402823466e+38f;
-  if (ep.changed && conv_changed(ep.conv_mode, c, v)) changed = 1;
+__device__ __forceinline__ float epilogue_value(int do_epi, int conv_mode, bool track, float v, float c,
+                                                int& changed) {
+  if (do_epi) v = Mac<OP>::add(v, c);
+  if (conv_mode == SIMD2_CONV_APLP && v > -1.0f && v < 1.0f) v = -3.402823466e+38f;
+  if (track && conv_changed(conv_mode, c, v)) changed = 1;
   return v;
 }
 
@@ -121,53 +128,54 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kConsumerWarps);
+      mbar_init(&empty[s], kSimtWarps);
     }
     fence_mbar_init();
   }
   __syncthreads();
 
-  if (warp == kConsumerWarps) {
-    // ---------------- producer ----------------
-    if (lane == 0) {
-      prefetch_tensormap(&tmA);
-      prefetch_tensormap(&tmB);
-      int issued = 0;
-      for (int kt = 0; kt < ktiles; kt++) {
-        const int s = kt % STAGES;
-        const uint32_t round = kt / STAGES;
-        if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
-          report_error(SIMD2_ERR_TIMEOUT);
-          break;
-        }
-        uint8_t* sa = smem + s * kStageBytes;
-        mbar_arrive_expect_tx(&full[s], kStageBytes);
-        tma_load_2d(sa, &tmA, &full[s], kt * kBK, m0);
-        tma_load_2d(sa + kATileBytes, &tmB, &full[s], 2 * n0, kt * (kBK / 2));
-        issued = kt + 1;
-      }
-      // Every issued copy must land before this CTA's shared memory is released.
-      for (int kt = max(0, issued - STAGES); kt < issued; kt++) {
-        if (!mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1)) report_error(SIMD2_ERR_TIMEOUT);
-      }
+  // Thread 0 issues the first STAGES tiles; refills happen inside the k loop.
+  if (threadIdx.x == 0) {
+    prefetch_tensormap(&tmA);
+    prefetch_tensormap(&tmB);
+    for (int kt = 0; kt < min(STAGES, ktiles); kt++) {
+      uint8_t* sa = smem + kt * kStageBytes;
+      mbar_arrive_expect_tx(&full[kt], kStageBytes);
+      tma_load_2d(sa, &tmA, &full[kt], kt * kBK, m0);
+      tma_load_2d(sa + kATileBytes, &tmB, &full[kt], 2 * n0, kt * (kBK / 2));
     }
-    return;
   }
 
-  // ---------------- consumers ----------------
+  constexpr int WN = 2;  // column pairs per thread
   const int tx = lane & 15;
-  const int ty = warp * 2 + (lane >> 4);
+  const int ty = (warp & 7) * 2 + (lane >> 4);
+  const int cbase = (warp >> 3) * 64;
   const int swz = ty & 7;  // row & 7 for every row this thread reads (rows ty + 16 i)
 
-  float acc[8][8];
+  float acc[8][2 * WN];
 #pragma unroll
   for (int i = 0; i < 8; i++)
 #pragma unroll
-    for (int j = 0; j < 8; j++) acc[i][j] = Mac<OP>::identity();
+    for (int j = 0; j < 2 * WN; j++) acc[i][j] = Mac<OP>::identity();
 
   bool ok = true;
+  int issued = min(STAGES, ktiles);
   for (int kt = 0; kt < ktiles; kt++) {
     const int s = kt % STAGES;
+    // Refill the stage that tile kt-1 used once every warp has released it.
+    if (threadIdx.x == 0 && kt >= 1 && kt - 1 + STAGES < ktiles) {
+      const int r = kt - 1, rs = r % STAGES;
+      if (mbar_wait(&empty[rs], (r / STAGES) & 1)) {
+        uint8_t* sa = smem + rs * kStageBytes;
+        const int nk = r + STAGES;
+        mbar_arrive_expect_tx(&full[rs], kStageBytes);
+        tma_load_2d(sa, &tmA, &full[rs], nk * kBK, m0);
+        tma_load_2d(sa + kATileBytes, &tmB, &full[rs], 2 * n0, nk * (kBK / 2));
+        issued = nk + 1;
+      } else {
+        report_error(SIMD2_ERR_TIMEOUT);
+      }
+    }
     if (!mbar_wait(&full[s], (kt / STAGES) & 1)) {
       report_error(SIMD2_ERR_TIMEOUT);
       ok = false;
@@ -183,15 +191,15 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
         a[i] = *reinterpret_cast<const float4*>(As + (ty + 16 * i) * kBK + ((q ^ swz) << 2));
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        float4 b[4];
+        float4 b[WN];
 #pragma unroll
-        for (int c = 0; c < 4; c++)
-          b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (32 * c + 2 * tx) * 2);
+        for (int c = 0; c < WN; c++)
+          b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (cbase + 32 * c + 2 * tx) * 2);
 #pragma unroll
         for (int i = 0; i < 8; i++) {
           const float2 ap = h == 0 ? make_float2(a[i].x, a[i].y) : make_float2(a[i].z, a[i].w);
 #pragma unroll
-          for (int c = 0; c < 4; c++) {
+          for (int c = 0; c < WN; c++) {
             acc[i][2 * c] = Mac<OP>::mac2(acc[i][2 * c], ap, make_float2(b[c].x, b[c].y));
             acc[i][2 * c + 1] = Mac<OP>::mac2(acc[i][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
           }
@@ -201,39 +209,51 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
-  if (!ok) return;
+  if (!ok) {
+    // Every issued copy must land before this CTA's shared memory is released.
+    if (threadIdx.x == 0)
+      for (int kt = max(0, issued - STAGES); kt < issued; kt++) mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1);
+    return;
+  }
 
   // ---------------- epilogue ----------------
+  const int do_epi = ep.do_epilogue;
+  const int conv_mode = ep.conv_mode;
+  const bool track = ep.changed != nullptr;
+  const float* Cbase = ep.C;
+  float* Dbase = ep.D;
+  const long long ldc = ep.ldc, ldd = ep.ldd;
+  const int vec2 = ep.vec2;
   int changed = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
     const int row = m0 + ty + 16 * i;
     if (row < M) {
-      const float* crow = ep.C + (long long)row * ep.ldc;
-      float* drow = ep.D + (long long)row * ep.ldd;
+      const float* crow = Cbase + (long long)row * ldc;
+      float* drow = Dbase + (long long)row * ldd;
 #pragma unroll
-      for (int c = 0; c < 4; c++) {
-        const int col = n0 + 32 * c + 2 * tx;
-        if (ep.vec2 && col + 1 < N) {
+      for (int c = 0; c < WN; c++) {
+        const int col = n0 + cbase + 32 * c + 2 * tx;
+        if (vec2 && col + 1 < N) {
           float2 cv = make_float2(0.f, 0.f);
-          if (ep.do_epilogue) cv = *reinterpret_cast<const float2*>(crow + col);
+          if (do_epi) cv = *reinterpret_cast<const float2*>(crow + col);
           float2 v;
-          v.x = epilogue_value<OP>(ep, acc[i][2 * c], cv.x, changed);
-          v.y = epilogue_value<OP>(ep, acc[i][2 * c + 1], cv.y, changed);
+          v.x = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c], cv.x, changed);
+          v.y = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + 1], cv.y, changed);
           *reinterpret_cast<float2*>(drow + col) = v;
         } else {
 #pragma unroll
           for (int e = 0; e < 2; e++) {
             if (col + e < N) {
-              const float cv = ep.do_epilogue ? crow[col + e] : 0.0f;
-              drow[col + e] = epilogue_value<OP>(ep, acc[i][2 * c + e], cv, changed);
+              const float cv = do_epi ? crow[col + e] : 0.0f;
+              drow[col + e] = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + e], cv, changed);
             }
           }
         }
       }
     }
   }
-  if (ep.changed) {
+  if (track) {
     if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
   }
 }

@@ -1,0 +1,337 @@
+// tc_gemm.cuh -- tensor-core (tcgen05 / TMEM) srgemm paths for sm_100a.
+//
+// Used for the semirings that are dense contractions:
+//   * or_and       : kind::i8, unsigned 0/1 bytes, S32 counts; D = (count > 0) | C.
+//   * plus_mul     : kind::f16 with BF16 hi/lo operands, FP32 accumulate:
+//                    a*b ~= a_hi*b_hi + a_hi*b_lo + a_lo*b_hi  (three MMAs per k step).
+//   * minus_square : the same BF16 hi/lo product gives a.b; the epilogue forms
+//                    |a|^2 + |b|^2 - 2 a.b with FP64-accumulated norms and
+//                    recomputes sum_k (a-b)^2 exactly in FP32 inside the
+//                    cancellation band (small distance relative to the norms).
+//
+// One CTA computes a 128 x 256 tile of D with 4 warps:
+//   warp 0 lane 0  -- TMA producer (2D tiled loads, no multicast, 128-byte swizzle),
+//   warp 1 lane 0  -- MMA issuer (tcgen05.mma, cta_group::1, M=128 N=256),
+//   warps 0..3     -- epilogue: tcgen05.ld of the TMEM accumulator (warp w reads
+//                     TMEM lanes 32w..32w+31 = tile rows), fused (+) C, stores.
+// Both operands are K-major in shared memory: A is [M][K] as given, B is
+// stored transposed ([N][K]) by the operand-prep kernel.
+#pragma once
+#include "common.cuh"
+
+namespace simd2 {
+
+constexpr int kTcBM = 128;
+constexpr int kTcBN = 256;
+constexpr int kTcThreads = 128;
+constexpr int kTcRowBytes = 128;  // one 128-byte swizzle row of K per operand row
+
+template <int KIND>
+struct TcCfg;
+// BF16 hi/lo: BK = 64 elements, two A tiles and two B tiles per stage.
+template <>
+struct TcCfg<0> {
+  static constexpr int kBK = 64;
+  static constexpr int kNumA = 2;
+  static constexpr int kNumB = 2;
+  static constexpr int kStages = 2;
+  static constexpr int kKStep = 16;  // K per tcgen05.mma kind::f16
+  // c_format F32 (1), a/b format BF16 (1), K-major A and B, N=256, M=128
+  static constexpr uint32_t kIdesc =
+      (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcBN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
+};
+// INT8 0/1: BK = 128 elements, one A and one B tile per stage.
+template <>
+struct TcCfg<1> {
+  static constexpr int kBK = 128;
+  static constexpr int kNumA = 1;
+  static constexpr int kNumB = 1;
+  static constexpr int kStages = 4;
+  static constexpr int kKStep = 32;  // K per tcgen05.mma kind::i8
+  // c_format S32 (2), a/b format unsigned 8-bit (0), K-major, N=256, M=128
+  static constexpr uint32_t kIdesc = (2u << 4) | ((uint32_t)(kTcBN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
+};
+
+constexpr int kTcATile = kTcBM * kTcRowBytes;  // 16 KiB
+constexpr int kTcBTile = kTcBN * kTcRowBytes;  // 32 KiB
+
+template <int KIND>
+__host__ __device__ constexpr int tc_stage_bytes() {
+  return TcCfg<KIND>::kNumA * kTcATile + TcCfg<KIND>::kNumB * kTcBTile;
+}
+template <int KIND>
+constexpr size_t tc_smem_bytes() {
+  return (size_t)TcCfg<KIND>::kStages * tc_stage_bytes<KIND>() + 1024 + 256;
+}
+
+// Shared-memory matrix descriptor for a K-major operand tile written by TMA
+// with 128-byte swizzle: rows of 128 bytes, 8-row core-matrix groups 1024
+// bytes apart (stride byte offset), leading byte offset unused (1), version 1,
+// layout type 2 = SWIZZLE_128B.  Advancing K inside the 128-byte row moves the
+// start address by the byte offset.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;           // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024u >> 4) << 32; // stride byte offset
+  d |= (uint64_t)1u << 46;           // descriptor version (sm_100)
+  d |= (uint64_t)2u << 61;           // SWIZZLE_128B
+  return d;
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+template <int KIND>
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  if constexpr (KIND == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(TcCfg<0>::kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(TcCfg<1>::kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+  }
+}
+
+// Arrive on `bar` once every tcgen05 operation issued so far by this thread completes.
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit columns: thread t of the warp gets lane t.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Epilogue arguments of the tensor-core paths.
+struct TcEpilogue {
+  int op;               // SIMD2_PLUS_MUL, SIMD2_MINUS_SQUARE or SIMD2_OR_AND
+  int do_epilogue;
+  const void* C;        // float (sums) or int32 / uint8 (or_and)
+  long long ldc;
+  void* D;
+  long long ldd;
+  int out_u8;           // or_and: 1 = uint8 C/D, 0 = int32 C/D
+  // minus_square: row norms of A (M), column norms of B (N), and the FP32
+  // operands for the exact recompute inside the cancellation band.
+  const float* norm_a;
+  const float* norm_b;
+  const float* A32;
+  long long lda32;
+  const float* B32;
+  long long ldb32;
+  int K;
+  float band;           // recompute when dist < band * (|a|^2 + |b|^2)
+  int* changed;         // or_and closure: set to 1 when any D differs from C
+};
+
+__device__ __forceinline__ float exact_minus_square(const float* a, long long lda_unused, const float* B, long long ldb,
+                                                    int col, int K) {
+  (void)lda_unused;
+  float s = 0.f;
+  for (int k = 0; k < K; k++) {
+    const float d = __fsub_rn(a[k], B[(long long)k * ldb + col]);
+    s = __fmaf_rn(d, d, s);
+  }
+  return s;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1,
+                   const __grid_constant__ CUtensorMap tmB0, const __grid_constant__ CUtensorMap tmB1, int M, int N,
+                   int K, TcEpilogue ep, int tiles_m, int tiles_n) {
+  using Cfg = TcCfg<KIND>;
+  constexpr int S = Cfg::kStages;
+  constexpr int kStage = tc_stage_bytes<KIND>();
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * kStage);
+  uint64_t* empty = full + S;
+  uint64_t* done = empty + S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+
+  // Grouped raster over (tile_m, tile_n): 8 tile rows per group.
+  const int group = 8;
+  const int per_group = group * tiles_n;
+  const int g = blockIdx.x / per_group;
+  const int first_m = g * group;
+  const int gsize = min(tiles_m - first_m, group);
+  const int local = blockIdx.x - g * per_group;
+  const int m0 = (first_m + local % gsize) * kTcBM;
+  const int n0 = (local / gsize) * kTcBN;
+  const int ktiles = (K + Cfg::kBK - 1) / Cfg::kBK;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    // 256 TMEM columns: the 128 x 256 FP32/S32 accumulator.
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  bool ok = true;
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    prefetch_tensormap(&tmA0);
+    prefetch_tensormap(&tmB0);
+    for (int kt = 0; kt < ktiles; kt++) {
+      const int s = kt % S;
+      if (!mbar_wait(&empty[s], ((kt / S) & 1) ^ 1)) {
+        report_timeout(101);
+        ok = false;
+        break;
+      }
+      uint8_t* st = smem + s * kStage;
+      mbar_arrive_expect_tx(&full[s], kStage);
+      const int kx = kt * Cfg::kBK;
+      tma_load_2d(st, &tmA0, &full[s], kx, m0);
+      if constexpr (Cfg::kNumA == 2) tma_load_2d(st + kTcATile, &tmA1, &full[s], kx, m0);
+      uint8_t* sb = st + Cfg::kNumA * kTcATile;
+      tma_load_2d(sb, &tmB0, &full[s], kx, n0);
+      if constexpr (Cfg::kNumB == 2) tma_load_2d(sb + kTcBTile, &tmB1, &full[s], kx, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    for (int kt = 0; kt < ktiles; kt++) {
+      const int s = kt % S;
+      if (!mbar_wait(&full[s], (kt / S) & 1)) {
+        report_timeout(102);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t st = smem_u32(smem + s * kStage);
+      const uint32_t a0 = st, a1 = st + kTcATile;
+      const uint32_t b0 = st + Cfg::kNumA * kTcATile, b1 = b0 + kTcBTile;
+#pragma unroll
+      for (int ks = 0; ks < Cfg::kBK / Cfg::kKStep; ks++) {
+        const uint32_t koff = ks * Cfg::kKStep * (KIND == 0 ? 2 : 1);  // bytes along the 128-byte row
+        const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
+        if constexpr (KIND == 0) {
+          // hi*hi, hi*lo, lo*hi
+          tc_mma<0>(tmem, umma_desc_sw128(a0 + koff), umma_desc_sw128(b0 + koff), acc0);
+          tc_mma<0>(tmem, umma_desc_sw128(a0 + koff), umma_desc_sw128(b1 + koff), 1u);
+          tc_mma<0>(tmem, umma_desc_sw128(a1 + koff), umma_desc_sw128(b0 + koff), 1u);
+        } else {
+          tc_mma<1>(tmem, umma_desc_sw128(a0 + koff), umma_desc_sw128(b0 + koff), acc0);
+        }
+      }
+      tc_commit(&empty[s]);  // stage s is free once these MMAs have read it
+    }
+    tc_commit(done);  // accumulator complete
+  }
+  __syncwarp();
+
+  // ---------------- epilogue (all 4 warps) ----------------
+  if (!mbar_wait(done, 0)) {
+    report_timeout(103);
+    ok = false;
+  }
+  tc_fence_after();
+  ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld below is warp-collective
+  const int row = m0 + warp * 32 + lane;
+  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+  int changed = 0;
+  if (ok) {
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+      uint32_t r[32];
+      tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
+      if (row >= M) continue;
+      const int colb = n0 + c0;
+      if constexpr (KIND == 1) {
+        if (ep.out_u8) {
+          const uint8_t* crow = static_cast<const uint8_t*>(ep.C) + (long long)row * ep.ldc;
+          uint8_t* drow = static_cast<uint8_t*>(ep.D) + (long long)row * ep.ldd;
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int col = colb + j;
+            if (col < N) {
+              uint8_t v = r[j] != 0u;
+              if (ep.do_epilogue) {
+                const uint8_t cv = crow[col] != 0;
+                v |= cv;
+                if (ep.changed && v != cv) changed = 1;
+              }
+              drow[col] = v;
+            }
+          }
+        } else {
+          const int32_t* crow = static_cast<const int32_t*>(ep.C) + (long long)row * ep.ldc;
+          int32_t* drow = static_cast<int32_t*>(ep.D) + (long long)row * ep.ldd;
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int col = colb + j;
+            if (col < N) {
+              int32_t v = r[j] != 0u;
+              if (ep.do_epilogue) v |= (crow[col] != 0);
+              drow[col] = v;
+            }
+          }
+        }
+      } else {
+        const float* crow = static_cast<const float*>(ep.C) + (long long)row * ep.ldc;
+        float* drow = static_cast<float*>(ep.D) + (long long)row * ep.ldd;
+        const float na = ep.op == SIMD2_MINUS_SQUARE ? ep.norm_a[row] : 0.f;
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const int col = colb + j;
+          if (col < N) {
+            float v = __uint_as_float(r[j]);
+            if (ep.op == SIMD2_MINUS_SQUARE) {
+              const float nb = ep.norm_b[col];
+              const float nsum = na + nb;
+              v = __fmaf_rn(-2.0f, v, nsum);
+              if (v < ep.band * nsum)
+                v = exact_minus_square(ep.A32 + (long long)row * ep.lda32, ep.lda32, ep.B32, ep.ldb32, col, ep.K);
+            }
+            if (ep.do_epilogue) v = __fadd_rn(v, crow[col]);
+            drow[col] = v;
+          }
+        }
+      }
+    }
+  }
+  if (ep.changed && KIND == 1) {
+    if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+  }
+}
+
+}  // namespace simd2
