@@ -52,7 +52,8 @@ typedef enum simd2_status {
   SIMD2_ERR_ALLOC = 4,         /* workspace allocation failed */
   SIMD2_ERR_TIMEOUT = 5,       /* a bounded device-side wait ran out */
   SIMD2_ERR_NOT_CONVERGED = 6, /* closure hit max_iter while still changing */
-  SIMD2_ERR_NO_DEVICE = 7      /* no sm_100 device visible */
+  SIMD2_ERR_NO_DEVICE = 7,     /* no sm_100 device visible */
+  SIMD2_ERR_SCRATCH_LIMIT = 8  /* problem needs more than SIMD2_NOALLOC_SCRATCH_BYTES */
 } simd2_status;
 
 /* Convergence test used by the closure entry points. */
@@ -135,6 +136,36 @@ int simd2_timeout_site(void);
 /* Read and clear the device-side error word that kernels set when a bounded
  * wait runs out (SIMD2_ERR_TIMEOUT).  Synchronizes the current device. */
 int simd2_device_status(void);
+
+/* Size of the fixed device scratch used by simd2_srgemm_noalloc (16 MiB).
+ * Every GPU that loads libsimd2 holds this much device memory until exit. */
+#define SIMD2_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* simd2_srgemm for the six min/max semirings (min_plus, max_plus, max_min,
+ * max_mul, min_mul, min_max) that allocates nothing.  No counterpart in the
+ * reference: it is for callers that must not call cudaMalloc -- code running
+ * under a caller-owned memory pool or allocator that forbids side
+ * allocations, real-time loops where an allocation may block, and processes
+ * that have already placed all device memory.  Same arguments and results
+ * as simd2_srgemm.
+ *
+ * Its working copy of B (k-pair interleaved, padded) and, when A's rows are
+ * not 16-byte aligned, a packed copy of A live in one file-scope device
+ * array of SIMD2_NOALLOC_SCRATCH_BYTES, so roundup(K,32) * roundup(N,128) * 4
+ * bytes (+ M * roundup(K,32) * 4 when A is repacked) must fit in it;
+ * larger problems return SIMD2_ERR_SCRATCH_LIMIT.  The other five semirings
+ * return SIMD2_ERR_UNSUPPORTED.
+ *
+ * The first call on each device looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current; make that first call before
+ * any stream capture.  Every call, on every stream, shares the one array and
+ * each call overwrites the part it uses completely before reading it (nothing
+ * has to start at zero), so calls whose kernels can overlap on the GPU race
+ * with each other: order them on one stream or synchronize between them. */
+int simd2_srgemm_noalloc(simd2_op op, int M, int N, int K,
+                         const float* A, int lda, const float* B, int ldb,
+                         const float* C, int ldc, float* D, int ldd,
+                         int do_epilogue, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

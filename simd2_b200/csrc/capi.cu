@@ -577,6 +577,7 @@ const char* simd2_status_string(int status) {
     case SIMD2_ERR_TIMEOUT: return "device-side wait timed out";
     case SIMD2_ERR_NOT_CONVERGED: return "closure did not converge within max_iter";
     case SIMD2_ERR_NO_DEVICE: return "no sm_100 device";
+    case SIMD2_ERR_SCRATCH_LIMIT: return "problem exceeds the fixed no-allocation scratch";
     default: return "unknown status";
   }
 }
@@ -720,3 +721,66 @@ int simd2_device_status(void) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// srgemm without allocation
+//
+// Some callers cannot call cudaMalloc: code that runs inside a caller-owned
+// memory pool or allocator that forbids side allocations, latency-critical
+// loops where an allocation may block or synchronize the device, and
+// processes that have already handed out all device memory.  For them the
+// min/max srgemm keeps its scratch (the interleaved copy of B, and a packed
+// copy of A when A is not TMA-aligned) in this fixed device array instead of
+// the per-stream workspace.  The array is part of the module image, so every
+// GPU that loads the library holds SIMD2_NOALLOC_SCRATCH_BYTES until exit.
+// ---------------------------------------------------------------------------
+namespace simd2 {
+namespace {
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[SIMD2_NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device.  In host code the symbol
+// name is only a host-side stand-in; the address a kernel may use comes from
+// cudaGetSymbolAddress, looked up once per device with that device current.
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+int noalloc_scratch(uint8_t** out) {
+  int dev = 0;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return SIMD2_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<uint8_t*>(g_noalloc_addr[dev]);
+  return SIMD2_OK;
+}
+
+}  // namespace
+}  // namespace simd2
+
+extern "C" int simd2_srgemm_noalloc(simd2_op op, int M, int N, int K, const float* A, int lda, const float* B,
+                                    int ldb, const float* C, int ldc, float* D, int ldd, int do_epilogue,
+                                    cudaStream_t stream) {
+  using namespace simd2;
+  if (!is_float_op(op)) return op == SIMD2_OR_AND ? SIMD2_ERR_UNSUPPORTED : SIMD2_ERR_INVALID_ARG;
+  if (is_sum_op(op)) return SIMD2_ERR_UNSUPPORTED;
+  int rc = check_dims(M, N, K, lda, ldb, ldc, ldd, A, B, C, D, do_epilogue);
+  if (rc || M == 0 || N == 0) return rc;
+  if ((rc = check_device())) return rc;
+  if (K == 0) return srgemm_k0(op, M, N, C, ldc, D, ldd, do_epilogue, stream);
+  const bool pack_a = !a_tma_ok(A, lda);
+  const Plan plan = make_plan(M, N, K, pack_a);
+  if (plan.total > (size_t)SIMD2_NOALLOC_SCRATCH_BYTES) return SIMD2_ERR_SCRATCH_LIMIT;
+  uint8_t* ws = nullptr;
+  if ((rc = noalloc_scratch(&ws))) return rc;
+  // Every byte of the plan is written by the prep kernels before the main
+  // kernel reads it, so the scratch needs no clearing between calls.
+  return srgemm_f32_ws(op, M, N, K, A, lda, B, ldb, C, ldc, D, ldd, do_epilogue, nullptr, 0, ws, stream);
+}
