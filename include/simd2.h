@@ -110,6 +110,28 @@ int simd2_closure(simd2_op op, int n, float* X, int ldx, int max_iter,
 int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter,
                            int* iters_out, cudaStream_t stream);
 
+/* Batched closure: `count` independent n[g] x n[g] matrices X[g] (device
+ * pointers, row pitch ldx[g]) closed in place in ONE persistent kernel launch,
+ * each graph by one CTA until its own fixed point (per-graph convergence,
+ * bit-exact per graph, same iteration counts as simd2_closure).  Six min/max
+ * semirings.  X, n and ldx are host arrays.
+ *   plan_create  allocates the plan's device memory and uploads descriptors
+ *                (synchronous);
+ *   plan_run     launches prep + persistent closure + copy-back on `stream`
+ *                and nothing else (no allocation, no host sync), so it can be
+ *                captured in a CUDA graph and replayed;
+ *   plan_iters   reads the per-graph step counts (synchronous);
+ *   closure_batched = create + run + iters + destroy, synchronous; returns
+ *                SIMD2_ERR_NOT_CONVERGED if any graph hit max_iter. */
+typedef struct simd2_batched_plan_st* simd2_batched_plan;
+int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int* n, const int* ldx, int max_iter,
+                              simd2_conv conv, simd2_batched_plan* plan_out);
+int simd2_batched_plan_run(simd2_batched_plan plan, cudaStream_t stream);
+int simd2_batched_plan_iters(simd2_batched_plan plan, int* iters_out, int* not_converged_out);
+int simd2_batched_plan_destroy(simd2_batched_plan plan);
+int simd2_closure_batched(simd2_op op, int count, float* const* X, const int* n, const int* ldx, int max_iter,
+                          simd2_conv conv, int* iters_out, cudaStream_t stream);
+
 /* Reserve the per-(device, stream) workspace for srgemm calls up to
  * M x N x K so that later calls (e.g. inside stream capture) allocate
  * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */

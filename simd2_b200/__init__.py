@@ -62,6 +62,12 @@ def lib() -> ctypes.CDLL:
         L.simd2_status_string.argtypes = [I]
         L.simd2_status_string.restype = ctypes.c_char_p
         L.simd2_version.restype = ctypes.c_char_p
+        PI = ctypes.POINTER(I)
+        L.simd2_batched_plan_create.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, ctypes.POINTER(P)]
+        L.simd2_batched_plan_run.argtypes = [P, P]
+        L.simd2_batched_plan_iters.argtypes = [P, PI, PI]
+        L.simd2_batched_plan_destroy.argtypes = [P]
+        L.simd2_closure_batched.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, PI, P]
         L.simd2_launch_count.argtypes = []
         L.simd2_launch_count.restype = ctypes.c_longlong
         L.simd2_profile_begin.argtypes = []
@@ -69,7 +75,9 @@ def lib() -> ctypes.CDLL:
                                         ctypes.POINTER(ctypes.c_longlong)]
         for name in ("simd2_srgemm", "simd2_srgemm_orand_i32", "simd2_srgemm_orand_u8", "simd2_closure",
                      "simd2_closure_orand_u8", "simd2_reserve_workspace", "simd2_release_workspaces",
-                     "simd2_device_status", "simd2_profile_begin", "simd2_profile_end"):
+                     "simd2_device_status", "simd2_profile_begin", "simd2_profile_end",
+                     "simd2_batched_plan_create", "simd2_batched_plan_run", "simd2_batched_plan_iters",
+                     "simd2_batched_plan_destroy", "simd2_closure_batched"):
             getattr(L, name).restype = I
         _lib = L
     return _lib
@@ -157,6 +165,62 @@ def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", 
         return it.value
     _check(rc, f"closure({op})")
     return it.value
+
+
+class BatchedClosure:
+    """Plan for closing many independent square matrices in one persistent launch.
+
+    ``mats`` are float32 CUDA tensors (n x n, row-major) closed in place by
+    ``run``.  ``run`` only launches kernels on the stream (no allocation, no
+    host synchronisation), so it can be captured in a CUDA graph.
+    """
+
+    def __init__(self, op: str, mats, max_iter: int = 500, conv: str = "exact"):
+        self.mats = list(mats)
+        count = len(self.mats)
+        ptrs = (ctypes.c_void_p * max(count, 1))(*[m.data_ptr() for m in self.mats])
+        ns = (ctypes.c_int * max(count, 1))(*[m.shape[0] for m in self.mats])
+        lds = (ctypes.c_int * max(count, 1))(*[_mat(m, "X") for m in self.mats])
+        for m in self.mats:
+            if m.dtype != torch.float32 or m.shape[0] != m.shape[1]:
+                raise ValueError("batched closure takes square float32 matrices")
+        self.count = count
+        self._plan = ctypes.c_void_p()
+        _check(lib().simd2_batched_plan_create(OP_ID[op], count, ptrs, ns, lds, max_iter, CONV[conv],
+                                               ctypes.byref(self._plan)), "batched_plan_create")
+
+    def run(self, stream=None):
+        _check(lib().simd2_batched_plan_run(self._plan, _stream(stream)), "batched_plan_run")
+
+    def iters(self):
+        it = (ctypes.c_int * max(self.count, 1))()
+        nc = ctypes.c_int(0)
+        _check(lib().simd2_batched_plan_iters(self._plan, it, ctypes.byref(nc)), "batched_plan_iters")
+        return list(it)[: self.count], nc.value
+
+    def close(self):
+        if self._plan:
+            lib().simd2_batched_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def closure_batched(op: str, mats, max_iter: int = 500, conv: str = "exact", stream=None):
+    """Closes every matrix of ``mats`` in place in one persistent launch; returns the step counts."""
+    mats = list(mats)
+    count = len(mats)
+    ptrs = (ctypes.c_void_p * max(count, 1))(*[m.data_ptr() for m in mats])
+    ns = (ctypes.c_int * max(count, 1))(*[m.shape[0] for m in mats])
+    lds = (ctypes.c_int * max(count, 1))(*[_mat(m, "X") for m in mats])
+    it = (ctypes.c_int * max(count, 1))()
+    rc = lib().simd2_closure_batched(OP_ID[op], count, ptrs, ns, lds, max_iter, CONV[conv], it, _stream(stream))
+    _check(rc, f"closure_batched({op})")
+    return list(it)[:count]
 
 
 def device_status() -> int:

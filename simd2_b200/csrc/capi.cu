@@ -17,6 +17,7 @@
 #include "prep.cuh"
 #include "srgemm_simt.cuh"
 #include "tc_gemm.cuh"
+#include "closure_batched.cuh"
 
 namespace simd2 {
 namespace {
@@ -560,6 +561,64 @@ int closure_f32(int op, int n, float* X, long long ldx, int max_iter, int conv, 
   return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// batched closure
+// ---------------------------------------------------------------------------
+struct BatchedPlan {
+  int dev;
+  int op;
+  int count;
+  int max_iter;
+  int conv;
+  void* mem;            // one device allocation: descriptors, order, queue, buffers
+  BatchGraph* d_graphs;
+  int* d_order;
+  int* d_queue;
+  std::vector<BatchGraph> host;
+};
+
+template <int OP>
+int launch_batched(BatchedPlan* p, cudaStream_t stream) {
+  auto kern = closure_batched_kernel<OP>;
+  const size_t smem = simt_smem_bytes(4);
+  static bool configured[64] = {};
+  if (!configured[p->dev]) {
+    SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured[p->dev] = true;
+  }
+  int sms = 0;
+  SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->dev));
+  const int grid = std::max(1, std::min(sms, p->count));
+  kern<<<grid, kSimtThreads, smem, stream>>>(p->d_graphs, p->d_order, p->count, p->d_queue, p->max_iter, p->conv);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+int batched_run(BatchedPlan* p, cudaStream_t stream) {
+  SIMD2_CUDA_TRY(cudaMemsetAsync(p->d_queue, 0, sizeof(int), stream));
+  dim3 pg(64, std::min(p->count, 65535));
+  batched_prep_kernel<<<pg, 256, 0, stream>>>(p->d_graphs, p->count);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  int rc;
+  switch (p->op) {
+    case SIMD2_MIN_PLUS: rc = launch_batched<SIMD2_MIN_PLUS>(p, stream); break;
+    case SIMD2_MAX_PLUS: rc = launch_batched<SIMD2_MAX_PLUS>(p, stream); break;
+    case SIMD2_MAX_MIN: rc = launch_batched<SIMD2_MAX_MIN>(p, stream); break;
+    case SIMD2_MAX_MUL: rc = launch_batched<SIMD2_MAX_MUL>(p, stream); break;
+    case SIMD2_MIN_MUL: rc = launch_batched<SIMD2_MIN_MUL>(p, stream); break;
+    case SIMD2_MIN_MAX: rc = launch_batched<SIMD2_MIN_MAX>(p, stream); break;
+    default: return SIMD2_ERR_UNSUPPORTED;
+  }
+  if (rc) return rc;
+  batched_finish_kernel<<<pg, 256, 0, stream>>>(p->d_graphs, p->count);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
 }  // namespace
 }  // namespace simd2
 
@@ -718,6 +777,133 @@ int simd2_device_status(void) {
   if (cudaMemcpyFromSymbol(&h, g_device_status, sizeof(int)) != cudaSuccess) return SIMD2_ERR_CUDA;
   if (cudaMemcpyToSymbol(g_device_status, &zero, sizeof(int)) != cudaSuccess) return SIMD2_ERR_CUDA;
   return h;
+}
+
+}  // extern "C"
+
+
+extern "C" {
+
+int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int* n, const int* ldx, int max_iter,
+                              simd2_conv conv, simd2_batched_plan* out) {
+  if (!out) return SIMD2_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (count < 0 || max_iter < 0 || (count > 0 && (!X || !n || !ldx))) return SIMD2_ERR_INVALID_ARG;
+  if (conv < SIMD2_CONV_EXACT || conv > SIMD2_CONV_APLP) return SIMD2_ERR_INVALID_ARG;
+  if (!is_float_op(op)) return op == SIMD2_OR_AND ? SIMD2_ERR_UNSUPPORTED : SIMD2_ERR_INVALID_ARG;
+  if (is_sum_op(op)) return SIMD2_ERR_UNSUPPORTED;
+  for (int g = 0; g < count; g++)
+    if (n[g] < 0 || (n[g] > 0 && (!X[g] || ldx[g] < n[g]))) return SIMD2_ERR_INVALID_ARG;
+  int rc = check_device();
+  if (rc) return rc;
+  auto* p = new BatchedPlan();
+  SIMD2_CUDA_TRY(cudaGetDevice(&p->dev));
+  p->op = op;
+  p->count = count;
+  p->max_iter = max_iter;
+  p->conv = conv;
+  p->host.resize(count);
+  // layout: [graphs][order][queue] then per-graph buffers
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
+  const size_t g_off = take(sizeof(BatchGraph) * std::max(count, 1));
+  const size_t o_off = take(sizeof(int) * std::max(count, 1));
+  const size_t q_off = take(sizeof(int));
+  std::vector<size_t> buf_off(count);
+  for (int g = 0; g < count; g++) {
+    BatchGraph& G = p->host[g];
+    G.n = n[g];
+    G.Mp = round_up(std::max(n[g], 1), kBM);
+    G.Kp = round_up(std::max(n[g], 1), kBK);
+    G.Np = round_up(std::max(n[g], 1), kBN);
+    G.user = X[g];
+    G.ldu = ldx[g];
+    const size_t xb = (size_t)G.Mp * G.Kp * 4, pb = (size_t)(G.Kp / 2) * 2 * G.Np * 4;
+    buf_off[g] = take(2 * xb + 2 * pb);
+  }
+  void* mem = nullptr;
+  if (cudaMalloc(&mem, std::max(off, (size_t)kAlign)) != cudaSuccess) {
+    cudaGetLastError();
+    delete p;
+    return SIMD2_ERR_ALLOC;
+  }
+  p->mem = mem;
+  uint8_t* base = static_cast<uint8_t*>(mem);
+  p->d_graphs = reinterpret_cast<BatchGraph*>(base + g_off);
+  p->d_order = reinterpret_cast<int*>(base + o_off);
+  p->d_queue = reinterpret_cast<int*>(base + q_off);
+  for (int g = 0; g < count; g++) {
+    BatchGraph& G = p->host[g];
+    const size_t xb = (size_t)G.Mp * G.Kp * 4, pb = (size_t)(G.Kp / 2) * 2 * G.Np * 4;
+    uint8_t* b = base + buf_off[g];
+    G.X[0] = reinterpret_cast<float*>(b);
+    G.X[1] = reinterpret_cast<float*>(b + xb);
+    G.P[0] = reinterpret_cast<float*>(b + 2 * xb);
+    G.P[1] = reinterpret_cast<float*>(b + 2 * xb + pb);
+    G.iters = 0;
+    G.changed = 0;
+  }
+  // longest-processing-time order: largest graphs first
+  std::vector<int> order(count);
+  for (int g = 0; g < count; g++) order[g] = g;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+  if (count > 0) {
+    if (cudaMemcpy(p->d_graphs, p->host.data(), sizeof(BatchGraph) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_order, order.data(), sizeof(int) * count, cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(mem);
+      delete p;
+      return SIMD2_ERR_CUDA;
+    }
+  }
+  *out = reinterpret_cast<simd2_batched_plan>(p);
+  return SIMD2_OK;
+}
+
+int simd2_batched_plan_run(simd2_batched_plan plan, cudaStream_t stream) {
+  auto* p = reinterpret_cast<BatchedPlan*>(plan);
+  if (!p) return SIMD2_ERR_INVALID_ARG;
+  if (p->count == 0 || p->max_iter == 0) return SIMD2_OK;
+  return batched_run(p, stream);
+}
+
+int simd2_batched_plan_iters(simd2_batched_plan plan, int* iters_out, int* not_converged_out) {
+  auto* p = reinterpret_cast<BatchedPlan*>(plan);
+  if (!p) return SIMD2_ERR_INVALID_ARG;
+  if (p->count == 0) {
+    if (not_converged_out) *not_converged_out = 0;
+    return SIMD2_OK;
+  }
+  std::vector<BatchGraph> h(p->count);
+  SIMD2_CUDA_TRY(cudaMemcpy(h.data(), p->d_graphs, sizeof(BatchGraph) * p->count, cudaMemcpyDeviceToHost));
+  int nc = 0;
+  for (int g = 0; g < p->count; g++) {
+    if (iters_out) iters_out[g] = h[g].iters;
+    nc += h[g].changed != 0;
+  }
+  if (not_converged_out) *not_converged_out = nc;
+  return SIMD2_OK;
+}
+
+int simd2_batched_plan_destroy(simd2_batched_plan plan) {
+  auto* p = reinterpret_cast<BatchedPlan*>(plan);
+  if (!p) return SIMD2_OK;
+  cudaFree(p->mem);
+  delete p;
+  return SIMD2_OK;
+}
+
+int simd2_closure_batched(simd2_op op, int count, float* const* X, const int* n, const int* ldx, int max_iter,
+                          simd2_conv conv, int* iters_out, cudaStream_t stream) {
+  simd2_batched_plan plan = nullptr;
+  int rc = simd2_batched_plan_create(op, count, X, n, ldx, max_iter, conv, &plan);
+  if (rc) return rc;
+  rc = simd2_batched_plan_run(plan, stream);
+  if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) rc = SIMD2_ERR_CUDA;
+  int nc = 0;
+  if (!rc) rc = simd2_batched_plan_iters(plan, iters_out, &nc);
+  simd2_batched_plan_destroy(plan);
+  if (!rc && nc > 0) rc = SIMD2_ERR_NOT_CONVERGED;
+  return rc;
 }
 
 }  // extern "C"
