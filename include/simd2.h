@@ -132,6 +132,47 @@ int simd2_batched_plan_destroy(simd2_batched_plan plan);
 int simd2_closure_batched(simd2_op op, int count, float* const* X, const int* n, const int* ldx, int max_iter,
                           simd2_conv conv, int* iters_out, cudaStream_t stream);
 
+/* Kernel configurations of the CUDA-core path (min/max semirings):
+ * config = s | (skip << 2), split-K factor 1 << s (s in 0..3) over a
+ * thread-block cluster whose CTAs fold their partial tiles through
+ * distributed shared memory, and skip = 1 to drop k-blocks whose A or B block
+ * holds only the (x)-annihilator (block occupancy computed per call; applies
+ * to min_plus, max_plus, max_min, min_max).  All configurations give the same
+ * bits.  No reference counterpart: the autotuner and the learned dispatch
+ * use it. */
+int simd2_srgemm_tuned(simd2_op op, int M, int N, int K,
+                       const float* A, int lda, const float* B, int ldb,
+                       const float* C, int ldc, float* D, int ldd,
+                       int do_epilogue, int config, cudaStream_t stream);
+
+typedef enum simd2_dispatch {
+  SIMD2_DISPATCH_DENSE = 0,   /* split 1, no skip: the plain dense path */
+  SIMD2_DISPATCH_FIXED = 1,   /* `fixed_config` every step */
+  SIMD2_DISPATCH_LEARNED = 2  /* the MLP cost model picks each step's config */
+} simd2_dispatch;
+
+/* simd2_closure with a dispatch policy.  mlp_params: device array of
+ * simd2_mlp_param_count() floats (LEARNED only).  Optional host outputs of
+ * max_iter entries: step_configs (config run per step), step_ms (device time
+ * of each step), step_features (7 floats per step: the cost-model features).
+ * Results are bit-identical for every policy. */
+int simd2_closure_ex(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_conv conv,
+                     simd2_dispatch dispatch, int fixed_config, const float* mlp_params,
+                     int* iters_out, int* step_configs, float* step_ms, float* step_features,
+                     cudaStream_t stream);
+
+/* Cost-model MLP (12-32-32-1, ReLU) kernels.  X: [batch][12] features+config,
+ * y: [batch] targets (log2 ms).  simd2_mlp_gradient writes d/dparams of
+ * mean((f(X)-y)^2) to grad (param_count floats) using sample_grads
+ * ([batch][param_count] floats) as scratch; the batch sum is deterministic.
+ * simd2_mlp_adam applies one Adam step (beta 0.9/0.999, eps 1e-8), step >= 1. */
+int simd2_mlp_param_count(void);
+int simd2_mlp_forward(const float* params, const float* X, int batch, float* out, cudaStream_t stream);
+int simd2_mlp_gradient(const float* params, const float* X, const float* y, int batch, float* grad,
+                       float* sample_grads, cudaStream_t stream);
+int simd2_mlp_adam(float* params, const float* grad, float* m, float* v, float lr, int step,
+                   cudaStream_t stream);
+
 /* Reserve the per-(device, stream) workspace for srgemm calls up to
  * M x N x K so that later calls (e.g. inside stream capture) allocate
  * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */

@@ -63,6 +63,13 @@ def lib() -> ctypes.CDLL:
         L.simd2_status_string.restype = ctypes.c_char_p
         L.simd2_version.restype = ctypes.c_char_p
         PI = ctypes.POINTER(I)
+        PF = ctypes.POINTER(ctypes.c_float)
+        L.simd2_srgemm_tuned.argtypes = [I, I, I, I, P, I, P, I, P, I, P, I, I, I, P]
+        L.simd2_closure_ex.argtypes = [I, I, P, I, I, I, I, I, P, PI, PI, PF, PF, P]
+        L.simd2_mlp_param_count.argtypes = []
+        L.simd2_mlp_forward.argtypes = [P, P, I, P, P]
+        L.simd2_mlp_gradient.argtypes = [P, P, P, I, P, P, P]
+        L.simd2_mlp_adam.argtypes = [P, P, P, P, ctypes.c_float, I, P]
         L.simd2_batched_plan_create.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, ctypes.POINTER(P)]
         L.simd2_batched_plan_run.argtypes = [P, P]
         L.simd2_batched_plan_iters.argtypes = [P, PI, PI]
@@ -77,7 +84,9 @@ def lib() -> ctypes.CDLL:
                      "simd2_closure_orand_u8", "simd2_reserve_workspace", "simd2_release_workspaces",
                      "simd2_device_status", "simd2_profile_begin", "simd2_profile_end",
                      "simd2_batched_plan_create", "simd2_batched_plan_run", "simd2_batched_plan_iters",
-                     "simd2_batched_plan_destroy", "simd2_closure_batched"):
+                     "simd2_batched_plan_destroy", "simd2_closure_batched", "simd2_srgemm_tuned",
+                     "simd2_closure_ex", "simd2_mlp_param_count", "simd2_mlp_forward", "simd2_mlp_gradient",
+                     "simd2_mlp_adam"):
             getattr(L, name).restype = I
         _lib = L
     return _lib
@@ -142,6 +151,57 @@ def srgemm(op: str, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = N
                                 ldd, int(do_epilogue), s)
     _check(rc, f"srgemm({op})")
     return D
+
+
+NUM_CONFIGS = 8
+DISPATCH = {"dense": 0, "fixed": 1, "learned": 2}
+
+
+def config_id(split: int, skip: bool) -> int:
+    """Kernel configuration of the CUDA-core path: split-K factor and block skipping."""
+    return {1: 0, 2: 1, 4: 2, 8: 3}[split] | (4 if skip else 0)
+
+
+def config_desc(cfg: int) -> str:
+    return f"split{1 << (cfg & 3)}{'+skip' if cfg >> 2 else ''}"
+
+
+def srgemm_tuned(op: str, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, do_epilogue: bool = False,
+                 D: torch.Tensor | None = None, config: int = 0, stream=None) -> torch.Tensor:
+    """srgemm for the min/max semirings with an explicit kernel configuration (same bits for every config)."""
+    M, K = A.shape
+    N = B.shape[1]
+    if D is None:
+        D = torch.empty((M, N), dtype=torch.float32, device=A.device)
+    cptr, ldc = (C.data_ptr(), _mat(C, "C")) if do_epilogue else (None, N)
+    rc = lib().simd2_srgemm_tuned(OP_ID[op], M, N, K, A.data_ptr(), _mat(A, "A"), B.data_ptr(), _mat(B, "B"), cptr,
+                                  ldc, D.data_ptr(), _mat(D, "D"), int(do_epilogue), int(config), _stream(stream))
+    _check(rc, f"srgemm_tuned({op}, {config})")
+    return D
+
+
+def closure_ex(op: str, X: torch.Tensor, dispatch: str = "dense", config: int = 0, mlp_params=None,
+               max_iter: int = 500, conv: str = "exact", record: bool = False, stream=None):
+    """Closure with a per-step dispatch policy.
+
+    Returns the step count, or with ``record`` a dict with the per-step
+    configurations, device times (ms) and cost-model features.
+    """
+    n = X.shape[0]
+    it = ctypes.c_int(0)
+    cfgs = (ctypes.c_int * max(max_iter, 1))()
+    ms = (ctypes.c_float * max(max_iter, 1))()
+    feats = (ctypes.c_float * (max(max_iter, 1) * 7))()
+    pp = None if mlp_params is None else ctypes.c_void_p(mlp_params.data_ptr())
+    rc = lib().simd2_closure_ex(OP_ID[op], n, X.data_ptr(), _mat(X, "X"), max_iter, CONV[conv], DISPATCH[dispatch],
+                                int(config), pp, ctypes.byref(it), cfgs if record else None,
+                                ms if record else None, feats if record else None, _stream(stream))
+    _check(rc, f"closure_ex({op}, {dispatch})")
+    if not record:
+        return it.value
+    k = it.value
+    return {"iters": k, "configs": list(cfgs)[:k], "ms": list(ms)[:k],
+            "features": [list(feats)[7 * i:7 * i + 7] for i in range(k)]}
 
 
 def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", stream=None,

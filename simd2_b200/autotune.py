@@ -1,0 +1,75 @@
+"""Autotuner of the closure-step kernel configuration.
+
+Runs a closure once per configuration (split-K 1/2/4/8 x block skip) with
+``simd2_closure_ex(dispatch="fixed")`` and records, for every step, the
+cost-model features and each configuration's device time.  Every
+configuration computes the same bits, so step t of all runs sees the same
+matrix.  The records train the cost model (``costmodel.train``) and give the
+best fixed configuration per workload; they are cached as JSON.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import torch
+
+from . import NUM_CONFIGS, closure_ex, config_desc
+
+
+def profile_closure(op: str, X0: torch.Tensor, configs=range(NUM_CONFIGS), repeats: int = 1, max_iter: int = 500):
+    """Per-step timings of every configuration on one input matrix.
+
+    Returns {"n", "iters", "features": [step][7], "ms": {config: [step]}}.
+    """
+    rec = {"n": int(X0.shape[0]), "ms": {}}
+    for cfg in configs:
+        best = None
+        for _ in range(repeats):
+            X = X0.clone()
+            r = closure_ex(op, X, dispatch="fixed", config=cfg, max_iter=max_iter, record=True)
+            best = r["ms"] if best is None else [min(a, b) for a, b in zip(best, r["ms"])]
+            rec["iters"] = r["iters"]
+            rec["features"] = r["features"]
+        rec["ms"][int(cfg)] = best
+    return rec
+
+
+def dataset(records):
+    """(inputs [rows][12], targets log2(ms) [rows]) from profile records."""
+    from .costmodel import encode
+    xs, ys = [], []
+    for rec in records:
+        for cfg, times in rec["ms"].items():
+            for t, ms in enumerate(times):
+                xs.append(encode(rec["features"][t], int(cfg)))
+                ys.append(math.log2(max(ms, 1e-4)))
+    return torch.tensor(xs, dtype=torch.float32), torch.tensor(ys, dtype=torch.float32)
+
+
+def best_fixed(records):
+    """Configuration with the smallest total time over all records."""
+    tot = {}
+    for rec in records:
+        for cfg, times in rec["ms"].items():
+            tot[int(cfg)] = tot.get(int(cfg), 0.0) + sum(times)
+    return min(tot, key=tot.get), tot
+
+
+def save(records, path):
+    with open(path, "w") as f:
+        json.dump(records, f)
+
+
+def load(path):
+    with open(path) as f:
+        recs = json.load(f)
+    for r in recs:
+        r["ms"] = {int(k): v for k, v in r["ms"].items()}
+    return recs
+
+
+def describe(records):
+    cfg, tot = best_fixed(records)
+    return {config_desc(c): round(t, 3) for c, t in sorted(tot.items())} | {"best": config_desc(cfg)}

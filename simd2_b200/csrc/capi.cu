@@ -18,6 +18,7 @@
 #include "srgemm_simt.cuh"
 #include "tc_gemm.cuh"
 #include "closure_batched.cuh"
+#include "mlp.cuh"
 
 namespace simd2 {
 namespace {
@@ -199,11 +200,30 @@ bool a_tma_ok(const void* A, long long lda) {
   return (reinterpret_cast<uintptr_t>(A) % 16 == 0) && ((lda * 4) % 16 == 0);
 }
 
-template <int OP>
-int launch_simt(int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& mB, const EpilogueArgs& ep,
-                cudaStream_t stream) {
+// Kernel configuration of the CUDA-core path: split-K factor over a
+// thread-block cluster (1, 2, 4, 8) and block skipping with occupancy maps.
+struct SimtConfig {
+  int split = 1;
+  bool skip = false;
+  const uint8_t* occA = nullptr;
+  const uint8_t* occB = nullptr;
+};
+
+// The (x)-annihilator whose products equal the (+)-identity: blocks made only
+// of it (or NaN) contribute nothing and may be skipped.  Defined for the four
+// semirings where the (+)-identity annihilates (x); others never skip.
+bool skip_supported(int op) {
+  return op == SIMD2_MIN_PLUS || op == SIMD2_MAX_PLUS || op == SIMD2_MAX_MIN || op == SIMD2_MIN_MAX;
+}
+float annihilator(int op) {
+  return (op == SIMD2_MIN_PLUS || op == SIMD2_MIN_MAX) ? __builtin_inff() : -__builtin_inff();
+}
+
+template <int OP, int SPLIT, bool SKIP>
+int launch_simt_cfg(int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& mB, const EpilogueArgs& ep,
+                    const SimtConfig& cfg, cudaStream_t stream) {
   constexpr int STAGES = kSimtStages;
-  auto kern = srgemm_simt_kernel<OP, STAGES>;
+  auto kern = srgemm_simt_kernel<OP, STAGES, SPLIT, SKIP>;
   const size_t smem = simt_smem_bytes(STAGES);
   static bool configured[64] = {};  // per instantiation and device
   int dev = 0;
@@ -211,39 +231,129 @@ int launch_simt(int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& m
   if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
   if (!configured[dev]) {
     SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (SPLIT > 1) SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     configured[dev] = true;
   }
   const int tiles_m = (M + kBM - 1) / kBM;
   const int tiles_n = (N + kBN - 1) / kBN;
   auto* ev = prof_slot(2LL * M * N * K);
   if (ev) cudaEventRecord(ev->first, stream);
-  kern<<<tiles_m * tiles_n, kSimtThreads, smem, stream>>>(mA, mB, M, N, K, ep, tiles_m, tiles_n);
+  if constexpr (SPLIT == 1) {
+    kern<<<tiles_m * tiles_n, kSimtThreads, smem, stream>>>(mA, mB, M, N, K, ep, tiles_m, tiles_n, cfg.occA,
+                                                            cfg.occB);
+  } else {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(tiles_m * tiles_n * SPLIT);
+    lc.blockDim = dim3(kSimtThreads);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = SPLIT;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    SIMD2_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, mA, mB, M, N, K, ep, tiles_m, tiles_n, cfg.occA, cfg.occB));
+  }
   count_launch();
   if (ev) cudaEventRecord(ev->second, stream);
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
 }
 
+template <int OP, bool SKIP>
+int launch_simt_split(int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& mB, const EpilogueArgs& ep,
+                      const SimtConfig& cfg, cudaStream_t stream) {
+  switch (cfg.split) {
+    case 1: return launch_simt_cfg<OP, 1, SKIP>(M, N, K, mA, mB, ep, cfg, stream);
+    case 2: return launch_simt_cfg<OP, 2, SKIP>(M, N, K, mA, mB, ep, cfg, stream);
+    case 4: return launch_simt_cfg<OP, 4, SKIP>(M, N, K, mA, mB, ep, cfg, stream);
+    case 8: return launch_simt_cfg<OP, 8, SKIP>(M, N, K, mA, mB, ep, cfg, stream);
+    default: return SIMD2_ERR_INVALID_ARG;
+  }
+}
+
+template <int OP>
+int launch_simt(int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& mB, const EpilogueArgs& ep,
+                const SimtConfig& cfg, cudaStream_t stream) {
+  if constexpr (OP == SIMD2_MIN_PLUS || OP == SIMD2_MAX_PLUS || OP == SIMD2_MAX_MIN || OP == SIMD2_MIN_MAX) {
+    if (cfg.skip && cfg.occA && cfg.occB) return launch_simt_split<OP, true>(M, N, K, mA, mB, ep, cfg, stream);
+  }
+  return launch_simt_split<OP, false>(M, N, K, mA, mB, ep, cfg, stream);
+}
+
 int dispatch_simt(int op, int M, int N, int K, const CUtensorMap& mA, const CUtensorMap& mB, const EpilogueArgs& ep,
-                  cudaStream_t stream) {
+                  const SimtConfig& cfg, cudaStream_t stream) {
   switch (op) {
-    case SIMD2_MIN_PLUS: return launch_simt<SIMD2_MIN_PLUS>(M, N, K, mA, mB, ep, stream);
-    case SIMD2_PLUS_MUL: return launch_simt<SIMD2_PLUS_MUL>(M, N, K, mA, mB, ep, stream);
-    case SIMD2_MAX_PLUS: return launch_simt<SIMD2_MAX_PLUS>(M, N, K, mA, mB, ep, stream);
-    case SIMD2_MAX_MIN: return launch_simt<SIMD2_MAX_MIN>(M, N, K, mA, mB, ep, stream);
-    case SIMD2_MAX_MUL: return launch_simt<SIMD2_MAX_MUL>(M, N, K, mA, mB, ep, stream);
-    case SIMD2_MIN_MUL: return launch_simt<SIMD2_MIN_MUL>(M, N, K, mA, mB, ep, stream);
-    case SIMD2_MIN_MAX: return launch_simt<SIMD2_MIN_MAX>(M, N, K, mA, mB, ep, stream);
-    case SIMD2_MINUS_SQUARE: return launch_simt<SIMD2_MINUS_SQUARE>(M, N, K, mA, mB, ep, stream);
+    case SIMD2_MIN_PLUS: return launch_simt<SIMD2_MIN_PLUS>(M, N, K, mA, mB, ep, cfg, stream);
+    case SIMD2_MAX_PLUS: return launch_simt<SIMD2_MAX_PLUS>(M, N, K, mA, mB, ep, cfg, stream);
+    case SIMD2_MAX_MIN: return launch_simt<SIMD2_MAX_MIN>(M, N, K, mA, mB, ep, cfg, stream);
+    case SIMD2_MAX_MUL: return launch_simt<SIMD2_MAX_MUL>(M, N, K, mA, mB, ep, cfg, stream);
+    case SIMD2_MIN_MUL: return launch_simt<SIMD2_MIN_MUL>(M, N, K, mA, mB, ep, cfg, stream);
+    case SIMD2_MIN_MAX: return launch_simt<SIMD2_MIN_MAX>(M, N, K, mA, mB, ep, cfg, stream);
     default: return SIMD2_ERR_UNSUPPORTED;
   }
+}
+
+// ---------------------------------------------------------------------------
+// block occupancy (for skip lists and the cost-model features)
+// ---------------------------------------------------------------------------
+struct OccPlan {
+  int brA, bcA, brB, bcB;  // 32 x 32 block grid of A (M x K) and B (K x N)
+  int tiles_m, tiles_n, ktiles;
+  size_t occ32A, occ32B, occA, occB, stats, total;
+};
+
+OccPlan make_occ_plan(int M, int N, int K, bool same) {
+  OccPlan o{};
+  o.brA = (M + 31) / 32;
+  o.bcA = (K + 31) / 32;
+  o.brB = (K + 31) / 32;
+  o.bcB = (N + 31) / 32;
+  o.tiles_m = (M + kBM - 1) / kBM;
+  o.tiles_n = (N + kBN - 1) / kBN;
+  o.ktiles = (K + kBK - 1) / kBK;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t r = off; off += align_up(std::max(bytes, (size_t)1), 256); return r; };
+  o.occ32A = take((size_t)o.brA * o.bcA);
+  o.occ32B = same ? o.occ32A : take((size_t)o.brB * o.bcB);
+  o.occA = take((size_t)o.tiles_m * o.ktiles);
+  o.occB = take((size_t)o.ktiles * o.tiles_n);
+  o.stats = take(4 * sizeof(unsigned long long));
+  o.total = off;
+  return o;
+}
+
+// Fills occA / occB and stats = {surviving (tm,tn,kt) triples, occupied A
+// blocks, occupied B blocks}.  When `same`, A and B are the same matrix
+// (closure), and one 32 x 32 pass serves both.
+int compute_occupancy(int op, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb,
+                      bool same, uint8_t* base, const OccPlan& o, cudaStream_t stream) {
+  const float ann = annihilator(op);
+  auto* occ32A = base + o.occ32A;
+  auto* occ32B = base + o.occ32B;
+  occupancy32_kernel<<<dim3(o.bcA, o.brA), dim3(32, 8), 0, stream>>>(A, lda, M, K, ann, occ32A, o.bcA);
+  count_launch();
+  if (!same) {
+    occupancy32_kernel<<<dim3(o.bcB, o.brB), dim3(32, 8), 0, stream>>>(B, ldb, K, N, ann, occ32B, o.bcB);
+    count_launch();
+  }
+  auto* stats = reinterpret_cast<unsigned long long*>(base + o.stats);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), stream));
+  occupancy_panels_kernel<<<std::min(o.ktiles, 148 * 4), 256, 0, stream>>>(
+      occ32A, o.bcA, o.brA, occ32B, o.bcB, o.brB, o.tiles_m, o.tiles_n, o.ktiles, base + o.occA, base + o.occB, stats);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
 }
 
 // Core float srgemm with an explicit workspace.  T/MODE describe how A and B
 // are read (float as-is, or any type normalised to {0,1}).
 template <typename T, int MODE>
 int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T* B, long long ldb,
-                const EpilogueArgs& ep, uint8_t* ws, const Plan& plan, bool pack_a, cudaStream_t stream) {
+                const EpilogueArgs& ep, uint8_t* ws, const Plan& plan, bool pack_a, cudaStream_t stream,
+                const SimtConfig& cfg = SimtConfig()) {
   const float pad = pad_value(op);
   float* Bp = reinterpret_cast<float*>(ws + plan.bp_off);
   interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 2), 256, 0, stream>>>(
@@ -267,7 +377,7 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   rc = make_map_f32(&mB, Bp, plan.Kp / 2, 2LL * plan.Np, 2LL * plan.Np, 2 * kBN, kBK / 2, CU_TENSOR_MAP_SWIZZLE_NONE,
                     false);
   if (rc) return rc;
-  return dispatch_simt(op, M, N, K, mA, mB, ep, stream);
+  return dispatch_simt(op, M, N, K, mA, mB, ep, cfg, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -512,26 +622,56 @@ int srgemm_orand(int M, int N, int K, const T* A, long long lda, const T* B, lon
 // ---------------------------------------------------------------------------
 namespace {
 
-int closure_f32(int op, int n, float* X, long long ldx, int max_iter, int conv, int* iters_out,
-                cudaStream_t stream) {
+// Closure by repeated squaring with a per-step kernel configuration:
+//   dispatch 0 (dense)  : split 1, no skip (the plain path);
+//   dispatch 1 (fixed)  : `fixed_cfg` (split = 1 << (cfg & 3), skip = cfg >> 2) every step;
+//   dispatch 2 (learned): block occupancy of X_t -> features -> the MLP
+//                         `mlp_params` predicts each configuration's time and
+//                         the cheapest one runs.
+// Every configuration computes the same bits, so the dispatch only moves time.
+// step_cfg / step_ms / step_feat (host arrays of max_iter, max_iter,
+// max_iter * kMlpFeat entries, each optional) record what each step ran, its
+// device time (occupancy + operand prep + srgemm) and its features.
+int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int conv, int dispatch, int fixed_cfg,
+                   const float* mlp_params, int* iters_out, int* step_cfg, float* step_ms, float* step_feat,
+                   cudaStream_t stream) {
   if (iters_out) *iters_out = 0;
-  if (n < 0 || max_iter < 0 || !is_float_op(op) || (n > 0 && (!X || ldx < n))) return SIMD2_ERR_INVALID_ARG;
+  if (n < 0 || max_iter < 0 || !is_float_op(op) || is_sum_op(op) || (n > 0 && (!X || ldx < n)))
+    return SIMD2_ERR_INVALID_ARG;
+  if (dispatch < 0 || dispatch > 2 || (dispatch == 2 && !mlp_params) || fixed_cfg < 0 || fixed_cfg >= kNumConfigs)
+    return SIMD2_ERR_INVALID_ARG;
   if (n == 0 || max_iter == 0) return SIMD2_OK;
   int rc = check_device();
   if (rc) return rc;
-  // Workspace: [srgemm plan][Xnew n x n][change flag]
+  int sms = 148;
+  {
+    int dev = 0;
+    SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+    SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const bool can_skip = skip_supported(op) && (n + kBK - 1) / kBK <= kMaxSkipKtiles;
+  const bool need_occ = dispatch == 2 || step_feat != nullptr || (dispatch == 1 && config_skip(fixed_cfg) && can_skip);
+  // Workspace: [srgemm plan][Xnew n x n][flag + decision][occupancy]
   const bool pack_a = !a_tma_ok(X, ldx) || (n % 4 != 0);
   const Plan plan = make_plan(n, n, n, pack_a);
+  const OccPlan occ = make_occ_plan(n, n, n, true);
   const size_t x_off = align_up(plan.total, kAlign);
-  const size_t x_bytes = align_up((size_t)n * n * 4, kAlign);
-  const size_t f_off = x_off + x_bytes;
-  const size_t total = f_off + kAlign;
+  const size_t f_off = x_off + align_up((size_t)n * n * 4, kAlign);
+  const size_t o_off = f_off + kAlign;
+  const size_t total = o_off + (need_occ ? align_up(occ.total, kAlign) : 0);
   void* p = nullptr;
   if ((rc = get_workspace(stream, total, &p))) return rc;
   uint8_t* ws = static_cast<uint8_t*>(p);
   float* Xn = reinterpret_cast<float*>(ws + x_off);
   int* flag = reinterpret_cast<int*>(ws + f_off);
+  int* decision = flag + 8;  // [0] config, [1..8] predictions
+  uint8_t* obase = ws + o_off;
 
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (step_ms) {
+    SIMD2_CUDA_TRY(cudaEventCreate(&e0));
+    SIMD2_CUDA_TRY(cudaEventCreate(&e1));
+  }
   float* cur = X;
   long long ldcur = ldx;
   float* nxt = Xn;
@@ -539,20 +679,72 @@ int closure_f32(int op, int n, float* X, long long ldx, int max_iter, int conv, 
   int it = 0;
   int changed = 1;
   while (changed && it < max_iter) {
+    if (e0) cudaEventRecord(e0, stream);
+    int cfg_id = dispatch == 1 ? fixed_cfg : 0;
+    SimtConfig cfg;
+    if (need_occ) {
+      rc = compute_occupancy(op, n, n, n, cur, ldcur, cur, ldcur, true, obase, occ, stream);
+      if (rc) break;
+      if (dispatch == 2) {
+        mlp_choose_kernel<<<1, 32, 0, stream>>>(mlp_params, reinterpret_cast<unsigned long long*>(obase + occ.stats),
+                                                n, occ.tiles_m, occ.tiles_n, occ.ktiles, sms, can_skip ? 1 : 0, 8,
+                                                decision);
+        count_launch();
+        int h = 0;
+        if (cudaMemcpyAsync(&h, decision, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+          rc = SIMD2_ERR_CUDA;
+          break;
+        }
+        cfg_id = h;
+      }
+      if (step_feat) {
+        unsigned long long st[3];
+        if (cudaMemcpyAsync(st, obase + occ.stats, sizeof(st), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+          rc = SIMD2_ERR_CUDA;
+          break;
+        }
+        mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, st[0], st[1], st[2], sms,
+                     step_feat + (size_t)it * kMlpFeat);
+      }
+    }
+    cfg.split = config_split(cfg_id);
+    cfg.skip = config_skip(cfg_id) && can_skip && need_occ;
+    if (cfg.skip) {
+      cfg.occA = obase + occ.occA;
+      cfg.occB = obase + occ.occB;
+    }
+    if (step_cfg) step_cfg[it] = (cfg.skip ? 4 : 0) | (cfg.split == 1 ? 0 : cfg.split == 2 ? 1 : cfg.split == 4 ? 2 : 3);
     it++;
-    SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), stream));
+    if (cudaMemsetAsync(flag, 0, sizeof(int), stream) != cudaSuccess) {
+      rc = SIMD2_ERR_CUDA;
+      break;
+    }
     const bool pk = !a_tma_ok(cur, ldcur);
     const Plan pl = make_plan(n, n, n, pk);
     const EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, flag, conv);
-    rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream);
-    if (rc) return rc;
+    rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream, cfg);
+    if (rc) break;
+    if (e1) cudaEventRecord(e1, stream);
     int h = 0;
-    SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+      rc = SIMD2_ERR_CUDA;
+      break;
+    }
+    if (step_ms) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      step_ms[it - 1] = ms;
+    }
     changed = h != 0;
     std::swap(cur, nxt);
     std::swap(ldcur, ldnxt);
   }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc) return rc;
   if (cur != X) {
     SIMD2_CUDA_TRY(cudaMemcpy2DAsync(X, ldx * 4, cur, ldcur * 4, (size_t)n * 4, n, cudaMemcpyDeviceToDevice, stream));
   }
@@ -561,6 +753,10 @@ int closure_f32(int op, int n, float* X, long long ldx, int max_iter, int conv, 
   return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
+int closure_f32(int op, int n, float* X, long long ldx, int max_iter, int conv, int* iters_out,
+                cudaStream_t stream) {
+  return closure_f32_ex(op, n, X, ldx, max_iter, conv, 0, 0, nullptr, iters_out, nullptr, nullptr, nullptr, stream);
+}
 
 // ---------------------------------------------------------------------------
 // batched closure
@@ -904,6 +1100,79 @@ int simd2_closure_batched(simd2_op op, int count, float* const* X, const int* n,
   simd2_batched_plan_destroy(plan);
   if (!rc && nc > 0) rc = SIMD2_ERR_NOT_CONVERGED;
   return rc;
+}
+
+}  // extern "C"
+
+
+extern "C" {
+
+int simd2_srgemm_tuned(simd2_op op, int M, int N, int K, const float* A, int lda, const float* B, int ldb,
+                       const float* C, int ldc, float* D, int ldd, int do_epilogue, int config, cudaStream_t stream) {
+  if (!is_float_op(op) || is_sum_op(op)) return op == SIMD2_OR_AND || is_sum_op(op) ? SIMD2_ERR_UNSUPPORTED
+                                                                                     : SIMD2_ERR_INVALID_ARG;
+  if (config < 0 || config >= kNumConfigs) return SIMD2_ERR_INVALID_ARG;
+  int rc = check_dims(M, N, K, lda, ldb, ldc, ldd, A, B, C, D, do_epilogue);
+  if (rc || M == 0 || N == 0) return rc;
+  if ((rc = check_device())) return rc;
+  if (K == 0) return srgemm_k0(op, M, N, C, ldc, D, ldd, do_epilogue, stream);
+  const bool pack_a = !a_tma_ok(A, lda);
+  const Plan plan = make_plan(M, N, K, pack_a);
+  const bool skip = config_skip(config) && skip_supported(op) && (K + kBK - 1) / kBK <= kMaxSkipKtiles;
+  const OccPlan occ = make_occ_plan(M, N, K, false);
+  const size_t o_off = align_up(plan.total, kAlign);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, o_off + (skip ? occ.total : 0), &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  SimtConfig cfg;
+  cfg.split = config_split(config);
+  if (skip) {
+    if ((rc = compute_occupancy(op, M, N, K, A, lda, B, ldb, false, ws + o_off, occ, stream))) return rc;
+    cfg.skip = true;
+    cfg.occA = ws + o_off + occ.occA;
+    cfg.occB = ws + o_off + occ.occB;
+  }
+  const EpilogueArgs ep = make_epilogue(C, ldc, D, ldd, do_epilogue, nullptr, 0);
+  return srgemm_core<float, 0>(op, M, N, K, A, lda, B, ldb, ep, ws, plan, pack_a, stream, cfg);
+}
+
+int simd2_closure_ex(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_conv conv, simd2_dispatch dispatch,
+                     int fixed_config, const float* mlp_params, int* iters_out, int* step_configs, float* step_ms,
+                     float* step_features, cudaStream_t stream) {
+  if (conv < SIMD2_CONV_EXACT || conv > SIMD2_CONV_APLP) return SIMD2_ERR_INVALID_ARG;
+  return closure_f32_ex(op, n, X, ldx, max_iter, conv, (int)dispatch, fixed_config, mlp_params, iters_out,
+                        step_configs, step_ms, step_features, stream);
+}
+
+int simd2_mlp_param_count(void) { return kMlpParams; }
+
+int simd2_mlp_forward(const float* params, const float* X, int batch, float* out, cudaStream_t stream) {
+  if (!params || !X || !out || batch < 0) return SIMD2_ERR_INVALID_ARG;
+  if (batch == 0) return SIMD2_OK;
+  mlp_forward_kernel<<<grid_for(batch, 128), 128, 0, stream>>>(params, X, batch, out);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+int simd2_mlp_gradient(const float* params, const float* X, const float* y, int batch, float* grad,
+                       float* sample_grads, cudaStream_t stream) {
+  if (!params || !X || !y || !grad || !sample_grads || batch <= 0) return SIMD2_ERR_INVALID_ARG;
+  mlp_sample_grad_kernel<<<grid_for(batch, 64), 64, 0, stream>>>(params, X, y, batch, sample_grads);
+  count_launch();
+  column_sum_kernel<<<grid_for(kMlpParams, 128), 128, 0, stream>>>(sample_grads, batch, kMlpParams, grad);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+int simd2_mlp_adam(float* params, const float* grad, float* m, float* v, float lr, int step, cudaStream_t stream) {
+  if (!params || !grad || !m || !v || step < 1) return SIMD2_ERR_INVALID_ARG;
+  adam_kernel<<<grid_for(kMlpParams, 256), 256, 0, stream>>>(params, grad, m, v, kMlpParams, lr, 0.9f, 0.999f, 1e-8f,
+                                                             step);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
 }
 
 }  // extern "C"

@@ -100,22 +100,58 @@ __device__ __forceinline__ float epilogue_value(int do_epi, int conv_mode, bool 
   return v;
 }
 
-template <int OP, int STAGES>
+// Largest k-tile count for which a skip list fits in shared memory.
+constexpr int kMaxSkipKtiles = 4096;
+
+// Distributed shared memory helpers (thread-block clusters).
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ float ld_dsmem_f32(const float* local_ptr, uint32_t rank) {
+  uint32_t remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(local_ptr)), "r"(rank));
+  float v;
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(remote) : "memory");
+  return v;
+}
+
+// One CTA (or one CTA of a SPLIT-wide cluster) per 128 x 128 output tile.
+//   SPLIT > 1 : the cluster's CTAs take every SPLIT-th k-tile of the tile's
+//               k list, park their partial tile in shared memory, and each
+//               CTA then folds 128/SPLIT rows of all partials (read through
+//               distributed shared memory) with (+) and runs the epilogue on
+//               them.  min/max are associative, so the result is exact.
+//   SKIP      : the k list holds only the k-tiles whose A block (128 rows x
+//               32 k) and B block (32 k x 128 columns) both contain an entry
+//               other than the (x)-annihilator (occupancy maps occA, occB);
+//               a skipped block can only produce identity products.
+template <int OP, int STAGES, int SPLIT, bool SKIP>
 __global__ void __launch_bounds__(kSimtThreads, 1)
     srgemm_simt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M,
-                       int N, int K, EpilogueArgs ep, int tiles_m, int tiles_n) {
+                       int N, int K, EpilogueArgs ep, int tiles_m, int tiles_n, const uint8_t* __restrict__ occA,
+                       const uint8_t* __restrict__ occB) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
   uint64_t* empty = full + STAGES;
+  __shared__ uint16_t s_klist[SKIP ? kMaxSkipKtiles : 1];
+  __shared__ int s_warp_cnt[kSimtWarps];
+  __shared__ int s_kcount;
 
   // Grouped raster: 8 consecutive tile rows share each B' column panel in L2.
+  const int tile = blockIdx.x / SPLIT;
+  const int rank = SPLIT > 1 ? (int)cluster_ctarank() : 0;
   const int group = 8;
   const int per_group = group * tiles_n;
-  const int g = blockIdx.x / per_group;
+  const int g = tile / per_group;
   const int first_m = g * group;
   const int gsize = min(tiles_m - first_m, group);
-  const int local = blockIdx.x - g * per_group;
+  const int local = tile - g * per_group;
   const int tm = first_m + local % gsize;
   const int tn = local / gsize;
   const int m0 = tm * kBM;
@@ -132,17 +168,48 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     }
     fence_mbar_init();
   }
-  __syncthreads();
 
-  // Thread 0 issues the first STAGES tiles; refills happen inside the k loop.
+  // ---- this CTA's k list: the tile's (occupied) k-tiles, every SPLIT-th one ----
+  int nlist = ktiles;
+  if constexpr (SKIP) {
+    int running = 0;
+    for (int base = 0; base < ktiles; base += kSimtThreads) {
+      const int kt = base + threadIdx.x;
+      const bool f = kt < ktiles && occA[(long long)tm * ktiles + kt] && occB[(long long)kt * tiles_n + tn];
+      const unsigned ballot = __ballot_sync(0xffffffffu, f);
+      if (lane == 0) s_warp_cnt[warp] = __popc(ballot);
+      __syncthreads();
+      int off = 0, total = 0;
+      for (int w = 0; w < kSimtWarps; w++) {
+        const int c = s_warp_cnt[w];
+        off += w < warp ? c : 0;
+        total += c;
+      }
+      if (f) s_klist[running + off + __popc(ballot & ((1u << lane) - 1u))] = (uint16_t)kt;
+      running += total;
+      __syncthreads();
+    }
+    nlist = running;
+  }
+  __syncthreads();
+  // entries i = rank, rank + SPLIT, ... of the list
+  const int nmine = nlist > rank ? (nlist - rank + SPLIT - 1) / SPLIT : 0;
+  auto kt_of = [&](int i) -> int {
+    const int li = rank + i * SPLIT;
+    if constexpr (SKIP) return s_klist[li];
+    else return li;
+  };
+
+  // Thread 0 issues the first STAGES k-tiles; refills happen inside the k loop.
   if (threadIdx.x == 0) {
     prefetch_tensormap(&tmA);
     prefetch_tensormap(&tmB);
-    for (int kt = 0; kt < min(STAGES, ktiles); kt++) {
-      uint8_t* sa = smem + kt * kStageBytes;
-      mbar_arrive_expect_tx(&full[kt], kStageBytes);
-      tma_load_2d(sa, &tmA, &full[kt], kt * kBK, m0);
-      tma_load_2d(sa + kATileBytes, &tmB, &full[kt], 2 * n0, kt * (kBK / 2));
+    for (int i = 0; i < min(STAGES, nmine); i++) {
+      const int kt = kt_of(i);
+      uint8_t* sa = smem + i * kStageBytes;
+      mbar_arrive_expect_tx(&full[i], kStageBytes);
+      tma_load_2d(sa, &tmA, &full[i], kt * kBK, m0);
+      tma_load_2d(sa + kATileBytes, &tmB, &full[i], 2 * n0, kt * (kBK / 2));
     }
   }
 
@@ -159,25 +226,25 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     for (int j = 0; j < 2 * WN; j++) acc[i][j] = Mac<OP>::identity();
 
   bool ok = true;
-  int issued = min(STAGES, ktiles);
-  for (int kt = 0; kt < ktiles; kt++) {
-    const int s = kt % STAGES;
-    // Refill the stage that tile kt-1 used once every warp has released it.
-    if (threadIdx.x == 0 && kt >= 1 && kt - 1 + STAGES < ktiles) {
-      const int r = kt - 1, rs = r % STAGES;
+  int issued = min(STAGES, nmine);
+  for (int i = 0; i < nmine; i++) {
+    const int s = i % STAGES;
+    // Refill the stage that list entry i-1 used once every warp has released it.
+    if (threadIdx.x == 0 && i >= 1 && i - 1 + STAGES < nmine) {
+      const int r = i - 1, rs = r % STAGES;
       if (mbar_wait(&empty[rs], (r / STAGES) & 1)) {
         uint8_t* sa = smem + rs * kStageBytes;
-        const int nk = r + STAGES;
+        const int nk = kt_of(r + STAGES);
         mbar_arrive_expect_tx(&full[rs], kStageBytes);
         tma_load_2d(sa, &tmA, &full[rs], nk * kBK, m0);
         tma_load_2d(sa + kATileBytes, &tmB, &full[rs], 2 * n0, nk * (kBK / 2));
-        issued = nk + 1;
+        issued = r + STAGES + 1;
       } else {
-        report_error(SIMD2_ERR_TIMEOUT);
+        report_timeout(1);
       }
     }
-    if (!mbar_wait(&full[s], (kt / STAGES) & 1)) {
-      report_error(SIMD2_ERR_TIMEOUT);
+    if (!mbar_wait(&full[s], (i / STAGES) & 1)) {
+      report_timeout(2);
       ok = false;
       break;
     }
@@ -187,8 +254,8 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     for (int q = 0; q < kBK / 4; q++) {
       float4 a[8];
 #pragma unroll
-      for (int i = 0; i < 8; i++)
-        a[i] = *reinterpret_cast<const float4*>(As + (ty + 16 * i) * kBK + ((q ^ swz) << 2));
+      for (int ii = 0; ii < 8; ii++)
+        a[ii] = *reinterpret_cast<const float4*>(As + (ty + 16 * ii) * kBK + ((q ^ swz) << 2));
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         float4 b[WN];
@@ -196,12 +263,12 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
         for (int c = 0; c < WN; c++)
           b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (cbase + 32 * c + 2 * tx) * 2);
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const float2 ap = h == 0 ? make_float2(a[i].x, a[i].y) : make_float2(a[i].z, a[i].w);
+        for (int ii = 0; ii < 8; ii++) {
+          const float2 ap = h == 0 ? make_float2(a[ii].x, a[ii].y) : make_float2(a[ii].z, a[ii].w);
 #pragma unroll
           for (int c = 0; c < WN; c++) {
-            acc[i][2 * c] = Mac<OP>::mac2(acc[i][2 * c], ap, make_float2(b[c].x, b[c].y));
-            acc[i][2 * c + 1] = Mac<OP>::mac2(acc[i][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
+            acc[ii][2 * c] = Mac<OP>::mac2(acc[ii][2 * c], ap, make_float2(b[c].x, b[c].y));
+            acc[ii][2 * c + 1] = Mac<OP>::mac2(acc[ii][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
           }
         }
       }
@@ -212,8 +279,8 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
   if (!ok) {
     // Every issued copy must land before this CTA's shared memory is released.
     if (threadIdx.x == 0)
-      for (int kt = max(0, issued - STAGES); kt < issued; kt++) mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1);
-    return;
+      for (int i = max(0, issued - STAGES); i < issued; i++) mbar_wait(&full[i % STAGES], (i / STAGES) & 1);
+    if constexpr (SPLIT == 1) return;
   }
 
   // ---------------- epilogue ----------------
@@ -223,38 +290,129 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
   const float* Cbase = ep.C;
   float* Dbase = ep.D;
   const long long ldc = ep.ldc, ldd = ep.ldd;
-  const int vec2 = ep.vec2;
   int changed = 0;
+
+  if constexpr (SPLIT == 1) {
+    const int vec2 = ep.vec2;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const int row = m0 + ty + 16 * i;
-    if (row < M) {
-      const float* crow = Cbase + (long long)row * ldc;
-      float* drow = Dbase + (long long)row * ldd;
+    for (int i = 0; i < 8; i++) {
+      const int row = m0 + ty + 16 * i;
+      if (row < M) {
+        const float* crow = Cbase + (long long)row * ldc;
+        float* drow = Dbase + (long long)row * ldd;
 #pragma unroll
-      for (int c = 0; c < WN; c++) {
-        const int col = n0 + cbase + 32 * c + 2 * tx;
-        if (vec2 && col + 1 < N) {
-          float2 cv = make_float2(0.f, 0.f);
-          if (do_epi) cv = *reinterpret_cast<const float2*>(crow + col);
-          float2 v;
-          v.x = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c], cv.x, changed);
-          v.y = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + 1], cv.y, changed);
-          *reinterpret_cast<float2*>(drow + col) = v;
-        } else {
+        for (int c = 0; c < WN; c++) {
+          const int col = n0 + cbase + 32 * c + 2 * tx;
+          if (vec2 && col + 1 < N) {
+            float2 cv = make_float2(0.f, 0.f);
+            if (do_epi) cv = *reinterpret_cast<const float2*>(crow + col);
+            float2 v;
+            v.x = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c], cv.x, changed);
+            v.y = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + 1], cv.y, changed);
+            *reinterpret_cast<float2*>(drow + col) = v;
+          } else {
 #pragma unroll
-          for (int e = 0; e < 2; e++) {
-            if (col + e < N) {
-              const float cv = do_epi ? crow[col + e] : 0.0f;
-              drow[col + e] = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + e], cv, changed);
+            for (int e = 0; e < 2; e++) {
+              if (col + e < N) {
+                const float cv = do_epi ? crow[col + e] : 0.0f;
+                drow[col + e] = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + e], cv, changed);
+              }
             }
           }
         }
       }
     }
+  } else {
+    // Park the partial tile (row-major 128 x 128, padded rows) in the now idle stage memory.
+    constexpr int kPitch = kBN + 4;
+    float* part = reinterpret_cast<float*>(smem);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int c = 0; c < WN; c++) {
+        const int r = ty + 16 * i, col = cbase + 32 * c + 2 * tx;
+        part[r * kPitch + col] = acc[i][2 * c];
+        part[r * kPitch + col + 1] = acc[i][2 * c + 1];
+      }
+    cluster_sync_all();  // every partial is in place
+    constexpr int kRows = kBM / SPLIT;
+    for (int e = threadIdx.x; e < kRows * kBN; e += kSimtThreads) {
+      const int r = rank * kRows + e / kBN;
+      const int col = e % kBN;
+      float v = part[r * kPitch + col];
+#pragma unroll
+      for (int peer = 0; peer < SPLIT; peer++)
+        if (peer != rank) v = Mac<OP>::add(v, ld_dsmem_f32(part + r * kPitch + col, (uint32_t)peer));
+      const int row = m0 + r, gcol = n0 + col;
+      if (ok && row < M && gcol < N) {
+        const float cv = do_epi ? Cbase[(long long)row * ldc + gcol] : 0.0f;
+        Dbase[(long long)row * ldd + gcol] = epilogue_value<OP>(do_epi, conv_mode, track, v, cv, changed);
+      }
+    }
+    cluster_sync_all();  // peers stay resident until every CTA has read their partials
   }
   if (track) {
     if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
+  }
+}
+
+// Block occupancy for the skip lists: occ32[bi][bj] = 1 when the 32 x 32
+// block (rows 32 bi.., cols 32 bj..) of X holds an entry that is neither NaN
+// nor `annihilator` (the value whose (x)-product is the (+)-identity).
+__global__ void occupancy32_kernel(const float* __restrict__ X, long long ldx, int rows, int cols, float annihilator,
+                                   uint8_t* __restrict__ occ32, int bcols) {
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  const int r = bi * 32 + threadIdx.y, c0 = bj * 32;
+  bool f = false;
+  for (int rr = r; rr < min(bi * 32 + 32, rows); rr += blockDim.y) {
+    const int c = c0 + threadIdx.x;
+    if (c < cols) {
+      const float v = X[(long long)rr * ldx + c];
+      f |= (v == v) && (v != annihilator);
+    }
+  }
+  const int any = __syncthreads_or(f);
+  if (threadIdx.x == 0 && threadIdx.y == 0) occ32[(long long)bi * bcols + bj] = (uint8_t)any;
+}
+
+// occA[tm][kt] = OR of occ32 over rows 4tm..4tm+3 at column block kt;
+// occB[kt][tn] = OR of occ32 over row block kt, column blocks 4tn..4tn+3.
+// Also counts surviving (tm, tn, kt) triples into stats[0], occupied A blocks
+// into stats[1] and occupied B blocks into stats[2].
+__global__ void occupancy_panels_kernel(const uint8_t* __restrict__ occ32A, int bcolsA, int browsA,
+                                        const uint8_t* __restrict__ occ32B, int bcolsB, int browsB, int tiles_m,
+                                        int tiles_n, int ktiles, uint8_t* __restrict__ occA,
+                                        uint8_t* __restrict__ occB, unsigned long long* stats) {
+  for (int kt = blockIdx.x; kt < ktiles; kt += gridDim.x) {
+    __shared__ int s_ca, s_cb;
+    if (threadIdx.x == 0) s_ca = s_cb = 0;
+    __syncthreads();
+    for (int tm = threadIdx.x; tm < tiles_m; tm += blockDim.x) {
+      uint8_t v = 0;
+      for (int q = 0; q < 4; q++) {
+        const int bi = tm * 4 + q;
+        if (bi < browsA && kt < bcolsA) v |= occ32A[(long long)bi * bcolsA + kt];
+      }
+      occA[(long long)tm * ktiles + kt] = v;
+      if (v) atomicAdd(&s_ca, 1);
+    }
+    for (int tn = threadIdx.x; tn < tiles_n; tn += blockDim.x) {
+      uint8_t v = 0;
+      for (int q = 0; q < 4; q++) {
+        const int bj = tn * 4 + q;
+        if (kt < browsB && bj < bcolsB) v |= occ32B[(long long)kt * bcolsB + bj];
+      }
+      occB[(long long)kt * tiles_n + tn] = v;
+      if (v) atomicAdd(&s_cb, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      atomicAdd(&stats[0], (unsigned long long)s_ca * (unsigned long long)s_cb);
+      atomicAdd(&stats[1], (unsigned long long)s_ca);
+      atomicAdd(&stats[2], (unsigned long long)s_cb);
+    }
+    __syncthreads();
   }
 }
 

@@ -1,0 +1,118 @@
+"""Kernel configurations (split-K clusters, block skipping) and the learned dispatch."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import simd2_b200 as s2
+from oracle import mlp as mlp_oracle
+from simd2_b200 import autotune, costmodel, datagen
+
+pytestmark = pytest.mark.gpu
+SKIPPABLE = ["min_plus", "max_plus", "max_min", "min_max"]
+
+
+def bits(x):
+    return np.ascontiguousarray(x).view(np.uint32)
+
+
+def sparse_operands(op, m, n, k, seed, density):
+    """Operands whose blocks are often entirely the (x)-annihilator."""
+    a, b, c = datagen.semiring_operands(op, m, n, k, seed=seed)
+    ann = np.float32(np.inf if op in ("min_plus", "min_max", "min_mul") else -np.inf)
+    rng = np.random.default_rng(seed)
+    # zero out whole 32 x 32 blocks with probability 1 - density
+    for x in (a, b):
+        br, bc = (x.shape[0] + 31) // 32, (x.shape[1] + 31) // 32
+        keep = rng.random((br, bc)) < density
+        mask = np.repeat(np.repeat(keep, 32, 0), 32, 1)[: x.shape[0], : x.shape[1]]
+        x[~mask] = ann
+    return a, b, c
+
+
+@pytest.mark.parametrize("op", SKIPPABLE + ["max_mul", "min_mul"])
+@pytest.mark.parametrize("shape", [(300, 260, 517), (128, 128, 96), (1, 513, 33), (700, 130, 1024)])
+def test_all_configs_bit_exact(cuda, op, shape):
+    m, n, k = shape
+    a, b, c = sparse_operands(op, m, n, k, seed=m + k, density=0.3)
+    want = oracle.srgemm(op, a, b, c, do_epilogue=True)
+    A, B, C = (torch.from_numpy(x).to(cuda) for x in (a, b, c))
+    for cfg in range(s2.NUM_CONFIGS):
+        D = s2.srgemm_tuned(op, A, B, C, do_epilogue=True, config=cfg)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(bits(D.cpu().numpy()), bits(want), err_msg=f"{op} {shape} {s2.config_desc(cfg)}")
+    assert s2.device_status() == 0
+
+
+def test_empty_k_lists(cuda):
+    """Rows/columns made only of +inf: every k-block is skipped, D = C."""
+    a = np.full((256, 300), np.inf, np.float32)
+    b = np.full((300, 256), np.inf, np.float32)
+    c = np.random.default_rng(1).random((256, 256)).astype(np.float32)
+    A, B, C = (torch.from_numpy(x).to(cuda) for x in (a, b, c))
+    for cfg in (4, 5, 7):
+        D = s2.srgemm_tuned("min_plus", A, B, C, do_epilogue=True, config=cfg)
+        np.testing.assert_array_equal(D.cpu().numpy(), c)
+
+
+@pytest.mark.parametrize("op", ["min_plus", "max_min"])
+def test_closure_every_config_identical(cuda, op):
+    x = datagen.rmat_graph(512, 3.0, seed=4) if op == "min_plus" else datagen.closure_graph(op, 400, 0.01, seed=4)
+    want, it_want = oracle.closure(op, x)
+    for cfg in range(s2.NUM_CONFIGS):
+        X = torch.from_numpy(x.copy()).to(cuda)
+        r = s2.closure_ex(op, X, dispatch="fixed", config=cfg, record=True)
+        assert r["iters"] == it_want
+        np.testing.assert_array_equal(bits(X.cpu().numpy()), bits(want), err_msg=s2.config_desc(cfg))
+        assert all(c == cfg for c in r["configs"])
+
+
+def test_mlp_gradient_matches_fp64_oracle(cuda):
+    rng = np.random.default_rng(3)
+    p = (rng.standard_normal(costmodel.param_count()) * 0.3).astype(np.float32)
+    X = rng.standard_normal((97, 12)).astype(np.float32)
+    y = rng.standard_normal(97).astype(np.float32)
+    P = torch.from_numpy(p).to(cuda)
+    g = costmodel.gradient(P, torch.from_numpy(X).to(cuda), torch.from_numpy(y).to(cuda)).cpu().numpy()
+    want = mlp_oracle.gradient(p.astype(np.float64), X.astype(np.float64), y.astype(np.float64))
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(g, want, rtol=1e-3, atol=1e-5 * scale)
+    out = costmodel.forward(P, torch.from_numpy(X).to(cuda)).cpu().numpy()
+    np.testing.assert_allclose(out, mlp_oracle.forward(p.astype(np.float64), X.astype(np.float64))[0], rtol=1e-4,
+                               atol=1e-5)
+    # deterministic batch sum: same gradient bits twice
+    g2 = costmodel.gradient(P, torch.from_numpy(X).to(cuda), torch.from_numpy(y).to(cuda)).cpu().numpy()
+    np.testing.assert_array_equal(g, g2)
+
+
+def test_mlp_training_fits(cuda):
+    rng = np.random.default_rng(5)
+    X = rng.random((512, 12)).astype(np.float32)
+    y = (np.sin(3 * X[:, 0]) + X[:, 1] * X[:, 2] - X[:, 7]).astype(np.float32)
+    Xt, yt = torch.from_numpy(X).to(cuda), torch.from_numpy(y).to(cuda)
+    params, losses = costmodel.train(Xt, yt, steps=1500, lr=3e-3)
+    assert losses[-1] < 0.1 * losses[0]
+    assert losses[-1] < 0.01
+
+
+def test_learned_dispatch_identical_and_not_slower(cuda):
+    """Train on autotuner timings of some R-MAT closures, then close held-out
+    R-MAT graphs with the learned dispatch: same bits as the dense path, and
+    no slower than it."""
+    train_graphs = [datagen.rmat_graph(2048, d, seed=10 + i) for i, d in enumerate((2, 8, 64))]
+    recs = [autotune.profile_closure("min_plus", torch.from_numpy(g).to(cuda)) for g in train_graphs]
+    Xd, yd = autotune.dataset(recs)
+    params, losses = costmodel.train(Xd.to(cuda), yd.to(cuda), steps=1500)
+    assert losses[-1] < losses[0]
+    t_dense = t_learned = 0.0
+    for i, d in enumerate((3, 16)):
+        g = datagen.rmat_graph(4096, d, seed=100 + i)
+        Xa = torch.from_numpy(g.copy()).to(cuda)
+        Xb = torch.from_numpy(g.copy()).to(cuda)
+        ra = s2.closure_ex("min_plus", Xa, dispatch="dense", record=True)
+        rb = s2.closure_ex("min_plus", Xb, dispatch="learned", mlp_params=params, record=True)
+        assert ra["iters"] == rb["iters"]
+        assert torch.equal(Xa.view(torch.int32), Xb.view(torch.int32))
+        t_dense += sum(ra["ms"])
+        t_learned += sum(rb["ms"])
+    assert t_learned <= 1.05 * t_dense, (t_learned, t_dense)
