@@ -56,6 +56,9 @@ def parse_args():
                    help="rows per semiring in the CPU sample (one per host core)")
     p.add_argument("--ops", default=",".join(SWEEP_OPS),
                    help="comma-separated subset of the sweep (profiling runs use one semiring)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the batched-closure / learned-dispatch / APSP-512 measurements")
+    p.add_argument("--batched-count", type=int, default=4096)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -204,6 +207,97 @@ def traffic_from_profile():
         return None
 
 
+def extra_measurements(args, dev):
+    """The metric's other two parts, on one GPU: batched APSP graphs/s against
+    per-graph launches, and the learned dispatch against the plain dense path
+    (plus the N=512 ER APSP closure)."""
+    import torch
+
+    import simd2_b200 as s2
+    from simd2_b200 import costmodel, datagen
+
+    out = {}
+    # --- plain APSP, directed ER N=512 p=0.05 (weights 1..100), closure to fixed point
+    x = torch.from_numpy(datagen.er_graph(512, 0.05, seed=1)).to(dev)
+    res = {}
+    weights = os.path.join(ROOT, "simd2_b200", "costmodel_weights.json")
+    params = costmodel.load(weights, dev) if os.path.exists(weights) else None
+    for mode in ("dense", "learned") if params is not None else ("dense",):
+        X = x.clone()
+        s2.closure_ex("min_plus", X, dispatch=mode, mlp_params=params)  # warm-up
+        best = None
+        for _ in range(5):
+            X = x.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = s2.closure_ex("min_plus", X, dispatch=mode, mlp_params=params, record=True)
+            dt = (time.perf_counter() - t0) * 1e3
+            best = dt if best is None else min(best, dt)
+        res[mode] = {"ms": best, "iters": r["iters"], "configs": [s2.config_desc(c) for c in r["configs"]],
+                     "gops": 2.0 * 512 ** 3 * r["iters"] / best / 1e6}
+    out["apsp_er512"] = res
+
+    # --- batched closure: graphs with N log-uniform in [32,1024], p in U[0.01,0.3]
+    graphs = datagen.batched_graphs(args.batched_count, 32, 1024, seed=3)
+    mats = [torch.from_numpy(g).to(dev) for g in graphs]
+    origs = [m.clone() for m in mats]
+    plan = s2.BatchedClosure("min_plus", mats)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for _ in range(3):
+        for m, o in zip(mats, origs):
+            m.copy_(o)
+        torch.cuda.synchronize()
+        ev0.record()
+        plan.run()
+        ev1.record()
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    its, nc = plan.iters()
+    plan.close()
+    bms = min(times)
+    ops = sum(2.0 * g.shape[0] ** 3 * it for g, it in zip(graphs, its))
+    for m, o in zip(mats, origs):
+        m.copy_(o)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    its_plain = [s2.closure("min_plus", m) for m in mats]
+    torch.cuda.synchronize()
+    pms = (time.perf_counter() - t0) * 1e3
+    out["batched_apsp"] = {
+        "graphs": len(graphs), "batched_ms": bms, "graphs_per_s": len(graphs) / bms * 1e3,
+        "gops_dense_equivalent": ops / bms / 1e6, "plain_ms": pms, "plain_graphs_per_s": len(graphs) / pms * 1e3,
+        "speedup_vs_plain": pms / bms, "iterations_match_plain": its == its_plain, "not_converged": nc,
+        "how": "one persistent launch (CUDA events) vs simd2_closure per graph (wall clock, host loop)"}
+    del mats, origs
+
+    # --- learned dispatch on mixed-density R-MAT (a=.57 b=.19 c=.19), vs the plain dense path
+    if params is not None:
+        rows = []
+        td = tl = 0.0
+        identical = True
+        for i, (n, d) in enumerate([(4096, 4), (4096, 64), (4096, 1024), (8192, 4), (8192, 64), (8192, 1024)]):
+            g = torch.from_numpy(datagen.rmat_graph(n, d, seed=500 + i)).to(dev)
+            Xa, Xb = g.clone(), g.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ra = s2.closure_ex("min_plus", Xa, dispatch="dense", record=True)
+            t1 = time.perf_counter()
+            rb = s2.closure_ex("min_plus", Xb, dispatch="learned", mlp_params=params, record=True)
+            t2 = time.perf_counter()
+            same = bool(torch.equal(Xa.view(torch.int32), Xb.view(torch.int32))) and ra["iters"] == rb["iters"]
+            identical &= same
+            td += (t1 - t0) * 1e3
+            tl += (t2 - t1) * 1e3
+            rows.append({"n": n, "degree": d, "iters": ra["iters"], "dense_ms": (t1 - t0) * 1e3,
+                         "learned_ms": (t2 - t1) * 1e3, "learned_configs": [s2.config_desc(c) for c in rb["configs"]]})
+            del g, Xa, Xb
+        out["learned_dispatch"] = {"graphs": rows, "dense_ms": td, "learned_ms": tl, "speedup": td / tl,
+                                   "outputs_identical": identical,
+                                   "how": "wall clock of simd2_closure_ex per graph, dense vs learned"}
+    return out
+
+
 def main():
     global SWEEP_OPS
     args = parse_args()
@@ -350,6 +444,10 @@ def main():
         cpu = {"value": o / s_ / 1e9, "unit": "Gop/s", "cores": threads, "kind": kind,
                "sample": f"{args.ref_rows} rows x {n} x {n} per semiring, all nine semirings, one sweep"}
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = extra_measurements(args, dev)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Gop/s", "n_gpus": world, "steps": args.steps,
@@ -370,6 +468,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -18,11 +18,26 @@ import torch
 from . import NUM_CONFIGS, closure_ex, config_desc
 
 
+_warm = set()
+
+
+def warm_up(op: str, device) -> None:
+    """Loads every configuration's kernel once so no timing includes module loading."""
+    if (op, str(device)) in _warm:
+        return
+    from .datagen import rmat_graph
+    g = torch.from_numpy(rmat_graph(256, 4.0, seed=0)).to(device)
+    for cfg in range(NUM_CONFIGS):
+        closure_ex(op, g.clone(), dispatch="fixed", config=cfg)
+    _warm.add((op, str(device)))
+
+
 def profile_closure(op: str, X0: torch.Tensor, configs=range(NUM_CONFIGS), repeats: int = 1, max_iter: int = 500):
     """Per-step timings of every configuration on one input matrix.
 
     Returns {"n", "iters", "features": [step][7], "ms": {config: [step]}}.
     """
+    warm_up(op, X0.device)
     rec = {"n": int(X0.shape[0]), "ms": {}}
     for cfg in configs:
         best = None
