@@ -173,6 +173,39 @@ int simd2_mlp_gradient(const float* params, const float* X, const float* y, int 
 int simd2_mlp_adam(float* params, const float* grad, float* m, float* v, float lr, int step,
                    cudaStream_t stream);
 
+/* k nearest neighbours, the PLD tail of the reference
+ * (apps/pld/cuASR/knncuda.cu:479-514: minus_square srgemm, then
+ * modified_insertion_sort_linear and compute_sqrt_linear).
+ * query [Q][D] (pitch ldq) and ref [R][D] (pitch ldr), row-major, device.
+ * Writes, per query, the k smallest Euclidean distances (sqrt of the
+ * minus_square sum, ascending) and the reference indices into out_dist /
+ * out_idx [Q][k] (pitch ldo) -- query-major, the transpose of the
+ * reference's k x Q layout.  Equal distances keep the lower index first.
+ * 1 <= k <= 32, R <= 2^21.  Squared distances come from the BF16 hi/lo
+ * tensor-core path with FP64 norms and the exact FP32 recompute inside the
+ * cancellation band (near-duplicate points). */
+int simd2_knn(const float* query, int Q, int ldq, const float* ref, int R, int ldr, int D, int k,
+              float* out_dist, int32_t* out_idx, int ldo, cudaStream_t stream);
+
+/* srgemm with FP16 A and B (row-major, __half*), FP32 C and D: the entry
+ * behind tensor_srgemm (kernel/tensor_srgemm.cuh:197-218).  The halves are
+ * widened to FP32 exactly and the FP32 engine runs; or_and treats any
+ * nonzero as true and writes 0/1.  (The reference's FP16 emulation kernel
+ * rounds each product to FP16 and starts the max semirings from 0; this
+ * entry keeps FP32 products and the true identities.) */
+int simd2_srgemm_f16(simd2_op op, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
+                     const float* C, int ldc, float* D, int ldd, int do_epilogue, cudaStream_t stream);
+
+/* The change test of the reference's closure loop (comp_update /
+ * comp_update2, kernel/converge.cuh:16-84) as one call: compares prev and
+ * cur (M x N, dense) under `mode` (SIMD2_CONV_TOL = comp_update,
+ * SIMD2_CONV_APLP = comp_update2, which also rewrites cur; SIMD2_CONV_EXACT =
+ * bitwise), copies cur into prev and returns *changed_out = 0/1.
+ * Synchronous, like the reference. */
+int simd2_compare_update(float* prev, float* cur, int M, int N, simd2_conv mode, int* changed_out,
+                         cudaStream_t stream);
+int simd2_compare_update_i32(int32_t* prev, int32_t* cur, int M, int N, int* changed_out, cudaStream_t stream);
+
 /* Reserve the per-(device, stream) workspace for srgemm calls up to
  * M x N x K so that later calls (e.g. inside stream capture) allocate
  * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */

@@ -75,6 +75,8 @@ def lib() -> ctypes.CDLL:
         L.simd2_batched_plan_iters.argtypes = [P, PI, PI]
         L.simd2_batched_plan_destroy.argtypes = [P]
         L.simd2_closure_batched.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, PI, P]
+        L.simd2_knn.argtypes = [P, I, I, P, I, I, I, I, P, P, I, P]
+        L.simd2_knn.restype = I
         L.simd2_launch_count.argtypes = []
         L.simd2_launch_count.restype = ctypes.c_longlong
         L.simd2_profile_begin.argtypes = []
@@ -281,6 +283,24 @@ def closure_batched(op: str, mats, max_iter: int = 500, conv: str = "exact", str
     rc = lib().simd2_closure_batched(OP_ID[op], count, ptrs, ns, lds, max_iter, CONV[conv], it, _stream(stream))
     _check(rc, f"closure_batched({op})")
     return list(it)[:count]
+
+
+def knn(query: torch.Tensor, ref: torch.Tensor, k: int, stream=None):
+    """k nearest references of every query (Euclidean): (dist [Q,k] float32, idx [Q,k] int32).
+
+    Mirrors the PLD path of the reference (minus_square srgemm, insertion-sort
+    top-k, sqrt); outputs are query-major.
+    """
+    Q, D = query.shape
+    R, D2 = ref.shape
+    if D != D2:
+        raise ValueError("query and ref dimensions differ")
+    dist = torch.empty((Q, k), dtype=torch.float32, device=query.device)
+    idx = torch.empty((Q, k), dtype=torch.int32, device=query.device)
+    rc = lib().simd2_knn(query.data_ptr(), Q, _mat(query, "query"), ref.data_ptr(), R, _mat(ref, "ref"), D, k,
+                         dist.data_ptr(), idx.data_ptr(), k, _stream(stream))
+    _check(rc, "knn")
+    return dist, idx
 
 
 def device_status() -> int:

@@ -19,6 +19,7 @@
 #include "tc_gemm.cuh"
 #include "closure_batched.cuh"
 #include "mlp.cuh"
+#include "knn.cuh"
 
 namespace simd2 {
 namespace {
@@ -1176,6 +1177,214 @@ int simd2_mlp_adam(float* params, const float* grad, float* m, float* v, float l
 }
 
 }  // extern "C"
+
+
+// ---------------------------------------------------------------------------
+// k nearest neighbours (PLD): minus_square on the tensor cores per query
+// chunk, then a warp-per-row top-k with sqrt.
+// ---------------------------------------------------------------------------
+namespace simd2 {
+namespace {
+
+template <int KT>
+int knn_topk_launch(const float* dist, long long ldd, int rows, int cols, float* od, int32_t* oi, long long ldo,
+                    int kout, cudaStream_t stream) {
+  knn_topk_kernel<KT><<<grid_for((long long)rows * 32, 256), 256, 0, stream>>>(dist, ldd, rows, cols, 0, od, oi, ldo,
+                                                                               kout, 1);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+// Query rows per chunk so that one chunk's distance block stays near 1 GiB.
+int knn_chunk_rows(int Q, int R) {
+  long long rows = (1LL << 30) / (4LL * std::max(R, 1));
+  rows = std::max(128LL, rows / 128 * 128);
+  return (int)std::min<long long>(rows, round_up(Q, 128));
+}
+
+}  // namespace
+}  // namespace simd2
+
+extern "C" int simd2_knn(const float* query, int Q, int ldq, const float* ref, int R, int ldr, int D, int k,
+                         float* out_dist, int32_t* out_idx, int ldo, cudaStream_t stream) {
+  using namespace simd2;
+  if (Q < 0 || R < 0 || D < 0 || k < 1 || k > kKnnMaxK || ldo < k) return SIMD2_ERR_INVALID_ARG;
+  if (Q == 0) return SIMD2_OK;
+  if (!query || !out_dist || !out_idx || ldq < D || (R > 0 && (!ref || ldr < D)) || R > (1 << 21) || D == 0)
+    return SIMD2_ERR_INVALID_ARG;
+  int rc = check_device();
+  if (rc) return rc;
+  if (R == 0) {
+    // no reference points: +inf distances, index -1
+    fill_kernel<float><<<grid_for((long long)Q * k), 256, 0, stream>>>(out_dist, ldo, Q, k, __builtin_inff());
+    fill_kernel<int32_t><<<grid_for((long long)Q * k), 256, 0, stream>>>(out_idx, ldo, Q, k, -1);
+    count_launch();
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    return SIMD2_OK;
+  }
+  const int Dp = round_up(D, 8);
+  const int Qc = knn_chunk_rows(Q, R);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
+  const size_t qhi = take((size_t)Q * Dp * 2), qlo = take((size_t)Q * Dp * 2);
+  const size_t rhi = take((size_t)R * Dp * 2), rlo = take((size_t)R * Dp * 2);
+  const size_t nq = take((size_t)Q * 4), nr = take((size_t)R * 4);
+  const size_t dch = take((size_t)Qc * R * 4);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, off, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  auto* q_hi = reinterpret_cast<__nv_bfloat16*>(ws + qhi);
+  auto* q_lo = reinterpret_cast<__nv_bfloat16*>(ws + qlo);
+  auto* r_hi = reinterpret_cast<__nv_bfloat16*>(ws + rhi);
+  auto* r_lo = reinterpret_cast<__nv_bfloat16*>(ws + rlo);
+  float* n_q = reinterpret_cast<float*>(ws + nq);
+  float* n_r = reinterpret_cast<float*>(ws + nr);
+  float* dist = reinterpret_cast<float*>(ws + dch);
+  split_rows_bf16_kernel<<<grid_for((long long)Q * Dp), 256, 0, stream>>>(query, ldq, Q, D, q_hi, q_lo, Dp);
+  split_rows_bf16_kernel<<<grid_for((long long)R * Dp), 256, 0, stream>>>(ref, ldr, R, D, r_hi, r_lo, Dp);
+  row_norms_kernel<<<grid_for((long long)Q * 32), 256, 0, stream>>>(query, ldq, Q, D, n_q);
+  row_norms_kernel<<<grid_for((long long)R * 32), 256, 0, stream>>>(ref, ldr, R, D, n_r);
+  for (int i = 0; i < 4; i++) count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  const auto BF = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  const auto SW = CU_TENSOR_MAP_SWIZZLE_128B;
+  CUtensorMap mb0, mb1;
+  if ((rc = make_map_2d(&mb0, BF, 2, r_hi, R, Dp, Dp, 64, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&mb1, BF, 2, r_lo, R, Dp, Dp, 64, kTcBN, SW))) return rc;
+  for (int q0 = 0; q0 < Q; q0 += Qc) {
+    const int rows = std::min(Qc, Q - q0);
+    CUtensorMap ma0, ma1;
+    if ((rc = make_map_2d(&ma0, BF, 2, q_hi + (size_t)q0 * Dp, rows, Dp, Dp, 64, kTcBM, SW))) return rc;
+    if ((rc = make_map_2d(&ma1, BF, 2, q_lo + (size_t)q0 * Dp, rows, Dp, Dp, 64, kTcBM, SW))) return rc;
+    TcEpilogue ep{};
+    ep.op = SIMD2_MINUS_SQUARE;
+    ep.do_epilogue = 0;
+    ep.C = dist;
+    ep.ldc = R;
+    ep.D = dist;
+    ep.ldd = R;
+    ep.norm_a = n_q + q0;
+    ep.norm_b = n_r;
+    ep.A32 = query + (size_t)q0 * ldq;
+    ep.lda32 = ldq;
+    ep.B32 = ref;
+    ep.ldb32 = ldr;
+    ep.b_rows = 1;
+    ep.K = D;
+    ep.band = kMinusSquareBand;
+    if ((rc = launch_tc<0>(rows, R, D, ma0, ma1, mb0, mb1, ep, stream))) return rc;
+    float* od = out_dist + (size_t)q0 * ldo;
+    int32_t* oi = out_idx + (size_t)q0 * ldo;
+    if (k <= 4) rc = knn_topk_launch<4>(dist, R, rows, R, od, oi, ldo, k, stream);
+    else if (k <= 8) rc = knn_topk_launch<8>(dist, R, rows, R, od, oi, ldo, k, stream);
+    else if (k <= 16) rc = knn_topk_launch<16>(dist, R, rows, R, od, oi, ldo, k, stream);
+    else rc = knn_topk_launch<32>(dist, R, rows, R, od, oi, ldo, k, stream);
+    if (rc) return rc;
+  }
+  return SIMD2_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// compatibility entries: FP16-input srgemm (tensor_srgemm) and the
+// convergence test (comp_update / comp_update2)
+// ---------------------------------------------------------------------------
+extern "C" int simd2_srgemm_f16(simd2_op op, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
+                                const float* C, int ldc, float* D, int ldd, int do_epilogue, cudaStream_t stream) {
+  using namespace simd2;
+  if ((int)op < 0 || (int)op > 8) return SIMD2_ERR_INVALID_ARG;
+  int rc = check_dims(M, N, K, lda, ldb, ldc, ldd, A, B, C, D, do_epilogue);
+  if (rc || M == 0 || N == 0) return rc;
+  if ((rc = check_device())) return rc;
+  // or_and on {0,1}: the max_min semiring on booleans (AND = min, OR = max)
+  const bool boolean = op == SIMD2_OR_AND;
+  const int run_op = boolean ? SIMD2_MAX_MIN : op;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(std::max(bytes, (size_t)4), kAlign); return o; };
+  const size_t a_off = take((size_t)M * K * 4), b_off = take((size_t)K * N * 4);
+  const size_t c_off = take(boolean && do_epilogue ? (size_t)M * N * 4 : 4);
+  const size_t plan_off = off;
+  const size_t need = is_sum_op(run_op) ? tc_plan_bf16(M, N, K).total : make_plan(M, N, K, false).total;
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, plan_off + need, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  float* Af = reinterpret_cast<float*>(ws + a_off);
+  float* Bf = reinterpret_cast<float*>(ws + b_off);
+  const float* Cuse = C;
+  long long ldc_use = ldc;
+  if (K > 0) {
+    if (boolean) {
+      half_to_float_kernel<1><<<grid_for((long long)M * K), 256, 0, stream>>>(static_cast<const __half*>(A), lda, M, K,
+                                                                              Af);
+      half_to_float_kernel<1><<<grid_for((long long)K * N), 256, 0, stream>>>(static_cast<const __half*>(B), ldb, K, N,
+                                                                              Bf);
+    } else {
+      half_to_float_kernel<0><<<grid_for((long long)M * K), 256, 0, stream>>>(static_cast<const __half*>(A), lda, M, K,
+                                                                              Af);
+      half_to_float_kernel<0><<<grid_for((long long)K * N), 256, 0, stream>>>(static_cast<const __half*>(B), ldb, K, N,
+                                                                              Bf);
+    }
+    count_launch();
+    count_launch();
+  }
+  if (boolean && do_epilogue) {
+    float* Cb = reinterpret_cast<float*>(ws + c_off);
+    float_bool_kernel<<<grid_for((long long)M * N), 256, 0, stream>>>(C, ldc, M, N, Cb);
+    count_launch();
+    Cuse = Cb;
+    ldc_use = N;
+  }
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  rc = srgemm_f32_ws(run_op, M, N, K, Af, K, Bf, N, Cuse, ldc_use, D, ldd, do_epilogue, nullptr, 0, ws + plan_off,
+                     stream);
+  if (rc) return rc;
+  if (boolean && K == 0 && !do_epilogue) {
+    // or_and identity is 0, not max_min's -inf
+    fill_kernel<float><<<grid_for((long long)M * N), 256, 0, stream>>>(D, ldd, M, N, 0.0f);
+    count_launch();
+  }
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+namespace simd2 {
+namespace {
+template <typename T>
+int compare_update(T* prev, T* cur, long long n, int mode, int* changed_out, cudaStream_t stream) {
+  if (!changed_out || n < 0 || (n > 0 && (!prev || !cur))) return SIMD2_ERR_INVALID_ARG;
+  *changed_out = 0;
+  if (n == 0) return SIMD2_OK;
+  int rc = check_device();
+  if (rc) return rc;
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, kAlign, &p))) return rc;  // stream-ordered: the flag word is free
+  int* flag = static_cast<int*>(p);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), stream));
+  compare_update_kernel<T><<<grid_for(n), 256, 0, stream>>>(prev, cur, n, mode, flag);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  int h = 0;
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  *changed_out = h != 0;
+  return SIMD2_OK;
+}
+}  // namespace
+}  // namespace simd2
+
+extern "C" int simd2_compare_update(float* prev, float* cur, int M, int N, simd2_conv mode, int* changed_out,
+                                    cudaStream_t stream) {
+  if (M < 0 || N < 0 || mode < SIMD2_CONV_EXACT || mode > SIMD2_CONV_APLP) return SIMD2_ERR_INVALID_ARG;
+  return simd2::compare_update<float>(prev, cur, (long long)M * N, (int)mode, changed_out, stream);
+}
+
+extern "C" int simd2_compare_update_i32(int32_t* prev, int32_t* cur, int M, int N, int* changed_out,
+                                        cudaStream_t stream) {
+  if (M < 0 || N < 0) return SIMD2_ERR_INVALID_ARG;
+  return simd2::compare_update<int32_t>(prev, cur, (long long)M * N, 0, changed_out, stream);
+}
 
 // ---------------------------------------------------------------------------
 // srgemm without allocation

@@ -1,6 +1,9 @@
 // prep.cuh -- operand preparation kernels (HBM-bound, one pass each).
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -59,6 +62,56 @@ __global__ void fill_kernel(T* D, long long ldd, int M, int N, T value) {
     const int j = (int)(t - (long long)i * N);
     D[(long long)i * ldd + j] = value;
   }
+}
+
+// half -> float (MODE 0) or half -> {0,1} float (MODE 1), [M][K] pitch lda -> dense [M][K].
+template <int MODE>
+__global__ void half_to_float_kernel(const __half* __restrict__ A, long long lda, int M, int K, float* __restrict__ out) {
+  const long long total = (long long)M * K;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / K);
+    const int k = (int)(t - (long long)i * K);
+    const float v = __half2float(A[(long long)i * lda + k]);
+    out[t] = MODE == 1 ? (v != 0.f ? 1.f : 0.f) : v;
+  }
+}
+
+// float -> {0,1} float, [M][N] pitch ldc -> dense.
+__global__ void float_bool_kernel(const float* __restrict__ C, long long ldc, int M, int N, float* __restrict__ out) {
+  const long long total = (long long)M * N;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / N);
+    const int j = (int)(t - (long long)i * N);
+    out[t] = C[(long long)i * ldc + j] != 0.f ? 1.f : 0.f;
+  }
+}
+
+// Change test + copy, the work of comp_update / comp_update2
+// (kernel/converge.cuh:6-84): mode 1 |prev-cur| > 1e-4, mode 2 maps cur values
+// in (-1,1) to -FLT_MAX first (in cur and prev) then tests inequality, mode 0
+// tests bitwise inequality; prev := cur.  One flag word, set by a warp vote.
+template <typename T>
+__global__ void compare_update_kernel(T* __restrict__ prev, T* __restrict__ cur, long long n, int mode,
+                                      int* __restrict__ flag) {
+  int ch = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    T c = cur[t];
+    const T pv = prev[t];
+    if constexpr (std::is_same<T, float>::value) {
+      if (mode == 2 && c > T(-1) && c < T(1)) {
+        c = T(-3.402823466e+38f);
+        cur[t] = c;
+      }
+      if (mode == 1) ch |= fabsf((float)pv - (float)c) > 0.0001f;
+      else ch |= __float_as_uint((float)pv) != __float_as_uint((float)c);
+    } else {
+      ch |= pv != c;
+    }
+    prev[t] = c;
+  }
+  if (__any_sync(0xffffffffu, ch) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
 // D = (C != 0) as 0/1 of type T.

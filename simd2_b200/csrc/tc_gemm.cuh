@@ -136,16 +136,26 @@ struct TcEpilogue {
   long long ldb32;
   int K;
   float band;           // recompute when dist < band * (|a|^2 + |b|^2)
+  int b_rows;           // 1: B32 holds B transposed ([N][K], e.g. k-NN reference points)
   int* changed;         // or_and closure: set to 1 when any D differs from C
 };
 
-__device__ __forceinline__ float exact_minus_square(const float* a, long long lda_unused, const float* B, long long ldb,
-                                                    int col, int K) {
-  (void)lda_unused;
+// sum_k (a[k] - B[k][col])^2 in FP32; B is [K][N] (pitch ldb) or, when
+// b_rows, stored transposed as [N][K].
+__device__ __forceinline__ float exact_minus_square(const float* a, const float* B, long long ldb, int col, int K,
+                                                    int b_rows) {
   float s = 0.f;
-  for (int k = 0; k < K; k++) {
-    const float d = __fsub_rn(a[k], B[(long long)k * ldb + col]);
-    s = __fmaf_rn(d, d, s);
+  if (b_rows) {
+    const float* b = B + (long long)col * ldb;
+    for (int k = 0; k < K; k++) {
+      const float d = __fsub_rn(a[k], b[k]);
+      s = __fmaf_rn(d, d, s);
+    }
+  } else {
+    for (int k = 0; k < K; k++) {
+      const float d = __fsub_rn(a[k], B[(long long)k * ldb + col]);
+      s = __fmaf_rn(d, d, s);
+    }
   }
   return s;
 }
@@ -313,7 +323,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               const float nsum = na + nb;
               v = __fmaf_rn(-2.0f, v, nsum);
               if (v < ep.band * nsum)
-                v = exact_minus_square(ep.A32 + (long long)row * ep.lda32, ep.lda32, ep.B32, ep.ldb32, col, ep.K);
+                v = exact_minus_square(ep.A32 + (long long)row * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows);
             }
             if (ep.do_epilogue) v = __fadd_rn(v, crow[col]);
             drow[col] = v;
