@@ -207,6 +207,47 @@ def traffic_from_profile():
         return None
 
 
+def batched_sharded(args, dev, rank, world):
+    """Batched APSP over `world` ranks: every rank builds the same seeded graph
+    list, closes its size-balanced shard in one persistent launch, and the
+    slowest rank's device time is the job's time (no collective in the data
+    path; only the timing is reduced)."""
+    import torch
+
+    import simd2_b200 as s2
+    from simd2_b200 import datagen
+    from simd2_b200.shard import assign_graphs, max_over_ranks
+
+    graphs = datagen.batched_graphs(args.batched_count, 32, 1024, seed=3)
+    mine = assign_graphs([g.shape[0] for g in graphs], world)[rank]
+    mats = [torch.from_numpy(graphs[g]).to(dev) for g in mine]
+    origs = [m.clone() for m in mats]
+    plan = s2.BatchedClosure("min_plus", mats)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for _ in range(3):
+        for m, o in zip(mats, origs):
+            m.copy_(o)
+        torch.cuda.synchronize()
+        ev0.record()
+        plan.run()
+        ev1.record()
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    its, nc = plan.iters()
+    plan.close()
+    local_ms = min(times)
+    ms = max_over_ranks(local_ms, device=dev) if world > 1 else local_ms
+    ops = sum(2.0 * graphs[g].shape[0] ** 3 * it for g, it in zip(mine, its))
+    if world > 1:
+        ops_t = torch.tensor([ops], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(ops_t)
+        ops = float(ops_t.item())
+    return {"graphs": len(graphs), "n_gpus": world, "batched_ms": ms, "graphs_per_s": len(graphs) / ms * 1e3,
+            "gops_dense_equivalent": ops / ms / 1e6, "not_converged": nc,
+            "how": "one persistent launch per rank on an n^3-balanced shard; max-over-ranks CUDA-event time"}, graphs
+
+
 def extra_measurements(args, dev):
     """The metric's other two parts, on one GPU: batched APSP graphs/s against
     per-graph launches, and the learned dispatch against the plain dense path
@@ -238,38 +279,19 @@ def extra_measurements(args, dev):
     out["apsp_er512"] = res
 
     # --- batched closure: graphs with N log-uniform in [32,1024], p in U[0.01,0.3]
-    graphs = datagen.batched_graphs(args.batched_count, 32, 1024, seed=3)
+    res_b, graphs = batched_sharded(args, dev, 0, 1)
     mats = [torch.from_numpy(g).to(dev) for g in graphs]
-    origs = [m.clone() for m in mats]
-    plan = s2.BatchedClosure("min_plus", mats)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    times = []
-    for _ in range(3):
-        for m, o in zip(mats, origs):
-            m.copy_(o)
-        torch.cuda.synchronize()
-        ev0.record()
-        plan.run()
-        ev1.record()
-        torch.cuda.synchronize()
-        times.append(ev0.elapsed_time(ev1))
-    its, nc = plan.iters()
-    plan.close()
-    bms = min(times)
-    ops = sum(2.0 * g.shape[0] ** 3 * it for g, it in zip(graphs, its))
-    for m, o in zip(mats, origs):
-        m.copy_(o)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    its_plain = [s2.closure("min_plus", m) for m in mats]
+    for m in mats:
+        s2.closure("min_plus", m)
     torch.cuda.synchronize()
     pms = (time.perf_counter() - t0) * 1e3
-    out["batched_apsp"] = {
-        "graphs": len(graphs), "batched_ms": bms, "graphs_per_s": len(graphs) / bms * 1e3,
-        "gops_dense_equivalent": ops / bms / 1e6, "plain_ms": pms, "plain_graphs_per_s": len(graphs) / pms * 1e3,
-        "speedup_vs_plain": pms / bms, "iterations_match_plain": its == its_plain, "not_converged": nc,
-        "how": "one persistent launch (CUDA events) vs simd2_closure per graph (wall clock, host loop)"}
-    del mats, origs
+    res_b.update({"plain_ms": pms, "plain_graphs_per_s": len(graphs) / pms * 1e3,
+                  "speedup_vs_plain": pms / res_b["batched_ms"],
+                  "how": "one persistent launch (CUDA events) vs simd2_closure per graph (wall clock, host loop)"})
+    out["batched_apsp"] = res_b
+    del mats
 
     # --- learned dispatch on mixed-density R-MAT (a=.57 b=.19 c=.19), vs the plain dense path
     if params is not None:
@@ -433,8 +455,20 @@ def main():
     peaks, peak_kind = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     issue_peak_gops = SMS * LANES * sm_max * 1e6 / 1e9  # 2 ops/MAC == 2 lane-instructions/MAC
-    achieved = kt.ops / (kt.kernel_ms / 1e3) / 1e9 if kt.kernel_ms > 0 else None
+    simt_ms, simt_n, simt_ops = kt.by_kind["simt"]
+    tc_ms, tc_n, tc_ops = kt.by_kind["tensor"]
+    achieved = simt_ops / (simt_ms / 1e3) / 1e9 if simt_ms > 0 else None
     traffic = traffic_from_profile()
+    # tensor-core family: plus_mul / minus_square issue 3 BF16 MMAs per product term
+    # (hi*hi, hi*lo, lo*hi), or_and one INT8 MMA at twice the BF16 rate; both are
+    # expressed as BF16-equivalent FLOP/s against the measured cuBLAS BF16 peak.
+    tc_equiv = 0.0
+    for op in SWEEP_OPS:
+        if op in ("plus_mul", "minus_square"):
+            tc_equiv += 3 * 2.0 * n ** 3 * args.steps
+        elif op == "or_and":
+            tc_equiv += 0.5 * 2.0 * n ** 3 * args.steps
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -445,8 +479,15 @@ def main():
                "sample": f"{args.ref_rows} rows x {n} x {n} per semiring, all nine semirings, one sweep"}
 
     extras = {}
-    if rank == 0 and world == 1 and not args.no_extras:
-        extras = extra_measurements(args, dev)
+    if not args.no_extras:
+        if world == 1:
+            extras = extra_measurements(args, dev)
+        else:
+            extras = {"batched_apsp": batched_sharded(args, dev, rank, world)[0]}
+    if world > 1:
+        lt = torch.tensor([launches], dtype=torch.float64, device=dev)
+        dist.all_reduce(lt)
+        launches = int(lt.item())
 
     if rank == 0:
         line = {
@@ -457,12 +498,19 @@ def main():
                        "l2": "inputs larger than L2: 9 semirings x (A,B,C) x 64 MiB rotated every step",
                        "parallelism": f"independent sweep per rank x{world}"},
             "per_semiring_kernel_gops": per_op,
-            "roofline": {"bound": "cuda_core_issue", "kernel": "srgemm_simt_kernel (all semirings)",
+            "roofline": {"bound": "cuda_core_issue",
+                         "kernel": "srgemm_simt_kernel (min_plus, max_plus, max_min, max_mul, min_mul, min_max)",
                          "achieved": achieved, "peak": issue_peak_gops, "unit": "Gop/s",
                          "frac": achieved / issue_peak_gops if achieved else None, "traffic": traffic,
                          "peak_source": f"{SMS} SMs x {LANES} lanes x {sm_max:.0f} MHz ({peak_kind} sm_max_mhz); "
                                         "2 ops per (x),(+) pair = 2 lane-instructions",
-                         "timed_launches": kt.launches},
+                         "share_of_kernel_time": simt_ms / (simt_ms + tc_ms) if simt_ms + tc_ms > 0 else None,
+                         "timed_launches": simt_n},
+            "roofline_tensor": {"bound": "tensor", "kernel": "tc_gemm_kernel (plus_mul, minus_square, or_and)",
+                                "achieved": tc_equiv / (tc_ms / 1e3) / 1e12 if tc_ms > 0 else None,
+                                "peak": bf16_peak, "unit": "TFLOP/s (BF16-equivalent)",
+                                "frac": (tc_equiv / (tc_ms / 1e3) / 1e12) / bf16_peak if tc_ms > 0 else None,
+                                "peak_source": f"{peak_kind} bf16_tflops (cuBLAS burst)", "timed_launches": tc_n},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

@@ -224,6 +224,9 @@ long long simd2_launch_count(void);
  * algorithmic operation count (2*M*N*K per launch). */
 int simd2_profile_begin(void);
 int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops);
+/* After simd2_profile_end: the same totals for one kernel family
+ * (0 = CUDA-core srgemm, 1 = tensor-core srgemm). */
+int simd2_profile_result(int kind, double* kernel_ms, long long* launches, long long* ops);
 
 /* Read and clear the id of the last bounded wait that ran out (0 = none);
  * a diagnostic companion of simd2_device_status(). */

@@ -80,6 +80,9 @@ def lib() -> ctypes.CDLL:
         L.simd2_launch_count.argtypes = []
         L.simd2_launch_count.restype = ctypes.c_longlong
         L.simd2_profile_begin.argtypes = []
+        L.simd2_profile_result.argtypes = [I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                           ctypes.POINTER(ctypes.c_longlong)]
+        L.simd2_profile_result.restype = I
         L.simd2_profile_end.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                         ctypes.POINTER(ctypes.c_longlong)]
         for name in ("simd2_srgemm", "simd2_srgemm_orand_i32", "simd2_srgemm_orand_u8", "simd2_closure",
@@ -325,6 +328,11 @@ class KernelTimer:
         ms, n, ops = ctypes.c_double(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
         _check(lib().simd2_profile_end(ctypes.byref(ms), ctypes.byref(n), ctypes.byref(ops)), "profile_end")
         self.kernel_ms, self.launches, self.ops = ms.value, n.value, ops.value
+        self.by_kind = {}
+        for kind, name in ((0, "simt"), (1, "tensor")):
+            _check(lib().simd2_profile_result(kind, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(ops)),
+                   "profile_result")
+            self.by_kind[name] = (ms.value, n.value, ops.value)
         return False
 
 

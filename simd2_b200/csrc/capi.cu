@@ -64,21 +64,32 @@ std::atomic<long long> g_launches{0};
 std::mutex g_prof_mu;
 bool g_prof_on = false;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
+std::vector<int> g_prof_kind;        // kernel family of each timed launch
+std::vector<long long> g_prof_opsv;  // algorithmic ops of each timed launch
 size_t g_prof_used = 0;
 long long g_prof_ops = 0;
+double g_prof_ms[4] = {};
+long long g_prof_n[4] = {}, g_prof_k_ops[4] = {};
 
 inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+// Kernel families reported separately by simd2_profile_result.
+enum ProfKind { kProfSimt = 0, kProfTensor = 1, kProfBatched = 2 };
+
 // Returns the event pair to bracket a main-kernel launch, or nullptr.
-std::pair<cudaEvent_t, cudaEvent_t>* prof_slot(long long ops) {
+std::pair<cudaEvent_t, cudaEvent_t>* prof_slot(long long ops, int kind = kProfSimt) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   if (!g_prof_on) return nullptr;
   if (g_prof_used == g_prof_events.size()) {
     cudaEvent_t a, b;
     if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return nullptr;
     g_prof_events.push_back({a, b});
+    g_prof_kind.push_back(0);
+    g_prof_opsv.push_back(0);
   }
   g_prof_ops += ops;
+  g_prof_kind[g_prof_used] = kind;
+  g_prof_opsv[g_prof_used] = ops;
   return &g_prof_events[g_prof_used++];
 }
 
@@ -399,7 +410,7 @@ int launch_tc(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1,
   }
   const int tiles_m = (M + kTcBM - 1) / kTcBM;
   const int tiles_n = (N + kTcBN - 1) / kTcBN;
-  auto* ev = prof_slot(2LL * M * N * K);
+  auto* ev = prof_slot(2LL * M * N * K, kProfTensor);
   if (ev) cudaEventRecord(ev->first, stream);
   kern<<<tiles_m * tiles_n, kTcThreads, smem, stream>>>(a0, a1, b0, b1, M, N, K, ep, tiles_m, tiles_n);
   count_launch();
@@ -940,6 +951,16 @@ int simd2_profile_begin(void) {
   g_prof_on = true;
   g_prof_used = 0;
   g_prof_ops = 0;
+  for (int k = 0; k < 4; k++) g_prof_ms[k] = 0.0, g_prof_n[k] = 0, g_prof_k_ops[k] = 0;
+  return SIMD2_OK;
+}
+
+int simd2_profile_result(int kind, double* kernel_ms, long long* launches, long long* ops) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (kind < 0 || kind > 3) return SIMD2_ERR_INVALID_ARG;
+  if (kernel_ms) *kernel_ms = g_prof_ms[kind];
+  if (launches) *launches = g_prof_n[kind];
+  if (ops) *ops = g_prof_k_ops[kind];
   return SIMD2_OK;
 }
 
@@ -953,6 +974,10 @@ int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops) {
     if (cudaEventElapsedTime(&ms, g_prof_events[i].first, g_prof_events[i].second) != cudaSuccess)
       return SIMD2_ERR_CUDA;
     total += ms;
+    const int k = g_prof_kind[i];
+    g_prof_ms[k] += ms;
+    g_prof_n[k] += 1;
+    g_prof_k_ops[k] += g_prof_opsv[i];
   }
   if (kernel_ms) *kernel_ms = total;
   if (launches) *launches = (long long)g_prof_used;
