@@ -59,6 +59,9 @@ def parse_args():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the batched-closure / learned-dispatch / APSP-512 measurements")
     p.add_argument("--batched-count", type=int, default=4096)
+    p.add_argument("--workload", choices=("sweep", "batched"), default="sweep",
+                   help="sweep: the nine-semiring srgemm line (default); batched: only the batched closure "
+                        "(used for profiling runs)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -345,6 +348,14 @@ def main():
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.workload == "batched":
+        res, _ = batched_sharded(args, dev, rank, world)
+        if rank == 0:
+            print(json.dumps({"workload": "batched closure", **res}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
 
     n = args.n
     s2.lib()

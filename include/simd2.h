@@ -146,7 +146,8 @@ int simd2_srgemm_tuned(simd2_op op, int M, int N, int K,
                        int do_epilogue, int config, cudaStream_t stream);
 
 typedef enum simd2_dispatch {
-  SIMD2_DISPATCH_DENSE = 0,   /* split 1, no skip: the plain dense path */
+  SIMD2_DISPATCH_DENSE = 0,   /* no block skipping; split-K chosen from the tile count
+                                 (the plain autotuned dense path) */
   SIMD2_DISPATCH_FIXED = 1,   /* `fixed_config` every step */
   SIMD2_DISPATCH_LEARNED = 2  /* the MLP cost model picks each step's config */
 } simd2_dispatch;

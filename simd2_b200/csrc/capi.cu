@@ -369,14 +369,15 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   const float pad = pad_value(op);
   float* Bp = reinterpret_cast<float*>(ws + plan.bp_off);
   interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 2), 256, 0, stream>>>(
-      B, ldb, K, N, Bp, plan.Kp, plan.Np, pad);
+      B, ldb, K, N, Bp, plan.Kp, plan.Np, pad, ep.gate);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   const void* a_base = A;
   long long a_pitch = lda;
   if (pack_a) {
     float* Ap = reinterpret_cast<float*>(ws + plan.ap_off);
-    pack_rows_kernel<T, MODE><<<grid_for((long long)M * plan.Kp), 256, 0, stream>>>(A, lda, M, K, Ap, plan.Kp, pad);
+    pack_rows_kernel<T, MODE><<<grid_for((long long)M * plan.Kp), 256, 0, stream>>>(A, lda, M, K, Ap, plan.Kp, pad,
+                                                                                    ep.gate);
     count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
     a_base = Ap;
@@ -421,7 +422,7 @@ int launch_tc(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1,
 
 struct TcPlan {
   int Kp;
-  size_t a0, a1, b0, b1, na, nb, total;
+  size_t a0, a1, b0, b1, na, nb, nb64, total;
 };
 
 // bf16 hi/lo operands (plus_mul, minus_square)
@@ -436,6 +437,7 @@ TcPlan tc_plan_bf16(int M, int N, int K) {
   p.b1 = take((size_t)N * p.Kp * 2);
   p.na = take((size_t)M * 4);
   p.nb = take((size_t)N * 4);
+  p.nb64 = take((size_t)N * 8);
   p.total = off;
   return p;
 }
@@ -450,7 +452,7 @@ TcPlan tc_plan_u8(int M, int N, int K) {
   p.b0 = take((size_t)N * p.Kp);
   p.a1 = p.a0;
   p.b1 = p.b0;
-  p.na = p.nb = 0;
+  p.na = p.nb = p.nb64 = 0;
   p.total = off;
   return p;
 }
@@ -466,15 +468,17 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   auto* alo = reinterpret_cast<__nv_bfloat16*>(ws + plan.a1);
   split_rows_bf16_kernel<<<grid_for((long long)M * Kp), 256, 0, stream>>>(A, lda, M, K, ahi, alo, Kp);
   count_launch();
-  dim3 tgrid((N + 31) / 32, (Kp + 31) / 32), tblock(32, 8);
-  transpose_prep_kernel<float, 0><<<tgrid, tblock, 0, stream>>>(B, ldb, K, N, ws + plan.b0, ws + plan.b1, Kp);
-  count_launch();
   float* na = reinterpret_cast<float*>(ws + plan.na);
   float* nb = reinterpret_cast<float*>(ws + plan.nb);
+  double* nb64 = op == SIMD2_MINUS_SQUARE ? reinterpret_cast<double*>(ws + plan.nb64) : nullptr;
+  if (nb64) SIMD2_CUDA_TRY(cudaMemsetAsync(nb64, 0, sizeof(double) * N, stream));
+  dim3 tgrid((N + 31) / 32, (Kp + 31) / 32), tblock(32, 8);
+  transpose_prep_kernel<float, 0><<<tgrid, tblock, 0, stream>>>(B, ldb, K, N, ws + plan.b0, ws + plan.b1, Kp, nb64);
+  count_launch();
   if (op == SIMD2_MINUS_SQUARE) {
     row_norms_kernel<<<grid_for((long long)M * 32), 256, 0, stream>>>(A, lda, M, K, na);
     count_launch();
-    col_norms_kernel<<<grid_for(N), 256, 0, stream>>>(B, ldb, K, N, nb);
+    round_norms_kernel<<<grid_for(N), 256, 0, stream>>>(nb64, N, nb);
     count_launch();
   }
   SIMD2_CUDA_TRY(cudaGetLastError());
@@ -634,8 +638,106 @@ int srgemm_orand(int M, int N, int K, const T* A, long long lda, const T* B, lon
 // ---------------------------------------------------------------------------
 namespace {
 
+// Split-K factor of the dense path: the largest power of two (at most 4)
+// with tiles * split <= SM count, so small problems still fill the GPU.
+int dense_split(int n, int sms) {
+  const long long tiles = (long long)((n + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
+  int s = 1;
+  while (s < 4 && tiles * s * 2 <= sms) s *= 2;
+  return s;
+}
+
+// Closure steps enqueued in chunks without a host round trip per step.
+// changed[t] is written by step t; every kernel of step t+1 reads changed[t]
+// as its gate and does nothing when it is 0, so steps enqueued past the fixed
+// point cost only their launches.  The host reads the chunk's flags once.
+int closure_gated(int op, int n, float* X, long long ldx, int max_iter, int conv, int fixed_cfg, bool fixed,
+                  bool can_skip, bool need_occ, const OccPlan& occ, uint8_t* ws, size_t x_off, int* changed,
+                  uint8_t* obase, int* iters_out, int* step_cfg, float* step_ms, int sms, cudaStream_t stream) {
+  int rc = SIMD2_OK;
+  const int auto_split = dense_split(n, sms);
+  float* bufs[2] = {X, reinterpret_cast<float*>(ws + x_off)};
+  const long long lds[2] = {ldx, n};
+  SIMD2_CUDA_TRY(cudaMemsetAsync(changed, 0, (size_t)(max_iter + 1) * sizeof(int), stream));
+  std::vector<cudaEvent_t> evs;
+  int done_at = -1;  // step index whose flag was 0 (converged), -1 while running
+  int enq = 0;
+  int chunk = 4;
+  std::vector<int> h(max_iter);
+  while (done_at < 0 && enq < max_iter && rc == SIMD2_OK) {
+    const int first = enq;
+    const int last = std::min(max_iter, enq + chunk);
+    for (int t = first; t < last; t++) {
+      float* cur = bufs[t & 1];
+      float* nxt = bufs[(t + 1) & 1];
+      const long long ldcur = lds[t & 1], ldnxt = lds[(t + 1) & 1];
+      const int* gate = t > 0 ? changed + (t - 1) : nullptr;
+      if (step_ms) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        evs.push_back(a);
+        evs.push_back(b);
+        cudaEventRecord(a, stream);
+      }
+      SimtConfig cfg;
+      cfg.split = fixed ? config_split(fixed_cfg) : auto_split;
+      cfg.skip = fixed && config_skip(fixed_cfg) && can_skip && need_occ;
+      if (cfg.skip) {
+        // occupancy of a gated-off step is harmless work on an unchanged matrix
+        if ((rc = compute_occupancy(op, n, n, n, cur, ldcur, cur, ldcur, true, obase, occ, stream))) break;
+        cfg.occA = obase + occ.occA;
+        cfg.occB = obase + occ.occB;
+      }
+      if (step_cfg) step_cfg[t] = (cfg.skip ? 4 : 0) | (cfg.split == 1 ? 0 : cfg.split == 2 ? 1 : cfg.split == 4 ? 2 : 3);
+      const bool pk = !a_tma_ok(cur, ldcur);
+      const Plan pl = make_plan(n, n, n, pk);
+      EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, changed + t, conv);
+      ep.gate = gate;
+      if ((rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream, cfg))) break;
+      if (step_ms) cudaEventRecord(evs.back(), stream);
+    }
+    if (rc) break;
+    enq = last;
+    if (cudaMemcpyAsync(h.data() + first, changed + first, sizeof(int) * (last - first), cudaMemcpyDeviceToHost,
+                        stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+      rc = SIMD2_ERR_CUDA;
+      break;
+    }
+    for (int t = first; t < last; t++)
+      if (h[t] == 0) {
+        done_at = t;
+        break;
+      }
+    chunk = std::min(chunk * 2, 64);
+  }
+  const int iters = done_at >= 0 ? done_at + 1 : enq;
+  if (rc == SIMD2_OK) {
+    // result of the last executed step t = iters - 1 is in bufs[iters & 1]
+    float* res = bufs[iters & 1];
+    if (res != X)
+      rc = cudaMemcpy2DAsync(X, ldx * 4, res, lds[iters & 1] * 4, (size_t)n * 4, n, cudaMemcpyDeviceToDevice,
+                             stream) == cudaSuccess
+               ? SIMD2_OK
+               : SIMD2_ERR_CUDA;
+  }
+  if (cudaStreamSynchronize(stream) != cudaSuccess && rc == SIMD2_OK) rc = SIMD2_ERR_CUDA;
+  if (step_ms) {
+    for (int t = 0; t < iters && 2 * t + 1 < (int)evs.size(); t++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, evs[2 * t], evs[2 * t + 1]);
+      step_ms[t] = ms;
+    }
+    for (auto e : evs) cudaEventDestroy(e);
+  }
+  if (rc) return rc;
+  if (iters_out) *iters_out = iters;
+  return done_at >= 0 ? SIMD2_OK : SIMD2_ERR_NOT_CONVERGED;
+}
+
 // Closure by repeated squaring with a per-step kernel configuration:
-//   dispatch 0 (dense)  : split 1, no skip (the plain path);
+//   dispatch 0 (dense)  : no skip, split-K from the tile count (the plain path);
 //   dispatch 1 (fixed)  : `fixed_cfg` (split = 1 << (cfg & 3), skip = cfg >> 2) every step;
 //   dispatch 2 (learned): block occupancy of X_t -> features -> the MLP
 //                         `mlp_params` predicts each configuration's time and
@@ -669,7 +771,8 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   const OccPlan occ = make_occ_plan(n, n, n, true);
   const size_t x_off = align_up(plan.total, kAlign);
   const size_t f_off = x_off + align_up((size_t)n * n * 4, kAlign);
-  const size_t o_off = f_off + kAlign;
+  // flag word + learned decision (256 bytes), then one change flag per step
+  const size_t o_off = f_off + align_up(256 + (size_t)(max_iter + 1) * sizeof(int), kAlign);
   const size_t total = o_off + (need_occ ? align_up(occ.total, kAlign) : 0);
   void* p = nullptr;
   if ((rc = get_workspace(stream, total, &p))) return rc;
@@ -679,6 +782,11 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   int* decision = flag + 8;  // [0] config, [1..8] predictions
   uint8_t* obase = ws + o_off;
 
+  if (dispatch != 2 && step_feat == nullptr) {
+    return closure_gated(op, n, X, ldx, max_iter, conv, fixed_cfg, dispatch == 1, can_skip, need_occ, occ, ws,
+                         x_off, reinterpret_cast<int*>(ws + f_off + 256), obase, iters_out, step_cfg, step_ms, sms,
+                         stream);
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (step_ms) {
     SIMD2_CUDA_TRY(cudaEventCreate(&e0));
@@ -692,7 +800,8 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   int changed = 1;
   while (changed && it < max_iter) {
     if (e0) cudaEventRecord(e0, stream);
-    int cfg_id = dispatch == 1 ? fixed_cfg : 0;
+    const int ds = dense_split(n, sms);
+    int cfg_id = dispatch == 1 ? fixed_cfg : (ds == 1 ? 0 : ds == 2 ? 1 : 2);
     SimtConfig cfg;
     if (need_occ) {
       rc = compute_occupancy(op, n, n, n, cur, ldcur, cur, ldcur, true, obase, occ, stream);

@@ -20,7 +20,9 @@ __device__ __forceinline__ float load_operand(const T* p) {
 
 template <typename T, int MODE>
 __global__ void interleave_pairs_kernel(const T* __restrict__ B, long long ldb, int K, int N,
-                                        float* __restrict__ Bp, int Kp, int Np, float pad) {
+                                        float* __restrict__ Bp, int Kp, int Np, float pad,
+                                        const int* gate = nullptr) {
+  if (gate && *gate == 0) return;
   const long long pairs_j = Np / 2;
   const long long total = (long long)(Kp / 2) * pairs_j;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
@@ -42,7 +44,8 @@ __global__ void interleave_pairs_kernel(const T* __restrict__ B, long long ldb, 
 // must be converted (or_and inputs).
 template <typename T, int MODE>
 __global__ void pack_rows_kernel(const T* __restrict__ A, long long lda, int M, int K, float* __restrict__ Ap,
-                                 int Kp, float pad) {
+                                 int Kp, float pad, const int* gate = nullptr) {
+  if (gate && *gate == 0) return;
   const long long total = (long long)M * Kp;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
@@ -187,9 +190,11 @@ __global__ void bool_rows_u8_kernel(const T* __restrict__ A, long long lda, int 
 // B [K][N] (pitch ldb) -> transposed K-major [N][Kp] through a 32 x 32 shared
 // tile (coalesced reads along n, coalesced writes along k).
 // MODE 0: BF16 hi/lo split (out0 = hi, out1 = lo); MODE 1: bytes {0,1} (out0).
+// colsq (nullable): sum over k of B[k][j]^2 accumulated in FP64 (atomicAdd per
+// 32-row tile; the caller zeroes it and rounds it to float afterwards).
 template <typename T, int MODE>
 __global__ void transpose_prep_kernel(const T* __restrict__ B, long long ldb, int K, int N, void* __restrict__ out0,
-                                      void* __restrict__ out1, int Kp) {
+                                      void* __restrict__ out1, int Kp, double* __restrict__ colsq = nullptr) {
   __shared__ float tile[32][33];
   const int k0 = blockIdx.y * 32;
   const int j0 = blockIdx.x * 32;
@@ -204,6 +209,14 @@ __global__ void transpose_prep_kernel(const T* __restrict__ B, long long ldb, in
     tile[i][threadIdx.x] = v;
   }
   __syncthreads();
+  if (colsq != nullptr && threadIdx.y == 0 && j0 + (int)threadIdx.x < N) {
+    double s = 0.0;
+    for (int i = 0; i < 32; i++) {
+      const double v = tile[i][threadIdx.x];
+      s += v * v;
+    }
+    atomicAdd(colsq + j0 + threadIdx.x, s);
+  }
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
     const int j = j0 + i, k = k0 + threadIdx.x;
     if (j < N && k < Kp) {
@@ -233,6 +246,11 @@ __global__ void row_norms_kernel(const float* __restrict__ A, long long lda, int
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (threadIdx.x % 32 == 0) out[i] = (float)s;
   }
+}
+
+// double -> float (norms accumulated in FP64).
+__global__ void round_norms_kernel(const double* __restrict__ in, int n, float* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) out[j] = (float)in[j];
 }
 
 // Squared column norms of B [K][N], accumulated in FP64, rounded to float.

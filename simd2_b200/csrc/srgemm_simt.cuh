@@ -84,6 +84,8 @@ struct EpilogueArgs {
   int vec2;       // C/D rows are 8-byte aligned: use float2 accesses
   int* changed;   // nullable: set to 1 when any D element differs from C
   int conv_mode;  // simd2_conv, used with `changed`
+  const int* gate;  // nullable: when *gate == 0 the kernel does nothing (closure
+                    // step enqueued after the fixed point was reached)
 };
 
 __device__ __forceinline__ bool conv_changed(int mode, float old_v, float new_v) {
@@ -135,6 +137,9 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     srgemm_simt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M,
                        int N, int K, EpilogueArgs ep, int tiles_m, int tiles_n, const uint8_t* __restrict__ occA,
                        const uint8_t* __restrict__ occB) {
+  // A closure step enqueued after the previous step reported no change does
+  // nothing; every CTA (every cluster member) sees the same word.
+  if (ep.gate && *ep.gate == 0) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
