@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <atomic>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -193,10 +194,13 @@ struct Plan {
   int Kp, Np;
   size_t bp_off, bp_bytes;  // interleaved B'
   size_t ap_off, ap_bytes;  // packed A (0 when TMA reads A in place)
+  int Kh;                   // FP16 selection path: K padded to 64 (0 = path off)
+  size_t ah_off, bh_off, flag_off;
   size_t total;
 };
 
-Plan make_plan(int M, int N, int K, bool pack_a) {
+// `half` reserves the FP16 selection path's operands (max_min / min_max).
+Plan make_plan(int M, int N, int K, bool pack_a, bool half = false) {
   Plan p{};
   p.Kp = round_up(std::max(K, 1), kBK);
   p.Np = round_up(std::max(N, 1), kBN);
@@ -205,8 +209,17 @@ Plan make_plan(int M, int N, int K, bool pack_a) {
   p.ap_off = p.bp_bytes;
   p.ap_bytes = pack_a ? align_up((size_t)M * p.Kp * 4, kAlign) : 0;
   p.total = p.ap_off + p.ap_bytes;
+  if (half) {
+    p.Kh = round_up(std::max(K, 1), kH2BK);
+    p.ah_off = p.total;
+    p.bh_off = p.ah_off + align_up((size_t)M * p.Kh * 2, kAlign);
+    p.flag_off = p.bh_off + align_up((size_t)(p.Kh / 2) * p.Np * 4, kAlign);
+    p.total = p.flag_off + kAlign;
+  }
   return p;
 }
+
+bool selection_op(int op) { return op == SIMD2_MAX_MIN || op == SIMD2_MIN_MAX; }
 
 bool a_tma_ok(const void* A, long long lda) {
   return (reinterpret_cast<uintptr_t>(A) % 16 == 0) && ((lda * 4) % 16 == 0);
@@ -360,6 +373,56 @@ int compute_occupancy(int op, int M, int N, int K, const float* A, long long lda
   return SIMD2_OK;
 }
 
+// FP16 selection path (max_min / min_max): on the device, check that A and B
+// hold only FP16 values; if so the packed-half kernel runs, else the FP32
+// kernel (both are enqueued, each gated by one of the two flags, so the call
+// stays asynchronous).  Same bits either way.
+int enqueue_half_path(int op, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb,
+                      const EpilogueArgs& ep, uint8_t* ws, const Plan& plan, cudaStream_t stream) {
+  int* flags = reinterpret_cast<int*>(ws + plan.flag_off);
+  auto* Ah = reinterpret_cast<__half*>(ws + plan.ah_off);
+  auto* Bh = reinterpret_cast<__half2*>(ws + plan.bh_off);
+  fp16_flags_init_kernel<<<1, 1, 0, stream>>>(flags);
+  fp16_exact_kernel<<<grid_for((long long)M * K + (long long)K * N), 256, 0, stream>>>(A, lda, M, K, B, ldb, N, flags,
+                                                                                       ep.gate);
+  fp16_flags_finish_kernel<<<1, 1, 0, stream>>>(flags);
+  pack_half_rows_kernel<<<grid_for((long long)M * plan.Kh), 256, 0, stream>>>(A, lda, M, K, Ah, plan.Kh, ep.gate,
+                                                                              flags);
+  interleave_half_kernel<<<grid_for((long long)(plan.Kh / 2) * plan.Np), 256, 0, stream>>>(B, ldb, K, N, Bh, plan.Kh,
+                                                                                            plan.Np, ep.gate, flags);
+  for (int i = 0; i < 5; i++) count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  CUtensorMap mA, mB;
+  int rc = make_map_2d(&mA, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, Ah, M, plan.Kh, plan.Kh, kH2BK, kBM,
+                       CU_TENSOR_MAP_SWIZZLE_128B);
+  if (rc) return rc;
+  rc = make_map_2d(&mB, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, Bh, plan.Kh / 2, plan.Np, plan.Np, kBN, kH2BK / 2,
+                   CU_TENSOR_MAP_SWIZZLE_NONE);
+  if (rc) return rc;
+  EpilogueArgs eh = ep;
+  eh.gate2 = flags;
+  const int tiles_m = (M + kBM - 1) / kBM;
+  const int tiles_n = (N + kBN - 1) / kBN;
+  const size_t smem = simt_smem_bytes(kSimtStages);
+  int dev = 0;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  static bool configured[2][64] = {};
+  const int which = op == SIMD2_MAX_MIN ? 0 : 1;
+  auto kern = op == SIMD2_MAX_MIN ? srgemm_h2_kernel<SIMD2_MAX_MIN> : srgemm_h2_kernel<SIMD2_MIN_MAX>;
+  if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
+  if (!configured[which][dev]) {
+    SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured[which][dev] = true;
+  }
+  auto* ev = prof_slot(2LL * M * N * K);
+  if (ev) cudaEventRecord(ev->first, stream);
+  kern<<<tiles_m * tiles_n, kSimtThreads, smem, stream>>>(mA, mB, M, N, K, eh, tiles_m, tiles_n);
+  count_launch();
+  if (ev) cudaEventRecord(ev->second, stream);
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
 // Core float srgemm with an explicit workspace.  T/MODE describe how A and B
 // are read (float as-is, or any type normalised to {0,1}).
 template <typename T, int MODE>
@@ -368,8 +431,18 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
                 const SimtConfig& cfg = SimtConfig()) {
   const float pad = pad_value(op);
   float* Bp = reinterpret_cast<float*>(ws + plan.bp_off);
+  const int* path_gate = nullptr;  // gates the FP32 path when the FP16 path is enqueued too
+  if constexpr (MODE == 0 && std::is_same<T, float>::value) {
+    if (plan.Kh > 0 && selection_op(op) && cfg.split == 1 && !cfg.skip) {
+      int rc = enqueue_half_path(op, M, N, K, A, lda, B, ldb, ep, ws, plan, stream);
+      if (rc) return rc;
+      path_gate = reinterpret_cast<const int*>(ws + plan.flag_off) + 1;
+    }
+  }
+  EpilogueArgs ep32 = ep;
+  ep32.gate2 = path_gate;
   interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 2), 256, 0, stream>>>(
-      B, ldb, K, N, Bp, plan.Kp, plan.Np, pad, ep.gate);
+      B, ldb, K, N, Bp, plan.Kp, plan.Np, pad, ep.gate, path_gate);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   const void* a_base = A;
@@ -377,7 +450,7 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   if (pack_a) {
     float* Ap = reinterpret_cast<float*>(ws + plan.ap_off);
     pack_rows_kernel<T, MODE><<<grid_for((long long)M * plan.Kp), 256, 0, stream>>>(A, lda, M, K, Ap, plan.Kp, pad,
-                                                                                    ep.gate);
+                                                                                    ep.gate, path_gate);
     count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
     a_base = Ap;
@@ -390,7 +463,7 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   rc = make_map_f32(&mB, Bp, plan.Kp / 2, 2LL * plan.Np, 2LL * plan.Np, 2 * kBN, kBK / 2, CU_TENSOR_MAP_SWIZZLE_NONE,
                     false);
   if (rc) return rc;
-  return dispatch_simt(op, M, N, K, mA, mB, ep, cfg, stream);
+  return dispatch_simt(op, M, N, K, mA, mB, ep32, cfg, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -593,7 +666,9 @@ int srgemm_f32_ws(int op, int M, int N, int K, const float* A, long long lda, co
     return srgemm_tc_sum(op, M, N, K, A, lda, B, ldb, C, ldc, D, ldd, do_epilogue, ws, tp, stream);
   }
   const bool pack_a = !a_tma_ok(A, lda);
-  const Plan plan = make_plan(M, N, K, pack_a);
+  // the FP16 selection path needs workspace beyond the base plan, so it is
+  // only planned when the library provides the workspace itself
+  const Plan plan = make_plan(M, N, K, pack_a, ws_or_null == nullptr && selection_op(op));
   uint8_t* ws = ws_or_null;
   if (!ws) {
     void* p = nullptr;
@@ -691,7 +766,7 @@ int closure_gated(int op, int n, float* X, long long ldx, int max_iter, int conv
       }
       if (step_cfg) step_cfg[t] = (cfg.skip ? 4 : 0) | (cfg.split == 1 ? 0 : cfg.split == 2 ? 1 : cfg.split == 4 ? 2 : 3);
       const bool pk = !a_tma_ok(cur, ldcur);
-      const Plan pl = make_plan(n, n, n, pk);
+      const Plan pl = make_plan(n, n, n, pk, selection_op(op));
       EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, changed + t, conv);
       ep.gate = gate;
       if ((rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream, cfg))) break;
@@ -767,7 +842,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   const bool need_occ = dispatch == 2 || step_feat != nullptr || (dispatch == 1 && config_skip(fixed_cfg) && can_skip);
   // Workspace: [srgemm plan][Xnew n x n][flag + decision][occupancy]
   const bool pack_a = !a_tma_ok(X, ldx) || (n % 4 != 0);
-  const Plan plan = make_plan(n, n, n, pack_a);
+  const Plan plan = make_plan(n, n, n, pack_a, selection_op(op));
   const OccPlan occ = make_occ_plan(n, n, n, true);
   const size_t x_off = align_up(plan.total, kAlign);
   const size_t f_off = x_off + align_up((size_t)n * n * 4, kAlign);
@@ -843,7 +918,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
       break;
     }
     const bool pk = !a_tma_ok(cur, ldcur);
-    const Plan pl = make_plan(n, n, n, pk);
+    const Plan pl = make_plan(n, n, n, pk, selection_op(op));
     const EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, flag, conv);
     rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream, cfg);
     if (rc) break;

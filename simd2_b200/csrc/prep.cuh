@@ -21,8 +21,8 @@ __device__ __forceinline__ float load_operand(const T* p) {
 template <typename T, int MODE>
 __global__ void interleave_pairs_kernel(const T* __restrict__ B, long long ldb, int K, int N,
                                         float* __restrict__ Bp, int Kp, int Np, float pad,
-                                        const int* gate = nullptr) {
-  if (gate && *gate == 0) return;
+                                        const int* gate = nullptr, const int* gate2 = nullptr) {
+  if ((gate && *gate == 0) || (gate2 && *gate2 == 0)) return;
   const long long pairs_j = Np / 2;
   const long long total = (long long)(Kp / 2) * pairs_j;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
@@ -44,8 +44,8 @@ __global__ void interleave_pairs_kernel(const T* __restrict__ B, long long ldb, 
 // must be converted (or_and inputs).
 template <typename T, int MODE>
 __global__ void pack_rows_kernel(const T* __restrict__ A, long long lda, int M, int K, float* __restrict__ Ap,
-                                 int Kp, float pad, const int* gate = nullptr) {
-  if (gate && *gate == 0) return;
+                                 int Kp, float pad, const int* gate = nullptr, const int* gate2 = nullptr) {
+  if ((gate && *gate == 0) || (gate2 && *gate2 == 0)) return;
   const long long total = (long long)M * Kp;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
@@ -115,6 +115,73 @@ __global__ void compare_update_kernel(T* __restrict__ prev, T* __restrict__ cur,
     prev[t] = c;
   }
   if (__any_sync(0xffffffffu, ch) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+// ---------------------------------------------------------------------------
+// FP16 selection path (max_min, min_max): gates and operand packing.
+// Both gates must be non-zero (or absent) for a gated kernel to run.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool gates_open(const int* g1, const int* g2) {
+  return (!g1 || *g1 != 0) && (!g2 || *g2 != 0);
+}
+
+// flags[0] = 1 (FP16 path), flags[1] = 0 (FP32 path) before the check.
+__global__ void fp16_flags_init_kernel(int* flags) {
+  flags[0] = 1;
+  flags[1] = 0;
+}
+
+// Clears flags[0] when some entry of A or B is not exactly an FP16 value
+// (round trip float -> half -> float changes its bits, NaN included).
+__global__ void fp16_exact_kernel(const float* __restrict__ A, long long lda, int M, int K,
+                                  const float* __restrict__ B, long long ldb, int N, int* flags, const int* gate) {
+  if (gate && *gate == 0) return;
+  bool bad = false;
+  const long long na = (long long)M * K, nb = (long long)K * N;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < na + nb;
+       t += (long long)gridDim.x * blockDim.x) {
+    float x;
+    if (t < na) {
+      const long long i = t / K, k = t - i * K;
+      x = A[i * lda + k];
+    } else {
+      const long long u = t - na, k = u / N, j = u - k * N;
+      x = B[k * ldb + j];
+    }
+    bad |= __float_as_uint(__half2float(__float2half_rn(x))) != __float_as_uint(x);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicAnd(flags, 0);
+}
+
+__global__ void fp16_flags_finish_kernel(int* flags) { flags[1] = flags[0] ? 0 : 1; }
+
+// A [M][K] -> half [M][Kp], NaN padding (k >= K).
+__global__ void pack_half_rows_kernel(const float* __restrict__ A, long long lda, int M, int K,
+                                      __half* __restrict__ out, int Kp, const int* g1, const int* g2) {
+  if (!gates_open(g1, g2)) return;
+  const long long total = (long long)M * Kp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / Kp), k = (int)(t - (long long)i * Kp);
+    out[t] = k < K ? __float2half_rn(A[(long long)i * lda + k]) : __ushort_as_half(0x7e00);
+  }
+}
+
+// B [K][N] -> k-pair words [Kp/2][Np]: word (p, j) = (half B[2p][j], half B[2p+1][j]),
+// NaN padding for k >= K and j >= N.
+__global__ void interleave_half_kernel(const float* __restrict__ B, long long ldb, int K, int N,
+                                       __half2* __restrict__ out, int Kp, int Np, const int* g1, const int* g2) {
+  if (!gates_open(g1, g2)) return;
+  const long long total = (long long)(Kp / 2) * Np;
+  const __half nanh = __ushort_as_half(0x7e00);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(t / Np), j = (int)(t - (long long)p * Np);
+    const int k0 = 2 * p, k1 = 2 * p + 1;
+    const __half lo = (k0 < K && j < N) ? __float2half_rn(B[(long long)k0 * ldb + j]) : nanh;
+    const __half hi = (k1 < K && j < N) ? __float2half_rn(B[(long long)k1 * ldb + j]) : nanh;
+    out[t] = __halves2half2(lo, hi);
+  }
 }
 
 // D = (C != 0) as 0/1 of type T.

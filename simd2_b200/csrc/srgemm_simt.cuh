@@ -86,6 +86,7 @@ struct EpilogueArgs {
   int conv_mode;  // simd2_conv, used with `changed`
   const int* gate;  // nullable: when *gate == 0 the kernel does nothing (closure
                     // step enqueued after the fixed point was reached)
+  const int* gate2;  // nullable second gate (the FP16 / FP32 path choice)
 };
 
 __device__ __forceinline__ bool conv_changed(int mode, float old_v, float new_v) {
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
                        const uint8_t* __restrict__ occB) {
   // A closure step enqueued after the previous step reported no change does
   // nothing; every CTA (every cluster member) sees the same word.
-  if (ep.gate && *ep.gate == 0) return;
+  if ((ep.gate && *ep.gate == 0) || (ep.gate2 && *ep.gate2 == 0)) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
@@ -356,6 +357,177 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
       }
     }
     cluster_sync_all();  // peers stay resident until every CTA has read their partials
+  }
+  if (track) {
+    if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP16 selection kernel for max_min / min_max.  Used when every entry of A and
+// B is exactly an FP16 value: (x) and (+) only select, so every product and
+// every accumulator value is one of those FP16 values and the result is
+// bit-identical to the FP32 computation.  Packed min/max.f16x2 handle two k
+// values per lane per instruction (2 ALU instructions per 2 pairs instead of
+// 3).  A is half [M][Kp] (128-byte swizzled TMA tiles of 128 rows x 64 k),
+// B is k-pair words [Kp/2][Np] (tiles of 32 pair-rows x 128 words); the
+// two halves of each accumulator hold the even- and odd-k partial results.
+// ---------------------------------------------------------------------------
+constexpr int kH2BK = 64;  // k per stage
+
+__device__ __forceinline__ uint32_t hmin2u(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("min.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t hmax2u(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("max.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(kSimtThreads, 1)
+    srgemm_h2_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
+                     int K, EpilogueArgs ep, int tiles_m, int tiles_n) {
+  static_assert(OP == SIMD2_MAX_MIN || OP == SIMD2_MIN_MAX, "selection semirings only");
+  constexpr int STAGES = kSimtStages;
+  if ((ep.gate && *ep.gate == 0) || (ep.gate2 && *ep.gate2 == 0)) return;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
+  uint64_t* empty = full + STAGES;
+
+  const int group = 8;
+  const int per_group = group * tiles_n;
+  const int g = blockIdx.x / per_group;
+  const int first_m = g * group;
+  const int gsize = min(tiles_m - first_m, group);
+  const int local = blockIdx.x - g * per_group;
+  const int m0 = (first_m + local % gsize) * kBM;
+  const int n0 = (local / gsize) * kBN;
+  const int ktiles = (K + kH2BK - 1) / kH2BK;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kSimtWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    prefetch_tensormap(&tmA);
+    prefetch_tensormap(&tmB);
+    for (int kt = 0; kt < min(STAGES, ktiles); kt++) {
+      uint8_t* sa = smem + kt * kStageBytes;
+      mbar_arrive_expect_tx(&full[kt], kStageBytes);
+      tma_load_2d(sa, &tmA, &full[kt], kt * kH2BK, m0);
+      tma_load_2d(sa + kATileBytes, &tmB, &full[kt], n0, kt * (kH2BK / 2));
+    }
+  }
+
+  const int tx = lane & 15;
+  const int ty = (warp & 7) * 2 + (lane >> 4);
+  const int cbase = (warp >> 3) * 64;
+  const int swz = ty & 7;
+  // identity of (+) in both halves: -inf (max) or +inf (min)
+  const uint32_t ident = OP == SIMD2_MAX_MIN ? 0xfc00fc00u : 0x7c007c00u;
+  uint32_t acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = ident;
+
+  bool ok = true;
+  int issued = min(STAGES, ktiles);
+  for (int kt = 0; kt < ktiles; kt++) {
+    const int s = kt % STAGES;
+    if (threadIdx.x == 0 && kt >= 1 && kt - 1 + STAGES < ktiles) {
+      const int r = kt - 1, rs = r % STAGES;
+      if (mbar_wait(&empty[rs], (r / STAGES) & 1)) {
+        uint8_t* sa = smem + rs * kStageBytes;
+        const int nk = r + STAGES;
+        mbar_arrive_expect_tx(&full[rs], kStageBytes);
+        tma_load_2d(sa, &tmA, &full[rs], nk * kH2BK, m0);
+        tma_load_2d(sa + kATileBytes, &tmB, &full[rs], n0, nk * (kH2BK / 2));
+        issued = nk + 1;
+      } else {
+        report_timeout(3);
+      }
+    }
+    if (!mbar_wait(&full[s], (kt / STAGES) & 1)) {
+      report_timeout(4);
+      ok = false;
+      break;
+    }
+    const uint8_t* As = smem + s * kStageBytes;                               // 128 rows x 128 bytes
+    const uint32_t* Bs = reinterpret_cast<const uint32_t*>(As + kATileBytes);  // 32 rows x 128 words
+#pragma unroll 2
+    for (int q = 0; q < 8; q++) {  // 16-byte chunk q = k pairs 4q .. 4q+3
+      uint4 a[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        a[i] = *reinterpret_cast<const uint4*>(As + (ty + 16 * i) * 128 + ((q ^ swz) << 4));
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        const int pr = 4 * q + h;
+        uint2 b[2];
+#pragma unroll
+        for (int c = 0; c < 2; c++) b[c] = *reinterpret_cast<const uint2*>(Bs + pr * kBN + cbase + 32 * c + 2 * tx);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const uint32_t ap = h == 0 ? a[i].x : h == 1 ? a[i].y : h == 2 ? a[i].z : a[i].w;
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            if constexpr (OP == SIMD2_MAX_MIN) {
+              acc[i][2 * c] = hmax2u(acc[i][2 * c], hmin2u(ap, b[c].x));
+              acc[i][2 * c + 1] = hmax2u(acc[i][2 * c + 1], hmin2u(ap, b[c].y));
+            } else {
+              acc[i][2 * c] = hmin2u(acc[i][2 * c], hmax2u(ap, b[c].x));
+              acc[i][2 * c + 1] = hmin2u(acc[i][2 * c + 1], hmax2u(ap, b[c].y));
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (!ok) {
+    if (threadIdx.x == 0)
+      for (int kt = max(0, issued - STAGES); kt < issued; kt++) mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1);
+    return;
+  }
+
+  const int do_epi = ep.do_epilogue;
+  const int conv_mode = ep.conv_mode;
+  const bool track = ep.changed != nullptr;
+  int changed = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int row = m0 + ty + 16 * i;
+    if (row < M) {
+      const float* crow = ep.C + (long long)row * ep.ldc;
+      float* drow = ep.D + (long long)row * ep.ldd;
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int col = n0 + cbase + 32 * c + 2 * tx + e;
+          if (col < N) {
+            const uint32_t w = acc[i][2 * c + e];
+            const float lo = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+            const float hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+            const float v = Semiring<OP>::add(lo, hi);
+            const float cv = do_epi ? crow[col] : 0.0f;
+            drow[col] = epilogue_value<OP>(do_epi, conv_mode, track, v, cv, changed);
+          }
+        }
+      }
+    }
   }
   if (track) {
     if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);

@@ -187,3 +187,27 @@ def test_full_size_row_sample(cuda, op):
     want = oracle.srgemm(op, a[rows], b, c[rows], do_epilogue=True)
     np.testing.assert_array_equal(bits(got[rows]), bits(want))
     assert s2.device_status() == 0
+
+
+@pytest.mark.parametrize("op", ["max_min", "min_max"])
+def test_selection_fp16_and_fp32_paths(cuda, op):
+    """max_min / min_max take the packed-FP16 kernel when every A and B entry
+    is an FP16 value, else the FP32 kernel; both must give host_srgemm's bits."""
+    rng = np.random.default_rng(12)
+    m, n, k = 257, 190, 333
+    a, b, c = datagen.semiring_operands(op, m, n, k, seed=12)  # integer-valued: FP16 path
+    cases = [("fp16-exact", a, b)]
+    af = rng.random((m, k), dtype=np.float32)  # generic floats: FP32 path
+    bf = rng.random((k, n), dtype=np.float32)
+    cases.append(("generic", af, bf))
+    a1 = a.copy()
+    a1[5, 7] = np.float32(1.0001)  # one non-FP16 entry switches the whole call to FP32
+    cases.append(("one-off", a1, b))
+    b2 = b.copy()
+    b2[3, 4] = np.float32(70000.0)  # above the FP16 range
+    cases.append(("overflow", a, b2))
+    for name, x, y in cases:
+        for epi in (False, True):
+            got = run_gpu(op, x, y, c, epi, cuda)
+            want = oracle.srgemm(op, x, y, c, do_epilogue=epi)
+            np.testing.assert_array_equal(bits(got), bits(want), err_msg=f"{op} {name} epi={epi}")
