@@ -106,6 +106,12 @@ int simd2_srgemm_orand_u8(int M, int N, int K,
 int simd2_closure(simd2_op op, int n, float* X, int ldx, int max_iter,
                   simd2_conv conv, int* iters_out, cudaStream_t stream);
 
+/* Bellman-Ford form X <- X (+) A0 (x) X with the adjacency A0 fixed (the
+ * reference's APBF build, apps/apsp/emulation/apsp_emulation.cu:99-105);
+ * same convergence tests and step counting as simd2_closure.  Synchronous. */
+int simd2_closure_bf(simd2_op op, int n, const float* A0, int lda0, float* X, int ldx, int max_iter,
+                     simd2_conv conv, int* iters_out, cudaStream_t stream);
+
 /* or_and transitive closure on uint8 0/1 (apps/gtc/cuASR), synchronous. */
 int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter,
                            int* iters_out, cudaStream_t stream);

@@ -27,12 +27,34 @@ NVCC_FLAGS = [
 
 def _newest_source_mtime() -> float:
     paths = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    paths.append(os.path.join(ROOT, "include", "simd2_cuasr.h"))
     paths.append(os.path.join(ROOT, "include", "simd2.h"))
     return max(os.path.getmtime(p) for p in paths if os.path.isfile(p))
 
 
 def needs_build() -> bool:
     return not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest_source_mtime()
+
+
+APP_SRC = os.path.join(HERE, "apps", "closure_app.cu")
+APP = os.path.join(HERE, "apps", "simd2_closure_app")
+
+
+def build_app(force: bool = False) -> str:
+    """The drop-in closure app driver, linked against libsimd2.so."""
+    build()
+    if not force and os.path.exists(APP) and os.path.getmtime(APP) >= max(os.path.getmtime(APP_SRC),
+                                                                              os.path.getmtime(LIB)):
+        return APP
+    nvcc = os.environ.get("NVCC", "nvcc")
+    cmd = [nvcc, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), APP_SRC, "-o", APP + ".tmp",
+           "-L", HERE, "-lsimd2", f"-Xlinker=-rpath,{HERE}"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("building simd2_closure_app failed")
+    os.replace(APP + ".tmp", APP)
+    return APP
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -56,3 +78,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    print(build_app(force="--force" in sys.argv))

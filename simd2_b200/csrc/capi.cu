@@ -728,7 +728,8 @@ int dense_split(int n, int sms) {
 // point cost only their launches.  The host reads the chunk's flags once.
 int closure_gated(int op, int n, float* X, long long ldx, int max_iter, int conv, int fixed_cfg, bool fixed,
                   bool can_skip, bool need_occ, const OccPlan& occ, uint8_t* ws, size_t x_off, int* changed,
-                  uint8_t* obase, int* iters_out, int* step_cfg, float* step_ms, int sms, cudaStream_t stream) {
+                  uint8_t* obase, int* iters_out, int* step_cfg, float* step_ms, int sms, cudaStream_t stream,
+                  const float* A0 = nullptr, long long lda0 = 0) {
   int rc = SIMD2_OK;
   const int auto_split = dense_split(n, sms);
   float* bufs[2] = {X, reinterpret_cast<float*>(ws + x_off)};
@@ -765,11 +766,14 @@ int closure_gated(int op, int n, float* X, long long ldx, int max_iter, int conv
         cfg.occB = obase + occ.occB;
       }
       if (step_cfg) step_cfg[t] = (cfg.skip ? 4 : 0) | (cfg.split == 1 ? 0 : cfg.split == 2 ? 1 : cfg.split == 4 ? 2 : 3);
-      const bool pk = !a_tma_ok(cur, ldcur);
+      // A operand: X_t (repeated squaring) or the fixed adjacency A0 (Bellman-Ford form)
+      const float* Aop = A0 ? A0 : cur;
+      const long long lda_op = A0 ? lda0 : ldcur;
+      const bool pk = !a_tma_ok(Aop, lda_op);
       const Plan pl = make_plan(n, n, n, pk, selection_op(op));
       EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, changed + t, conv);
       ep.gate = gate;
-      if ((rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream, cfg))) break;
+      if ((rc = srgemm_core<float, 0>(op, n, n, n, Aop, lda_op, cur, ldcur, ep, ws, pl, pk, stream, cfg))) break;
       if (step_ms) cudaEventRecord(evs.back(), stream);
     }
     if (rc) break;
@@ -1593,6 +1597,36 @@ extern "C" int simd2_compare_update_i32(int32_t* prev, int32_t* cur, int M, int 
                                         cudaStream_t stream) {
   if (M < 0 || N < 0) return SIMD2_ERR_INVALID_ARG;
   return simd2::compare_update<int32_t>(prev, cur, (long long)M * N, 0, changed_out, stream);
+}
+
+
+// Bellman-Ford form of the closure (the reference's APBF build of
+// apps/apsp/emulation/apsp_emulation.cu:99-105 and apps/aplp/emulation):
+// X_{t+1} = X_t (+) A0 (x) X_t with the adjacency A0 fixed.
+extern "C" int simd2_closure_bf(simd2_op op, int n, const float* A0, int lda0, float* X, int ldx, int max_iter,
+                                simd2_conv conv, int* iters_out, cudaStream_t stream) {
+  using namespace simd2;
+  if (iters_out) *iters_out = 0;
+  if (n < 0 || max_iter < 0 || !is_float_op(op) || is_sum_op(op) || (n > 0 && (!X || !A0 || ldx < n || lda0 < n)))
+    return SIMD2_ERR_INVALID_ARG;
+  if (conv < SIMD2_CONV_EXACT || conv > SIMD2_CONV_APLP) return SIMD2_ERR_INVALID_ARG;
+  if (n == 0 || max_iter == 0) return SIMD2_OK;
+  int rc = check_device();
+  if (rc) return rc;
+  int dev = 0, sms = 148;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const Plan plan = make_plan(n, n, n, true, selection_op(op));
+  const OccPlan occ = make_occ_plan(n, n, n, true);
+  const size_t x_off = align_up(plan.total, kAlign);
+  const size_t f_off = x_off + align_up((size_t)n * n * 4, kAlign);
+  const size_t total = f_off + align_up((size_t)(max_iter + 1) * sizeof(int), kAlign);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, total, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  return closure_gated(op, n, X, ldx, max_iter, conv, 0, false, false, false, occ, ws, x_off,
+                       reinterpret_cast<int*>(ws + f_off), nullptr, iters_out, nullptr, nullptr, sms, stream, A0,
+                       lda0);
 }
 
 // ---------------------------------------------------------------------------
