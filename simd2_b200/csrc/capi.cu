@@ -232,6 +232,7 @@ struct SimtConfig {
   bool skip = false;
   const uint8_t* occA = nullptr;
   const uint8_t* occB = nullptr;
+  bool count_ops = true;  // false when an alternative kernel of the same call already counts them
 };
 
 // The (x)-annihilator whose products equal the (+)-identity: blocks made only
@@ -261,7 +262,7 @@ int launch_simt_cfg(int M, int N, int K, const CUtensorMap& mA, const CUtensorMa
   }
   const int tiles_m = (M + kBM - 1) / kBM;
   const int tiles_n = (N + kBN - 1) / kBN;
-  auto* ev = prof_slot(2LL * M * N * K);
+  auto* ev = prof_slot(cfg.count_ops ? 2LL * M * N * K : 0LL);
   if (ev) cudaEventRecord(ev->first, stream);
   if constexpr (SPLIT == 1) {
     kern<<<tiles_m * tiles_n, kSimtThreads, smem, stream>>>(mA, mB, M, N, K, ep, tiles_m, tiles_n, cfg.occA,
@@ -441,6 +442,8 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   }
   EpilogueArgs ep32 = ep;
   ep32.gate2 = path_gate;
+  SimtConfig cfg32 = cfg;
+  if (path_gate) cfg32.count_ops = false;  // the FP16 kernel's slot carries the operation count
   interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 2), 256, 0, stream>>>(
       B, ldb, K, N, Bp, plan.Kp, plan.Np, pad, ep.gate, path_gate);
   count_launch();
@@ -463,7 +466,7 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   rc = make_map_f32(&mB, Bp, plan.Kp / 2, 2LL * plan.Np, 2LL * plan.Np, 2 * kBN, kBK / 2, CU_TENSOR_MAP_SWIZZLE_NONE,
                     false);
   if (rc) return rc;
-  return dispatch_simt(op, M, N, K, mA, mB, ep32, cfg, stream);
+  return dispatch_simt(op, M, N, K, mA, mB, ep32, cfg32, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -866,49 +869,59 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
                          x_off, reinterpret_cast<int*>(ws + f_off + 256), obase, iters_out, step_cfg, step_ms, sms,
                          stream);
   }
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (step_ms) {
-    SIMD2_CUDA_TRY(cudaEventCreate(&e0));
-    SIMD2_CUDA_TRY(cudaEventCreate(&e1));
-  }
+  // Per-step loop (learned dispatch, or feature recording): the occupancy and
+  // the cost-model choice for step t+1 are enqueued right after step t's
+  // srgemm, so one host synchronisation per step reads step t's change flag
+  // together with step t+1's decision (and features).
+  cudaEvent_t ev[4] = {};  // srgemm start/end, occupancy start/end
+  if (step_ms)
+    for (auto& e : ev) SIMD2_CUDA_TRY(cudaEventCreate(&e));
+  float occ_ms = 0.f;
+  auto enqueue_occ = [&](const float* m, long long ld) -> int {
+    if (step_ms) cudaEventRecord(ev[2], stream);
+    int r = compute_occupancy(op, n, n, n, m, ld, m, ld, true, obase, occ, stream);
+    if (r) return r;
+    if (dispatch == 2) {
+      mlp_choose_kernel<<<1, 32, 0, stream>>>(mlp_params, reinterpret_cast<unsigned long long*>(obase + occ.stats), n,
+                                              occ.tiles_m, occ.tiles_n, occ.ktiles, sms, can_skip ? 1 : 0, 8,
+                                              decision);
+      count_launch();
+    }
+    if (step_ms) cudaEventRecord(ev[3], stream);
+    return SIMD2_OK;
+  };
+  // host copies of {flag, decision[0..8]} and the occupancy statistics
+  int hbuf[9] = {};
+  unsigned long long hst[3] = {};
+  auto read_back = [&](bool want_flag, bool want_dec) -> int {
+    if (want_flag || want_dec) {
+      if (cudaMemcpyAsync(hbuf, flag, sizeof(hbuf), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+        return SIMD2_ERR_CUDA;
+    }
+    if (want_dec && step_feat) {
+      if (cudaMemcpyAsync(hst, obase + occ.stats, sizeof(hst), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+        return SIMD2_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return SIMD2_ERR_CUDA;
+    if (step_ms && want_dec) cudaEventElapsedTime(&occ_ms, ev[2], ev[3]);
+    return SIMD2_OK;
+  };
+  const int ds = dense_split(n, sms);
+  const int default_cfg = dispatch == 1 ? fixed_cfg : (ds == 1 ? 0 : ds == 2 ? 1 : 2);
   float* cur = X;
   long long ldcur = ldx;
   float* nxt = Xn;
   long long ldnxt = n;
   int it = 0;
   int changed = 1;
+  int cfg_id = default_cfg;
+  if (need_occ) {
+    if ((rc = enqueue_occ(cur, ldcur)) || (rc = read_back(false, true))) return rc;
+    if (dispatch == 2) cfg_id = hbuf[8];  // decision[0]
+    if (step_feat) mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst[0], hst[1], hst[2], sms, step_feat);
+  }
   while (changed && it < max_iter) {
-    if (e0) cudaEventRecord(e0, stream);
-    const int ds = dense_split(n, sms);
-    int cfg_id = dispatch == 1 ? fixed_cfg : (ds == 1 ? 0 : ds == 2 ? 1 : 2);
     SimtConfig cfg;
-    if (need_occ) {
-      rc = compute_occupancy(op, n, n, n, cur, ldcur, cur, ldcur, true, obase, occ, stream);
-      if (rc) break;
-      if (dispatch == 2) {
-        mlp_choose_kernel<<<1, 32, 0, stream>>>(mlp_params, reinterpret_cast<unsigned long long*>(obase + occ.stats),
-                                                n, occ.tiles_m, occ.tiles_n, occ.ktiles, sms, can_skip ? 1 : 0, 8,
-                                                decision);
-        count_launch();
-        int h = 0;
-        if (cudaMemcpyAsync(&h, decision, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-            cudaStreamSynchronize(stream) != cudaSuccess) {
-          rc = SIMD2_ERR_CUDA;
-          break;
-        }
-        cfg_id = h;
-      }
-      if (step_feat) {
-        unsigned long long st[3];
-        if (cudaMemcpyAsync(st, obase + occ.stats, sizeof(st), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-            cudaStreamSynchronize(stream) != cudaSuccess) {
-          rc = SIMD2_ERR_CUDA;
-          break;
-        }
-        mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, st[0], st[1], st[2], sms,
-                     step_feat + (size_t)it * kMlpFeat);
-      }
-    }
     cfg.split = config_split(cfg_id);
     cfg.skip = config_skip(cfg_id) && can_skip && need_occ;
     if (cfg.skip) {
@@ -916,34 +929,39 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
       cfg.occB = obase + occ.occB;
     }
     if (step_cfg) step_cfg[it] = (cfg.skip ? 4 : 0) | (cfg.split == 1 ? 0 : cfg.split == 2 ? 1 : cfg.split == 4 ? 2 : 3);
-    it++;
+    const float step_occ_ms = (need_occ && cfg.skip) ? occ_ms : 0.f;  // a skip step pays for its occupancy pass
     if (cudaMemsetAsync(flag, 0, sizeof(int), stream) != cudaSuccess) {
       rc = SIMD2_ERR_CUDA;
       break;
     }
+    if (step_ms) cudaEventRecord(ev[0], stream);
     const bool pk = !a_tma_ok(cur, ldcur);
     const Plan pl = make_plan(n, n, n, pk, selection_op(op));
     const EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, flag, conv);
     rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream, cfg);
     if (rc) break;
-    if (e1) cudaEventRecord(e1, stream);
-    int h = 0;
-    if (cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-        cudaStreamSynchronize(stream) != cudaSuccess) {
-      rc = SIMD2_ERR_CUDA;
-      break;
-    }
+    if (step_ms) cudaEventRecord(ev[1], stream);
+    it++;
+    const bool next = need_occ && it < max_iter;
+    if (next && (rc = enqueue_occ(nxt, ldnxt))) break;
+    float srg_ms = 0.f;
+    if ((rc = read_back(true, next))) break;
     if (step_ms) {
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      step_ms[it - 1] = ms;
+      cudaEventElapsedTime(&srg_ms, ev[0], ev[1]);
+      step_ms[it - 1] = srg_ms + step_occ_ms;
     }
-    changed = h != 0;
+    changed = hbuf[0] != 0;
+    if (next) {
+      if (dispatch == 2) cfg_id = hbuf[8];
+      if (step_feat && changed)
+        mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst[0], hst[1], hst[2], sms,
+                     step_feat + (size_t)it * kMlpFeat);
+    }
     std::swap(cur, nxt);
     std::swap(ldcur, ldnxt);
   }
-  if (e0) cudaEventDestroy(e0);
-  if (e1) cudaEventDestroy(e1);
+  if (step_ms)
+    for (auto& e : ev) cudaEventDestroy(e);
   if (rc) return rc;
   if (cur != X) {
     SIMD2_CUDA_TRY(cudaMemcpy2DAsync(X, ldx * 4, cur, ldcur * 4, (size_t)n * 4, n, cudaMemcpyDeviceToDevice, stream));
