@@ -985,8 +985,9 @@ struct BatchedPlan {
   int count;
   int max_iter;
   int conv;
-  void* mem;            // one device allocation: descriptors, order, queue, buffers
+  void* mem;            // one device allocation: descriptors, maps, order, queue, buffers
   BatchGraph* d_graphs;
+  BatchMaps* d_maps;
   int* d_order;
   int* d_queue;
   std::vector<BatchGraph> host;
@@ -1004,7 +1005,8 @@ int launch_batched(BatchedPlan* p, cudaStream_t stream) {
   int sms = 0;
   SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->dev));
   const int grid = std::max(1, std::min(sms, p->count));
-  kern<<<grid, kSimtThreads, smem, stream>>>(p->d_graphs, p->d_order, p->count, p->d_queue, p->max_iter, p->conv);
+  kern<<<grid, kSimtThreads, smem, stream>>>(p->d_graphs, p->d_maps, p->d_order, p->count, p->d_queue, p->max_iter,
+                                             p->conv);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
@@ -1235,6 +1237,7 @@ int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
   const size_t g_off = take(sizeof(BatchGraph) * std::max(count, 1));
+  const size_t m_off = take(sizeof(BatchMaps) * std::max(count, 1));
   const size_t o_off = take(sizeof(int) * std::max(count, 1));
   const size_t q_off = take(sizeof(int));
   std::vector<size_t> buf_off(count);
@@ -1258,6 +1261,7 @@ int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int
   p->mem = mem;
   uint8_t* base = static_cast<uint8_t*>(mem);
   p->d_graphs = reinterpret_cast<BatchGraph*>(base + g_off);
+  p->d_maps = reinterpret_cast<BatchMaps*>(base + m_off);
   p->d_order = reinterpret_cast<int*>(base + o_off);
   p->d_queue = reinterpret_cast<int*>(base + q_off);
   for (int g = 0; g < count; g++) {
@@ -1270,6 +1274,25 @@ int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int
     G.P[1] = reinterpret_cast<float*>(b + 2 * xb + pb);
     G.iters = 0;
     G.changed = 0;
+  }
+  // tensor maps: A role = X[b] [Mp][Kp], B role = P[b] [Kp/2][2Np] (all padded, never out of bounds)
+  std::vector<BatchMaps> hmaps(count);
+  for (int g = 0; g < count; g++) {
+    BatchGraph& G = p->host[g];
+    for (int b = 0; b < 2 && rc == SIMD2_OK; b++) {
+      rc = make_map_f32(&hmaps[g].a[b], G.X[b], G.Mp, G.Kp, G.Kp, kBK, kBM, CU_TENSOR_MAP_SWIZZLE_128B, false);
+      if (rc == SIMD2_OK)
+        rc = make_map_f32(&hmaps[g].b[b], G.P[b], G.Kp / 2, 2LL * G.Np, 2LL * G.Np, 2 * kBN, kBK / 2,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, false);
+    }
+  }
+  if (rc == SIMD2_OK && count > 0 &&
+      cudaMemcpy(p->d_maps, hmaps.data(), sizeof(BatchMaps) * count, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = SIMD2_ERR_CUDA;
+  if (rc) {
+    cudaFree(mem);
+    delete p;
+    return rc;
   }
   // longest-processing-time order: largest graphs first
   std::vector<int> order(count);

@@ -12,9 +12,13 @@
 // (the B operand of the CUDA-core micro-kernel, see srgemm_simt.cuh).  All
 // padding (rows/cols >= n) is NaN, written once by the prep kernel and never
 // overwritten, so every tile load is in bounds and a padded k contributes a
-// NaN product, which min/max drop.  Tiles are staged with cp.async (16-byte
-// copies, 4-stage ring, one __syncthreads per k-tile); the epilogue of
-// iteration t writes both layouts of X_{t+1} and a per-graph change flag.
+// NaN product, which min/max drop.  Tiles are staged by TMA through
+// per-graph tensor maps kept in device memory (encoded once per plan) into
+// the same 4-stage mbarrier ring as the single srgemm, with the barrier
+// phases running on across tiles and graphs; the epilogue of iteration t
+// writes both layouts of X_{t+1} and a per-graph change flag, then a
+// generic-to-async proxy fence orders those writes before the next step's
+// TMA reads.
 #pragma once
 #include "srgemm_simt.cuh"
 
@@ -62,14 +66,30 @@ __device__ __forceinline__ void batch_stage_load(uint8_t* st, const float* X, in
   }
 }
 
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+// Tensor maps of one graph, in device memory: A role X[0], X[1] ([Mp][Kp],
+// 128 x 32 boxes, 128-byte swizzle) and B role P[0], P[1] ([Kp/2][2Np],
+// 16 x 256 boxes).  Encoded once on the host when the plan is made.
+struct BatchMaps {
+  CUtensorMap a[2];
+  CUtensorMap b[2];
+};
+
 template <int OP>
 __global__ void __launch_bounds__(kSimtThreads, 1)
-    closure_batched_kernel(BatchGraph* graphs, const int* order, int count, int* queue, int max_iter, int conv_mode) {
-  constexpr int STAGES = 4;
+    closure_batched_kernel(BatchGraph* graphs, const BatchMaps* __restrict__ maps, const int* order, int count,
+                           int* queue, int max_iter, int conv_mode) {
+  constexpr int STAGES = kSimtStages;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
+  uint64_t* empty = full + STAGES;
   __shared__ int s_graph;
   __shared__ int s_changed;
+  __shared__ int s_failed;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -79,28 +99,63 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
   const int swz = ty & 7;
   constexpr int WN = 2;
 
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kSimtWarps);
+    }
+    fence_mbar_init();
+    s_failed = 0;
+  }
+  __syncthreads();
+  // Running k-tile counter of this CTA: load number g uses stage g % STAGES
+  // with phase parity (g / STAGES) & 1, across tiles, iterations and graphs.
+  uint32_t gk = 0;
+
   while (true) {
     if (threadIdx.x == 0) {
       const int q = atomicAdd(queue, 1);
-      s_graph = q < count ? order[q] : -1;
+      s_graph = (q < count && !s_failed) ? order[q] : -1;
     }
     __syncthreads();
     const int gi = s_graph;
     if (gi < 0) break;
     BatchGraph& G = graphs[gi];
+    const BatchMaps* mp = maps + gi;
     const int n = G.n, Kp = G.Kp, Np = G.Np;
     const int tiles_m = G.Mp / kBM, tiles_n = Np / kBN, ktiles = Kp / kBK;
     int it = 0, changed_any = 1;
     while (changed_any && it < max_iter) {
       const int cur = it & 1, nxt = cur ^ 1;
       const float* X = G.X[cur];
-      const float* P = G.P[cur];
       float* Xn = G.X[nxt];
       float* Pn = G.P[nxt];
+      const CUtensorMap* tmA = &mp->a[cur];
+      const CUtensorMap* tmB = &mp->b[cur];
       if (threadIdx.x == 0) s_changed = 0;
       __syncthreads();
       int changed = 0;
-      for (int t = 0; t < tiles_m * tiles_n; t++) {
+      // The step's loads form one stream over (tile, k): load j = tile j / ktiles,
+      // k-tile j % ktiles, so the next tile's first loads are in flight while the
+      // current tile runs its epilogue.
+      const int ntiles = tiles_m * tiles_n;
+      const int nloads = ntiles * ktiles;
+      auto issue = [&](int j) {
+        const uint32_t g = gk + j;
+        const int s = g % STAGES;
+        if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1)) {
+          report_timeout(21);
+          s_failed = 1;
+        }
+        const int tile = j / ktiles, kk = j - tile * ktiles;
+        uint8_t* sa = smem + s * kStageBytes;
+        mbar_arrive_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(sa, tmA, &full[s], kk * kBK, (tile % tiles_m) * kBM);
+        tma_load_2d(sa + kATileBytes, tmB, &full[s], 2 * (tile / tiles_m) * kBN, kk * (kBK / 2));
+      };
+      if (threadIdx.x == 0)
+        for (int j = 0; j < min(STAGES, nloads); j++) issue(j);
+      for (int t = 0; t < ntiles; t++) {
         const int m0 = (t % tiles_m) * kBM;
         const int n0 = (t / tiles_m) * kBN;
         float acc[8][2 * WN];
@@ -108,27 +163,24 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
         for (int i = 0; i < 8; i++)
 #pragma unroll
           for (int j = 0; j < 2 * WN; j++) acc[i][j] = Mac<OP>::identity();
-        // prologue: STAGES-1 tiles in flight
-#pragma unroll
-        for (int s = 0; s < STAGES - 1; s++) {
-          if (s < ktiles) batch_stage_load(smem + s * kStageBytes, X, Kp, P, Np, m0, n0, s);
-          cp_async_commit();
-        }
-        for (int kt = 0; kt < ktiles; kt++) {
-          cp_async_wait<STAGES - 2>();
-          __syncthreads();  // tile kt visible to all; every thread is done with tile kt-1
-          const int nk = kt + STAGES - 1;
-          if (nk < ktiles) batch_stage_load(smem + (nk % STAGES) * kStageBytes, X, Kp, P, Np, m0, n0, nk);
-          cp_async_commit();
-          const uint8_t* st = smem + (kt % STAGES) * kStageBytes;
-          const float* As = reinterpret_cast<const float*>(st);
-          const float* Bs = reinterpret_cast<const float*>(st + kATileBytes);
+        for (int i = 0; i < ktiles; i++) {
+          const int j = t * ktiles + i;
+          const uint32_t g = gk + j;
+          const int s = g % STAGES;
+          // refill: load j-1+STAGES goes into the stage that load j-1 used
+          if (threadIdx.x == 0 && j >= 1 && j - 1 + STAGES < nloads) issue(j - 1 + STAGES);
+          if (!mbar_wait(&full[s], (g / STAGES) & 1)) {
+            report_timeout(23);
+            s_failed = 1;
+          }
+          const float* As = reinterpret_cast<const float*>(smem + s * kStageBytes);
+          const float* Bs = reinterpret_cast<const float*>(smem + s * kStageBytes + kATileBytes);
 #pragma unroll 2
           for (int q = 0; q < kBK / 4; q++) {
             float4 a[8];
 #pragma unroll
-            for (int i = 0; i < 8; i++)
-              a[i] = *reinterpret_cast<const float4*>(As + (ty + 16 * i) * kBK + ((q ^ swz) << 2));
+            for (int ii = 0; ii < 8; ii++)
+              a[ii] = *reinterpret_cast<const float4*>(As + (ty + 16 * ii) * kBK + ((q ^ swz) << 2));
 #pragma unroll
             for (int h = 0; h < 2; h++) {
               float4 b[WN];
@@ -136,19 +188,19 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
               for (int c = 0; c < WN; c++)
                 b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (cbase + 32 * c + 2 * tx) * 2);
 #pragma unroll
-              for (int i = 0; i < 8; i++) {
-                const float2 ap = h == 0 ? make_float2(a[i].x, a[i].y) : make_float2(a[i].z, a[i].w);
+              for (int ii = 0; ii < 8; ii++) {
+                const float2 ap = h == 0 ? make_float2(a[ii].x, a[ii].y) : make_float2(a[ii].z, a[ii].w);
 #pragma unroll
                 for (int c = 0; c < WN; c++) {
-                  acc[i][2 * c] = Mac<OP>::mac2(acc[i][2 * c], ap, make_float2(b[c].x, b[c].y));
-                  acc[i][2 * c + 1] = Mac<OP>::mac2(acc[i][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
+                  acc[ii][2 * c] = Mac<OP>::mac2(acc[ii][2 * c], ap, make_float2(b[c].x, b[c].y));
+                  acc[ii][2 * c + 1] = Mac<OP>::mac2(acc[ii][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
                 }
               }
             }
           }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&empty[s]);
         }
-        cp_async_wait<0>();
-        __syncthreads();  // stages free for the next tile
         // epilogue: X_{t+1} = X_t (+) acc in both layouts, change test against X_t
 #pragma unroll
         for (int i = 0; i < 8; i++) {
@@ -172,14 +224,17 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
           }
         }
       }
+      gk += nloads;
       if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(&s_changed, 1);
-      __syncthreads();  // X_{t+1} complete (block-level ordering of the global writes)
-      changed_any = s_changed;
+      // X_{t+1} was written through the generic proxy; the next step reads it with TMA.
+      fence_proxy_async_global();
+      __syncthreads();
+      changed_any = s_changed && !s_failed;
       it++;
     }
     if (threadIdx.x == 0) {
       G.iters = it;
-      G.changed = changed_any;
+      G.changed = changed_any || s_failed;
     }
     __syncthreads();
   }
