@@ -59,7 +59,9 @@ def parse_args():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the batched-closure / learned-dispatch / APSP-512 measurements")
     p.add_argument("--batched-count", type=int, default=4096)
-    p.add_argument("--workload", choices=("sweep", "batched"), default="sweep",
+    p.add_argument("--knn-q", type=int, default=16384)
+    p.add_argument("--knn-r", type=int, default=65536)
+    p.add_argument("--workload", choices=("sweep", "batched", "knn"), default="sweep",
                    help="sweep: the nine-semiring srgemm line (default); batched: only the batched closure "
                         "(used for profiling runs)")
     p.add_argument("--no-e2e", action="store_true")
@@ -296,6 +298,49 @@ def extra_measurements(args, dev):
     out["batched_apsp"] = res_b
     del mats
 
+    # --- dense-contraction workloads at full size (tensor cores)
+    cfg4 = {}
+    n4 = 16384
+    rng = np.random.default_rng(44)
+    m4 = 2 * n4
+    X = torch.zeros((n4, n4), dtype=torch.uint8, device=dev)
+    X[torch.from_numpy(rng.integers(0, n4, m4)).to(dev), torch.from_numpy(rng.integers(0, n4, m4)).to(dev)] = 1
+    X.fill_diagonal_(1)
+    s2.closure("or_and", X.clone())  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    it4 = s2.closure("or_and", X)
+    ms4 = (time.perf_counter() - t0) * 1e3
+    cfg4["or_and_closure_16384"] = {"ms": ms4, "iters": it4, "gops": 2.0 * n4 ** 3 * it4 / ms4 / 1e6,
+                                    "how": "simd2_closure_orand_u8 wall clock, INT8 tcgen05 per squaring"}
+    del X
+    q, r = datagen.point_cloud(16384, 65536, 128, seed=4, dup_frac=0.05)
+    Q, R = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
+    s2.knn(Q[:1024], R, 16)  # warm-up
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    s2.knn(Q, R, 16)
+    ev1.record()
+    torch.cuda.synchronize()
+    kms = ev0.elapsed_time(ev1)
+    cfg4["knn_16384x65536x128_k16"] = {"ms": kms, "queries_per_s": 16384 / kms * 1e3,
+                                       "gops": 2.0 * 16384 * 65536 * 128 / kms / 1e6,
+                                       "how": "simd2_knn, CUDA events (BF16 hi/lo minus_square + top-k + sqrt)"}
+    del Q, R
+    A = torch.randn((8192, 8192), device=dev)
+    B = torch.randn((8192, 8192), device=dev)
+    s2.srgemm("plus_mul", A, B)
+    ev0.record()
+    for _ in range(3):
+        s2.srgemm("plus_mul", A, B)
+    ev1.record()
+    torch.cuda.synchronize()
+    pms = ev0.elapsed_time(ev1) / 3
+    cfg4["plus_mul_8192"] = {"ms": pms, "gops": 2.0 * 8192 ** 3 / pms / 1e6,
+                             "bf16_equiv_tflops": 3 * 2.0 * 8192 ** 3 / pms / 1e9}
+    del A, B
+    out["dense_contraction"] = cfg4
+
     # --- learned dispatch on mixed-density R-MAT (a=.57 b=.19 c=.19), vs the plain dense path
     if params is not None:
         rows = []
@@ -349,6 +394,24 @@ def main():
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.workload == "knn":
+        from simd2_b200 import datagen
+        q, r = datagen.point_cloud(args.knn_q, args.knn_r, 128, seed=4, dup_frac=0.05)
+        Q, R = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
+        for _ in range(max(args.warmup, 1)):
+            s2.knn(Q, R, 16)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(args.steps):
+            s2.knn(Q, R, 16)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        if rank == 0:
+            print(json.dumps({"workload": f"knn Q={args.knn_q} R={args.knn_r} D=128 k=16", "ms": ms,
+                              "queries_per_s": args.knn_q / ms * 1e3}), flush=True)
+        return 0
 
     if args.workload == "batched":
         res, _ = batched_sharded(args, dev, rank, world)

@@ -235,6 +235,14 @@ int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops);
  * (0 = CUDA-core srgemm, 1 = tensor-core srgemm). */
 int simd2_profile_result(int kind, double* kernel_ms, long long* launches, long long* ops);
 
+/* Failure-detection self-test: one kernel waits, for at most limit_us
+ * microseconds (<= 2 s), on a barrier that nothing completes, then records
+ * SIMD2_ERR_TIMEOUT (wait site 99) in the device error word exactly as a
+ * real lost arrival would.  Synchronous; afterwards simd2_device_status()
+ * returns SIMD2_ERR_TIMEOUT and the device stays usable.  No counterpart in
+ * the reference. */
+int simd2_selftest_timeout(unsigned int limit_us);
+
 /* Read and clear the id of the last bounded wait that ran out (0 = none);
  * a diagnostic companion of simd2_device_status(). */
 int simd2_timeout_site(void);

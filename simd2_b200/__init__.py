@@ -77,6 +77,10 @@ def lib() -> ctypes.CDLL:
         L.simd2_closure_batched.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, PI, P]
         L.simd2_knn.argtypes = [P, I, I, P, I, I, I, I, P, P, I, P]
         L.simd2_knn.restype = I
+        L.simd2_selftest_timeout.argtypes = [ctypes.c_uint]
+        L.simd2_selftest_timeout.restype = I
+        L.simd2_timeout_site.argtypes = []
+        L.simd2_timeout_site.restype = I
         L.simd2_launch_count.argtypes = []
         L.simd2_launch_count.restype = ctypes.c_longlong
         L.simd2_profile_begin.argtypes = []

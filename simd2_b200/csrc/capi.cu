@@ -1193,6 +1193,17 @@ int simd2_profile_end(double* kernel_ms, long long* launches, long long* ops) {
   return SIMD2_OK;
 }
 
+int simd2_selftest_timeout(unsigned int limit_us) {
+  if (limit_us == 0 || limit_us > 2000000u) return SIMD2_ERR_INVALID_ARG;
+  int rc = check_device();
+  if (rc) return rc;
+  wait_timeout_selftest_kernel<<<1, 32>>>((uint64_t)limit_us * 1000ull);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  SIMD2_CUDA_TRY(cudaDeviceSynchronize());
+  return SIMD2_OK;
+}
+
 int simd2_timeout_site(void) {
   int h = 0, zero = 0;
   if (cudaDeviceSynchronize() != cudaSuccess) return -1;
@@ -1443,8 +1454,8 @@ namespace {
 template <int KT>
 int knn_topk_launch(const float* dist, long long ldd, int rows, int cols, float* od, int32_t* oi, long long ldo,
                     int kout, cudaStream_t stream) {
-  knn_topk_kernel<KT><<<grid_for((long long)rows * 32, 256), 256, 0, stream>>>(dist, ldd, rows, cols, 0, od, oi, ldo,
-                                                                               kout, 1);
+  knn_topk_kernel<KT><<<std::max(1, std::min(rows, 148 * 16)), kKnnWarps * 32, 0, stream>>>(dist, ldd, rows, cols, 0,
+                                                                                            od, oi, ldo, kout, 1);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;

@@ -67,13 +67,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait on phase `parity`.  Returns false if kWaitLimitNs elapsed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   while (true) {
     for (int i = 0; i < 64; i++)
       if (mbar_try_wait(bar, parity)) return true;
-    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
 
@@ -96,6 +96,21 @@ __device__ __forceinline__ void report_timeout(int site) {
   atomicOr(&g_device_status, SIMD2_ERR_TIMEOUT);
   atomicMax(&g_timeout_site, site);
 }
+
+// Self-test of the bounded wait: waits on a fresh barrier that nothing
+// arrives on (its phase never completes) for at most limit_ns, then reports
+// SIMD2_ERR_TIMEOUT with wait-site 99 through the normal error word and
+// returns.  Nothing faults or hangs: the wait simply runs out.
+__global__ void wait_timeout_selftest_kernel(uint64_t limit_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0, limit_ns)) report_timeout(99);
+}
+
 
 // ---------------------------------------------------------------------------
 // Semiring operators.  The add step keeps host_srgemm's accumulator-first

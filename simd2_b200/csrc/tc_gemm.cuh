@@ -269,66 +269,129 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   tc_fence_after();
   ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld below is warp-collective
-  const int row = m0 + warp * 32 + lane;
+  // Each warp owns tile rows 32w..32w+31 (its TMEM lanes); tcgen05.ld gives
+  // lane l the 32 accumulators of tile row 32w+l for 32 consecutive columns.
   const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+  const int row0 = m0 + warp * 32;
   int changed = 0;
   if (ok) {
+    if constexpr (KIND == 1) {
+      // or_and: 32 flags of one row are 32 contiguous bytes (u8) or 128 bytes
+      // (i32), so each lane writes its own row with 16-byte vector stores.
+      const int row = row0 + lane;
+      const bool u8 = ep.out_u8 != 0;
+      const int esz = u8 ? 1 : 4;
+      const bool vec_ok = ((ep.ldd * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.D) & 15) == 0) &&
+                          (!ep.do_epilogue ||
+                           (((ep.ldc * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.C) & 15) == 0)));
 #pragma unroll 1
-    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
-      uint32_t r[32];
-      tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
-      if (row >= M) continue;
-      const int colb = n0 + c0;
-      if constexpr (KIND == 1) {
-        if (ep.out_u8) {
+      for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+        uint32_t r[32];
+        tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
+        if (row >= M) continue;
+        const int colb = n0 + c0;
+        if (u8) {
           const uint8_t* crow = static_cast<const uint8_t*>(ep.C) + (long long)row * ep.ldc;
           uint8_t* drow = static_cast<uint8_t*>(ep.D) + (long long)row * ep.ldd;
+          if (vec_ok && colb + 32 <= N) {
+            uint32_t w[8];
 #pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const int col = colb + j;
-            if (col < N) {
-              uint8_t v = r[j] != 0u;
-              if (ep.do_epilogue) {
-                const uint8_t cv = crow[col] != 0;
-                v |= cv;
-                if (ep.changed && v != cv) changed = 1;
+            for (int q = 0; q < 8; q++)
+              w[q] = (r[4 * q] != 0u) | ((r[4 * q + 1] != 0u) << 8) | ((r[4 * q + 2] != 0u) << 16) |
+                     ((uint32_t)(r[4 * q + 3] != 0u) << 24);
+            if (ep.do_epilogue) {
+              const uint4 c0v = *reinterpret_cast<const uint4*>(crow + colb);
+              const uint4 c1v = *reinterpret_cast<const uint4*>(crow + colb + 16);
+              const uint32_t cw[8] = {c0v.x, c0v.y, c0v.z, c0v.w, c1v.x, c1v.y, c1v.z, c1v.w};
+#pragma unroll
+              for (int q = 0; q < 8; q++) {
+                // normalise C's bytes to 0/1 before the OR
+                uint32_t cb = cw[q];
+                cb = ((cb & 0x7f7f7f7fu) + 0x7f7f7f7fu | cb) & 0x80808080u;
+                cb >>= 7;
+                const uint32_t v = w[q] | cb;
+                if (ep.changed && v != cb) changed = 1;
+                w[q] = v;
               }
-              drow[col] = v;
+            }
+            *reinterpret_cast<uint4*>(drow + colb) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(drow + colb + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const int col = colb + j;
+              if (col < N) {
+                uint8_t v = r[j] != 0u;
+                if (ep.do_epilogue) {
+                  const uint8_t cv = crow[col] != 0;
+                  v |= cv;
+                  if (ep.changed && v != cv) changed = 1;
+                }
+                drow[col] = v;
+              }
             }
           }
         } else {
           const int32_t* crow = static_cast<const int32_t*>(ep.C) + (long long)row * ep.ldc;
           int32_t* drow = static_cast<int32_t*>(ep.D) + (long long)row * ep.ldd;
+          if (vec_ok && colb + 32 <= N) {
 #pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const int col = colb + j;
-            if (col < N) {
-              int32_t v = r[j] != 0u;
-              if (ep.do_epilogue) v |= (crow[col] != 0);
-              drow[col] = v;
+            for (int q = 0; q < 8; q++) {
+              int4 v = make_int4(r[4 * q] != 0u, r[4 * q + 1] != 0u, r[4 * q + 2] != 0u, r[4 * q + 3] != 0u);
+              if (ep.do_epilogue) {
+                const int4 c = *reinterpret_cast<const int4*>(crow + colb + 4 * q);
+                v.x |= c.x != 0;
+                v.y |= c.y != 0;
+                v.z |= c.z != 0;
+                v.w |= c.w != 0;
+              }
+              *reinterpret_cast<int4*>(drow + colb + 4 * q) = v;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const int col = colb + j;
+              if (col < N) {
+                int32_t v = r[j] != 0u;
+                if (ep.do_epilogue) v |= (crow[col] != 0);
+                drow[col] = v;
+              }
             }
           }
         }
-      } else {
-        const float* crow = static_cast<const float*>(ep.C) + (long long)row * ep.ldc;
-        float* drow = static_cast<float*>(ep.D) + (long long)row * ep.ldd;
-        const float na = ep.op == SIMD2_MINUS_SQUARE ? ep.norm_a[row] : 0.f;
+      }
+    } else {
+      // Sums: a 32 x 32 chunk is transposed through shared memory (the stage
+      // ring is idle now) and written row by row: lane l handles column l, so
+      // every store instruction covers 32 consecutive floats of one row.
+      uint32_t* tile = reinterpret_cast<uint32_t*>(smem) + warp * (32 * 33);
+#pragma unroll 1
+      for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+        uint32_t r[32];
+        tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
 #pragma unroll
-        for (int j = 0; j < 32; j++) {
-          const int col = colb + j;
-          if (col < N) {
-            float v = __uint_as_float(r[j]);
-            if (ep.op == SIMD2_MINUS_SQUARE) {
-              const float nb = ep.norm_b[col];
-              const float nsum = na + nb;
-              v = __fmaf_rn(-2.0f, v, nsum);
-              if (v < ep.band * nsum)
-                v = exact_minus_square(ep.A32 + (long long)row * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows);
-            }
-            if (ep.do_epilogue) v = __fadd_rn(v, crow[col]);
-            drow[col] = v;
+        for (int j = 0; j < 32; j++) tile[lane * 33 + j] = r[j];
+        __syncwarp();
+        const int col = n0 + c0 + lane;
+        const bool col_ok = col < N;
+        const float nb = (ep.op == SIMD2_MINUS_SQUARE && col_ok) ? ep.norm_b[col] : 0.f;
+#pragma unroll 4
+        for (int rr = 0; rr < 32; rr++) {
+          const int row = row0 + rr;
+          if (row >= M) break;
+          const uint32_t x = tile[rr * 33 + lane];
+          if (!col_ok) continue;
+          float v = __uint_as_float(x);
+          if (ep.op == SIMD2_MINUS_SQUARE) {
+            const float nsum = ep.norm_a[row] + nb;
+            v = __fmaf_rn(-2.0f, v, nsum);
+            if (v < ep.band * nsum)
+              v = exact_minus_square(ep.A32 + (long long)row * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows);
           }
+          if (ep.do_epilogue) v = __fadd_rn(v, static_cast<const float*>(ep.C)[(long long)row * ep.ldc + col]);
+          static_cast<float*>(ep.D)[(long long)row * ep.ldd + col] = v;
         }
+        __syncwarp();
       }
     }
   }

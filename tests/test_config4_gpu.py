@@ -1,0 +1,66 @@
+"""The dense-contraction workloads at full size, checked through properties
+that do not need the full CPU result:
+  * or_and transitive closure, N = 16384, edge probability 2/N (INT8 tensor
+    cores): sampled rows equal BFS reachability from those vertices;
+  * k-NN, Q = 16384 queries x R = 65536 references x D = 128, k = 16, with 5 %
+    near-duplicate queries: sampled queries against the FP64 oracle;
+  * plus_mul 8192^3 on N(0,1) (BF16 hi/lo): sampled rows inside the FP64 bound.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+from scipy.sparse.csgraph import breadth_first_order
+import torch
+
+import oracle
+import simd2_b200 as s2
+from simd2_b200 import datagen
+
+pytestmark = pytest.mark.gpu
+
+
+def test_orand_closure_16384(cuda):
+    n = 16384
+    rng = np.random.default_rng(44)
+    m = int(2 * n)  # expected edges at p = 2/N
+    src = rng.integers(0, n, m)
+    dst = rng.integers(0, n, m)
+    X = torch.zeros((n, n), dtype=torch.uint8, device=cuda)
+    X[torch.from_numpy(src).to(cuda), torch.from_numpy(dst).to(cuda)] = 1
+    X.fill_diagonal_(1)
+    it = s2.closure("or_and", X)
+    assert 2 <= it <= 40
+    adj = sp.csr_matrix((np.ones(m, np.int8), (src, dst)), shape=(n, n))
+    for v in rng.choice(n, size=64, replace=False):
+        reach = np.zeros(n, np.uint8)
+        reach[breadth_first_order(adj, int(v), directed=True, return_predecessors=False)] = 1
+        np.testing.assert_array_equal(X[int(v)].cpu().numpy(), reach, err_msg=f"row {v}")
+    assert s2.device_status() == 0
+
+
+def test_knn_16384_x_65536(cuda):
+    q, r = datagen.point_cloud(16384, 65536, 128, seed=4, dup_frac=0.05)
+    Q, R = torch.from_numpy(q).to(cuda), torch.from_numpy(r).to(cuda)
+    dist, idx = s2.knn(Q, R, 16)
+    torch.cuda.synchronize()
+    dist, idx = dist.cpu().numpy(), idx.cpu().numpy()
+    sample = np.random.default_rng(0).choice(16384, size=48, replace=False)
+    want_d, want_i, want_sq = oracle.knn(q[sample], r, 16)
+    match = (idx[sample] == want_i).mean()
+    assert match >= 0.99, match
+    rel = np.abs(dist[sample].astype(np.float64) - np.sqrt(want_sq)) / np.maximum(np.sqrt(want_sq), 1e-30)
+    assert rel.max() < 5e-3, rel.max()
+
+
+def test_plus_mul_8192(cuda):
+    n = 8192
+    a, b, _ = datagen.semiring_operands("plus_mul", n, n, 1, seed=5)
+    rng = np.random.default_rng(6)
+    a = rng.standard_normal((n, n), dtype=np.float32)
+    b = rng.standard_normal((n, n), dtype=np.float32)
+    D = s2.srgemm("plus_mul", torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda))
+    rows = rng.choice(n, size=8, replace=False)
+    got = D[torch.from_numpy(rows).to(cuda)].cpu().numpy().astype(np.float64)
+    want = oracle.srgemm_f64("plus_mul", a[rows], b)
+    bound = (4 * 2.0 ** -16 + 2 * n * 2.0 ** -24) * (np.abs(a[rows]).astype(np.float64) @ np.abs(b))
+    assert np.all(np.abs(got - want) <= bound)
