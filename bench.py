@@ -316,16 +316,19 @@ def extra_measurements(args, dev):
     del X
     q, r = datagen.point_cloud(16384, 65536, 128, seed=4, dup_frac=0.05)
     Q, R = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
-    s2.knn(Q[:1024], R, 16)  # warm-up
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    s2.knn(Q, R, 16)
-    ev1.record()
-    torch.cuda.synchronize()
-    kms = ev0.elapsed_time(ev1)
-    cfg4["knn_16384x65536x128_k16"] = {"ms": kms, "queries_per_s": 16384 / kms * 1e3,
-                                       "gops": 2.0 * 16384 * 65536 * 128 / kms / 1e6,
-                                       "how": "simd2_knn, CUDA events (BF16 hi/lo minus_square + top-k + sqrt)"}
+    for mode in ("fused", "materialised"):
+        s2.knn(Q[:1024], R, 16, mode=mode)  # warm-up
+        ev0.record()
+        s2.knn(Q, R, 16, mode=mode)
+        ev1.record()
+        torch.cuda.synchronize()
+        kms = ev0.elapsed_time(ev1)
+        cfg4[f"knn_16384x65536x128_k16_{mode}"] = {
+            "ms": kms, "queries_per_s": 16384 / kms * 1e3, "gops": 2.0 * 16384 * 65536 * 128 / kms / 1e6,
+            "how": "simd2_knn_ex, CUDA events: " + (
+                "selection inside the BF16 hi/lo distance MMA's epilogue, then a per-query merge" if mode == "fused"
+                else "BF16 hi/lo minus_square blocks of 1 GiB written, then top-k + sqrt")}
     del Q, R
     A = torch.randn((8192, 8192), device=dev)
     B = torch.randn((8192, 8192), device=dev)
@@ -399,18 +402,22 @@ def main():
         from simd2_b200 import datagen
         q, r = datagen.point_cloud(args.knn_q, args.knn_r, 128, seed=4, dup_frac=0.05)
         Q, R = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
-        for _ in range(max(args.warmup, 1)):
-            s2.knn(Q, R, 16)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record()
-        for _ in range(args.steps):
-            s2.knn(Q, R, 16)
-        ev1.record()
-        torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1) / args.steps
+        out = {"workload": f"knn Q={args.knn_q} R={args.knn_r} D=128 k=16"}
+        for mode in ("fused", "materialised"):
+            for _ in range(max(args.warmup, 1)):
+                s2.knn(Q, R, 16, mode=mode)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with s2.KernelTimer() as kt:
+                ev0.record()
+                for _ in range(args.steps):
+                    s2.knn(Q, R, 16, mode=mode)
+                ev1.record()
+                torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1) / args.steps
+            out[mode] = {"ms": ms, "queries_per_s": args.knn_q / ms * 1e3,
+                         "distance_kernel_ms": kt.by_kind.get("tensor", (0, 0, 0))[0] / args.steps}
         if rank == 0:
-            print(json.dumps({"workload": f"knn Q={args.knn_q} R={args.knn_r} D=128 k=16", "ms": ms,
-                              "queries_per_s": args.knn_q / ms * 1e3}), flush=True)
+            print(json.dumps(out), flush=True)
         return 0
 
     if args.workload == "batched":

@@ -194,6 +194,19 @@ int simd2_mlp_adam(float* params, const float* grad, float* m, float* v, float l
 int simd2_knn(const float* query, int Q, int ldq, const float* ref, int R, int ldr, int D, int k,
               float* out_dist, int32_t* out_idx, int ldo, cudaStream_t stream);
 
+/* Execution strategy of simd2_knn_ex.  Both give bit-identical results. */
+typedef enum {
+  SIMD2_KNN_AUTO = 0,         /* FUSED when D <= 128, else MATERIALISED */
+  SIMD2_KNN_FUSED = 1,        /* selection inside the distance MMA's epilogue; D <= 128
+                                 (SIMD2_ERR_UNSUPPORTED otherwise) */
+  SIMD2_KNN_MATERIALISED = 2  /* distance blocks of ~1 GiB written, then selected */
+} simd2_knn_mode;
+
+/* simd2_knn with an explicit strategy; simd2_knn(...) is
+ * simd2_knn_ex(..., SIMD2_KNN_AUTO, stream). */
+int simd2_knn_ex(const float* query, int Q, int ldq, const float* ref, int R, int ldr, int D, int k,
+                 float* out_dist, int32_t* out_idx, int ldo, int mode, cudaStream_t stream);
+
 /* srgemm with FP16 A and B (row-major, __half*), FP32 C and D: the entry
  * behind tensor_srgemm (kernel/tensor_srgemm.cuh:197-218).  The halves are
  * widened to FP32 exactly and the FP32 engine runs; or_and treats any

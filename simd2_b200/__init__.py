@@ -77,6 +77,8 @@ def lib() -> ctypes.CDLL:
         L.simd2_closure_batched.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, PI, P]
         L.simd2_knn.argtypes = [P, I, I, P, I, I, I, I, P, P, I, P]
         L.simd2_knn.restype = I
+        L.simd2_knn_ex.argtypes = [P, I, I, P, I, I, I, I, P, P, I, I, P]
+        L.simd2_knn_ex.restype = I
         L.simd2_selftest_timeout.argtypes = [ctypes.c_uint]
         L.simd2_selftest_timeout.restype = I
         L.simd2_timeout_site.argtypes = []
@@ -292,20 +294,28 @@ def closure_batched(op: str, mats, max_iter: int = 500, conv: str = "exact", str
     return list(it)[:count]
 
 
-def knn(query: torch.Tensor, ref: torch.Tensor, k: int, stream=None):
+KNN_MODES = {"auto": 0, "fused": 1, "materialised": 2}
+
+
+def knn(query: torch.Tensor, ref: torch.Tensor, k: int, stream=None, mode: str = "auto"):
     """k nearest references of every query (Euclidean): (dist [Q,k] float32, idx [Q,k] int32).
 
     Mirrors the PLD path of the reference (minus_square srgemm, insertion-sort
-    top-k, sqrt); outputs are query-major.
+    top-k, sqrt); outputs are query-major.  ``mode``: "fused" selects inside
+    the distance kernel (D <= 128), "materialised" writes distance blocks and
+    selects from them, "auto" picks fused when it applies; results are
+    bit-identical.
     """
     Q, D = query.shape
     R, D2 = ref.shape
     if D != D2:
         raise ValueError("query and ref dimensions differ")
+    if mode not in KNN_MODES:
+        raise ValueError(f"unknown k-NN mode {mode!r}")
     dist = torch.empty((Q, k), dtype=torch.float32, device=query.device)
     idx = torch.empty((Q, k), dtype=torch.int32, device=query.device)
-    rc = lib().simd2_knn(query.data_ptr(), Q, _mat(query, "query"), ref.data_ptr(), R, _mat(ref, "ref"), D, k,
-                         dist.data_ptr(), idx.data_ptr(), k, _stream(stream))
+    rc = lib().simd2_knn_ex(query.data_ptr(), Q, _mat(query, "query"), ref.data_ptr(), R, _mat(ref, "ref"), D, k,
+                            dist.data_ptr(), idx.data_ptr(), k, KNN_MODES[mode], _stream(stream))
     _check(rc, "knn")
     return dist, idx
 

@@ -21,6 +21,7 @@
 #include "closure_batched.cuh"
 #include "mlp.cuh"
 #include "knn.cuh"
+#include "knn_fused.cuh"
 
 namespace simd2 {
 namespace {
@@ -1461,6 +1462,54 @@ int knn_topk_launch(const float* dist, long long ldd, int rows, int cols, float*
   return SIMD2_OK;
 }
 
+// Reference chunks per 128 queries for the fused kernel: one CTA per
+// (query block, chunk), so the grid has qblocks * chunks CTAs, one per SM at a
+// time.  Minimises waves * (tiles per chunk + a fixed cost of about three
+// tiles: TMEM allocation, query load, pipeline fill and drain).
+int knn_fused_chunks(int qblocks, int tiles, int sms, long long max_lists) {
+  int best = 1;
+  double best_cost = 1e300;
+  for (int c = 1; c <= tiles; c++) {
+    const int tpc = (tiles + c - 1) / c;
+    const int chunks = (tiles + tpc - 1) / tpc;
+    if (chunks != c) continue;
+    if (2LL * chunks > max_lists) break;
+    const long long units = (long long)qblocks * chunks;
+    const double cost = (double)((units + sms - 1) / sms) * (tpc + 3.0);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = c;
+    }
+  }
+  return best;
+}
+
+template <int KT>
+int knn_fused_launch(const CUtensorMap& mqh, const CUtensorMap& mql, const CUtensorMap& mrh, const CUtensorMap& mrl,
+                     const KnnFusedArgs& args, int qblocks, float* od, int32_t* oi, long long ldo, int kout,
+                     cudaStream_t stream) {
+  static bool configured[64] = {};
+  int dev = 0;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
+  if (!configured[dev]) {
+    SIMD2_CUDA_TRY(
+        cudaFuncSetAttribute(knn_fused_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kKfSmemBytes));
+    configured[dev] = true;
+  }
+  auto* ev = prof_slot(2LL * args.Q * args.R * args.D, kProfTensor);
+  if (ev) cudaEventRecord(ev->first, stream);
+  knn_fused_kernel<KT><<<qblocks * args.chunks, kKfThreads, kKfSmemBytes, stream>>>(mqh, mql, mrh, mrl, args);
+  count_launch();
+  if (ev) cudaEventRecord(ev->second, stream);
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  knn_merge_kernel<KT><<<grid_for((long long)args.Q * 32), 256, 0, stream>>>(args.part_d, args.part_i, args.Q,
+                                                                            2 * args.chunks, od, oi, ldo, kout);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
 // Query rows per chunk so that one chunk's distance block stays near 1 GiB.
 int knn_chunk_rows(int Q, int R) {
   long long rows = (1LL << 30) / (4LL * std::max(R, 1));
@@ -1471,10 +1520,105 @@ int knn_chunk_rows(int Q, int R) {
 }  // namespace
 }  // namespace simd2
 
+namespace simd2 {
+namespace {
+
+// The fused path: operand prep, one knn_fused_kernel launch over all
+// (query block, reference chunk) units, and the per-query merge.
+int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int ldr, int D, int k, float* out_dist,
+              int32_t* out_idx, int ldo, cudaStream_t stream) {
+  const int Dp = round_up(D, 8);
+  const int KT = k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
+  const int qblocks = (Q + kKfBM - 1) / kKfBM;
+  const int tiles = (R + kKfBN - 1) / kKfBN;
+  // partial lists: at most 256 MiB of (distance, index) pairs
+  const long long max_lists = std::max(2LL, (256LL << 20) / (8LL * KT * std::max(Q, 1)));
+  int dev = 0, sms = 148;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int chunks = knn_fused_chunks(qblocks, tiles, sms, max_lists);
+  const int tpc = (tiles + chunks - 1) / chunks;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
+  const size_t qhi = take((size_t)Q * Dp * 2), qlo = take((size_t)Q * Dp * 2);
+  const size_t rhi = take((size_t)R * Dp * 2), rlo = take((size_t)R * Dp * 2);
+  const size_t nq = take((size_t)Q * 4), nr = take((size_t)tiles * kKfBN * 4), tm = take((size_t)tiles * 4);
+  const size_t pd = take((size_t)Q * 2 * chunks * KT * 4), pi = take((size_t)Q * 2 * chunks * KT * 4);
+  const size_t rf = take((size_t)qblocks * chunks * 4);
+  void* p = nullptr;
+  int rc = get_workspace(stream, off, &p);
+  if (rc) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  auto* q_hi = reinterpret_cast<__nv_bfloat16*>(ws + qhi);
+  auto* q_lo = reinterpret_cast<__nv_bfloat16*>(ws + qlo);
+  auto* r_hi = reinterpret_cast<__nv_bfloat16*>(ws + rhi);
+  auto* r_lo = reinterpret_cast<__nv_bfloat16*>(ws + rlo);
+  float* n_q = reinterpret_cast<float*>(ws + nq);
+  float* n_r = reinterpret_cast<float*>(ws + nr);
+  float* t_max = reinterpret_cast<float*>(ws + tm);
+  split_rows_bf16_kernel<<<grid_for((long long)Q * Dp), 256, 0, stream>>>(query, ldq, Q, D, q_hi, q_lo, Dp);
+  split_rows_bf16_kernel<<<grid_for((long long)R * Dp), 256, 0, stream>>>(ref, ldr, R, D, r_hi, r_lo, Dp);
+  row_norms_kernel<<<grid_for((long long)Q * 32), 256, 0, stream>>>(query, ldq, Q, D, n_q);
+  row_norms_kernel<<<grid_for((long long)R * 32), 256, 0, stream>>>(ref, ldr, R, D, n_r);
+  for (int i = 0; i < 4; i++) count_launch();
+  const int pad = tiles * kKfBN - R;
+  if (pad > 0) {
+    // references past R: +inf norm, so their distances never enter a list
+    fill_kernel<float><<<grid_for(pad), 256, 0, stream>>>(n_r + R, pad, 1, pad, __builtin_inff());
+    count_launch();
+  }
+  tile_max_kernel<<<grid_for((long long)tiles * 32), 256, 0, stream>>>(n_r, R, tiles, t_max);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  const auto BF = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  const auto SW = CU_TENSOR_MAP_SWIZZLE_128B;
+  CUtensorMap mqh, mql, mrh, mrl;
+  if ((rc = make_map_2d(&mqh, BF, 2, q_hi, Q, Dp, Dp, 64, kKfBM, SW))) return rc;
+  if ((rc = make_map_2d(&mql, BF, 2, q_lo, Q, Dp, Dp, 64, kKfBM, SW))) return rc;
+  if ((rc = make_map_2d(&mrh, BF, 2, r_hi, R, Dp, Dp, 64, kKfBN, SW))) return rc;
+  if ((rc = make_map_2d(&mrl, BF, 2, r_lo, R, Dp, Dp, 64, kKfBN, SW))) return rc;
+  KnnFusedArgs a{};
+  a.Q = Q;
+  a.R = R;
+  a.D = D;
+  a.panels = (Dp + 63) / 64;
+  a.chunks = chunks;
+  a.tiles_per_chunk = tpc;
+  a.num_tiles = tiles;
+  a.norm_q = n_q;
+  a.norm_r = n_r;
+  a.tile_nrmax = t_max;
+  a.q32 = query;
+  a.ldq = ldq;
+  a.r32 = ref;
+  a.ldr = ldr;
+  a.band = kMinusSquareBand;
+  a.part_d = reinterpret_cast<float*>(ws + pd);
+  a.part_i = reinterpret_cast<int32_t*>(ws + pi);
+  a.ready = reinterpret_cast<unsigned*>(ws + rf);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(a.ready, 0, (size_t)qblocks * chunks * 4, stream));
+  switch (KT) {
+    case 4: return knn_fused_launch<4>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
+    case 8: return knn_fused_launch<8>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
+    case 16: return knn_fused_launch<16>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
+    default: return knn_fused_launch<32>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
+  }
+}
+
+}  // namespace
+}  // namespace simd2
+
 extern "C" int simd2_knn(const float* query, int Q, int ldq, const float* ref, int R, int ldr, int D, int k,
                          float* out_dist, int32_t* out_idx, int ldo, cudaStream_t stream) {
+  return simd2_knn_ex(query, Q, ldq, ref, R, ldr, D, k, out_dist, out_idx, ldo, SIMD2_KNN_AUTO, stream);
+}
+
+extern "C" int simd2_knn_ex(const float* query, int Q, int ldq, const float* ref, int R, int ldr, int D, int k,
+                            float* out_dist, int32_t* out_idx, int ldo, int mode, cudaStream_t stream) {
   using namespace simd2;
   if (Q < 0 || R < 0 || D < 0 || k < 1 || k > kKnnMaxK || ldo < k) return SIMD2_ERR_INVALID_ARG;
+  if (mode != SIMD2_KNN_AUTO && mode != SIMD2_KNN_FUSED && mode != SIMD2_KNN_MATERIALISED)
+    return SIMD2_ERR_INVALID_ARG;
   if (Q == 0) return SIMD2_OK;
   if (!query || !out_dist || !out_idx || ldq < D || (R > 0 && (!ref || ldr < D)) || R > (1 << 21) || D == 0)
     return SIMD2_ERR_INVALID_ARG;
@@ -1490,6 +1634,9 @@ extern "C" int simd2_knn(const float* query, int Q, int ldq, const float* ref, i
     return SIMD2_OK;
   }
   const int Dp = round_up(D, 8);
+  const bool fused = mode == SIMD2_KNN_FUSED || (mode == SIMD2_KNN_AUTO && Dp <= 64 * kKfMaxPanels);
+  if (fused && Dp > 64 * kKfMaxPanels) return SIMD2_ERR_UNSUPPORTED;
+  if (fused) return knn_fused(query, Q, ldq, ref, R, ldr, D, k, out_dist, out_idx, ldo, stream);
   const int Qc = knn_chunk_rows(Q, R);
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32)
                     float* __restrict__ out_d, int32_t* __restrict__ out_i, long long ldo, int kout, int take_sqrt) {
   __shared__ float s_d[kKnnWarps][K];
   __shared__ int s_i[kKnnWarps][K];
+  __shared__ float s_scr[8][kKnnWarps * 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const float inf = __int_as_float(0x7f800000);
   for (int r = blockIdx.x; r < rows; r += gridDim.x) {
@@ -80,10 +81,20 @@ __global__ void __launch_bounds__(kKnnWarps * 32)
           v1.z = d + 2 < c1 ? row[d + 2] : inf;
         }
         const float vals[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+        uint32_t mask = 0;
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int idx = (u < 4 ? c : d) + (u & 3);
-          if (vals[u] < bd[K - 1]) topk_insert<K>(bd, bi, vals[u], col_base + idx);
+        for (int u = 0; u < 8; u++) mask |= (vals[u] < bd[K - 1] ? 1u : 0u) << u;
+        if (mask) {
+          // one copy of the insertion code; the values go through this
+          // thread's shared-memory column for indexed access
+#pragma unroll
+          for (int u = 0; u < 8; u++) s_scr[u][threadIdx.x] = vals[u];
+          do {
+            const int u = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const float v = s_scr[u][threadIdx.x];
+            if (v < bd[K - 1]) topk_insert<K>(bd, bi, v, col_base + (u < 4 ? c : d) + (u & 3));
+          } while (mask);
         }
       }
     } else {

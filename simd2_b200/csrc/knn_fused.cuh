@@ -1,0 +1,437 @@
+// knn_fused.cuh -- k-NN with the distance block never written to memory.
+//
+// The materialised path (knn.cuh) writes the Q x R squared-distance matrix
+// with the tensor-core minus_square kernel and reads it back for selection:
+// 2 x 4 bytes of HBM traffic per (query, reference) pair.  Here the top-k
+// selection runs in the epilogue of the distance MMA, so a pair costs no HBM
+// traffic at all; what remains is reading the reference points (BF16 hi/lo,
+// from L2 after the first CTA touches them) and writing k candidates per
+// query and unit.
+//
+// Work unit = 128 queries x a chunk of reference tiles (256 references each).
+// One CTA per unit, 10 warps:
+//   warp 0 lane 0  -- TMA producer: the unit's query panels (BF16 hi and lo,
+//                     64-element K panels, 128-byte swizzle) once, then per
+//                     reference tile and K panel its hi and lo parts through
+//                     a 5-deep ring of 32 KiB stages,
+//   warp 1 lane 0  -- MMA issuer: per reference tile q.r ~ qh.rh + qh.rl + ql.rh
+//                     (tcgen05.mma kind::f16, M=128, N=256, FP32 accumulate)
+//                     into one of two TMEM accumulators (2 x 256 columns), so
+//                     the MMAs of tile t+1 run while tile t is selected,
+//   warps 2..9     -- selection: warp w reads TMEM lanes 32(w%4).. (its 32
+//                     queries, lane = query) and half (w-2)/4 of the 256
+//                     columns; each thread keeps the k smallest
+//                     (distance, index) pairs of its query and column half
+//                     in registers.
+// Distances are formed exactly as the materialised minus_square epilogue
+// forms them (|q|^2 + |r|^2 - 2 q.r with the FP64-accumulated norms rounded
+// to FP32, and the exact FP32 sum_k (q_k - r_k)^2 inside the cancellation
+// band), so both paths select from bit-identical values.  A candidate is
+// examined only when it can matter: v < max(thr, band * (|q|^2 + max |r|^2
+// over the tile)), thr = min(this list's k-th, the k-th of any finished
+// earlier chunk of the same queries); everything else costs an FADD, an FFMA
+// and a compare.
+//
+// Each unit writes, per query, two sorted lists of k (one per column half);
+// knn_merge_kernel merges the 2 x chunks lists of a query by (distance,
+// index) and writes the k results with their square roots.  Ties keep the
+// lower reference index first, the order of apps/pld/emulation/knncuda.cu:
+// 171-238 (insertion sort over increasing reference index).
+#pragma once
+#include "common.cuh"
+#include "knn.cuh"
+#include "tc_gemm.cuh"
+
+namespace simd2 {
+
+constexpr int kKfBM = 128;                     // queries per unit (TMEM lanes)
+constexpr int kKfBN = 256;                     // references per tile (MMA N)
+constexpr int kKfMaxPanels = 2;                // D <= 128: two 64-element K panels
+constexpr int kKfStages = 5;                   // B ring depth (2.5 K panels of hi + lo)
+constexpr int kKfATile = kKfBM * 128;          // 16 KiB: one K panel of 128 query rows
+constexpr int kKfBTile = kKfBN * 128;          // 32 KiB: one K panel of 256 reference rows
+constexpr int kKfEpiWarps = 8;
+constexpr int kKfThreads = (2 + kKfEpiWarps) * 32;
+constexpr int kKfTmemCols = 512;               // two 128 x 256 FP32 accumulators
+constexpr size_t kKfSmemBytes =
+    (size_t)kKfMaxPanels * 2 * kKfATile + (size_t)kKfStages * kKfBTile + 1024 /* align */ + 256 /* barriers */;
+
+struct KnnFusedArgs {
+  int Q, R, D;
+  int panels;             // ceil(round_up(D, 8) / 64), 1 or 2
+  int chunks;             // reference chunks (units per 128 queries)
+  int tiles_per_chunk;    // reference tiles of 256 per chunk
+  int num_tiles;          // ceil(R / 256)
+  const float* norm_q;    // [Q]
+  const float* norm_r;    // [num_tiles * 256], +inf past R
+  const float* tile_nrmax;// [num_tiles]: max |r|^2 over the tile's valid references
+  const float* q32;       // FP32 queries (exact recompute), row pitch ldq
+  long long ldq;
+  const float* r32;       // FP32 references, row pitch ldr
+  long long ldr;
+  float band;
+  float* part_d;          // [Q][2 * chunks][K]
+  int32_t* part_i;
+  unsigned* ready;        // [query blocks][chunks]: 1 once the unit's lists are written (zeroed per call)
+};
+
+// 32-way register select by a runtime index: a 5-level tree of selects, so
+// the array stays in registers.
+__device__ __forceinline__ uint32_t pick32(const uint32_t (&r)[32], int j) {
+  uint32_t a[16], b[8], c[4], d[2];
+#pragma unroll
+  for (int i = 0; i < 16; i++) a[i] = (j & 1) ? r[2 * i + 1] : r[2 * i];
+#pragma unroll
+  for (int i = 0; i < 8; i++) b[i] = (j & 2) ? a[2 * i + 1] : a[2 * i];
+#pragma unroll
+  for (int i = 0; i < 4; i++) c[i] = (j & 4) ? b[2 * i + 1] : b[2 * i];
+#pragma unroll
+  for (int i = 0; i < 2; i++) d[i] = (j & 8) ? c[2 * i + 1] : c[2 * i];
+  return (j & 16) ? d[1] : d[0];
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Pruning bound from the finished units of earlier chunks of this query
+// block: each of their lists holds K pairs no larger than its last distance,
+// all at lower reference indices than this chunk's, so a candidate of this
+// chunk at or above that distance is outranked K times and cannot be
+// selected.  +inf when no earlier unit of the query block has finished.
+template <int K>
+__device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblock, int chunk, int row) {
+  float T = __int_as_float(0x7f800000);
+  for (int cc = chunk - 1; cc >= 0 && cc >= chunk - 4; cc--) {
+    if (ld_acquire_gpu(a.ready + (long long)qblock * a.chunks + cc)) {
+      const long long base = ((long long)row * (2 * a.chunks) + 2 * cc) * K;
+      T = fminf(T, fminf(__ldcg(a.part_d + base + K - 1), __ldcg(a.part_d + base + 2 * K - 1)));
+    }
+  }
+  return T;
+}
+
+template <int K>
+__global__ void __launch_bounds__(kKfThreads, 1)
+    knn_fused_kernel(const __grid_constant__ CUtensorMap tmQh, const __grid_constant__ CUtensorMap tmQl,
+                     const __grid_constant__ CUtensorMap tmRh, const __grid_constant__ CUtensorMap tmRl,
+                     KnnFusedArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = smem;                                    // [panel][hi, lo] 16 KiB each
+  uint8_t* sB = smem + kKfMaxPanels * 2 * kKfATile;      // [stage] 32 KiB each
+  uint64_t* a_full = reinterpret_cast<uint64_t*>(sB + kKfStages * kKfBTile);
+  uint64_t* full = a_full + 1;
+  uint64_t* empty = full + kKfStages;
+  uint64_t* acc_full = empty + kKfStages;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* fin = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
+
+  // chunk-major unit order: the CTAs resident at one time share reference chunks in L2
+  const int qblocks = (a.Q + kKfBM - 1) / kKfBM;
+  const int chunk = blockIdx.x / qblocks;
+  const int m0 = (blockIdx.x - chunk * qblocks) * kKfBM;
+  const int t0 = chunk * a.tiles_per_chunk;
+  const int ntiles = min(a.num_tiles, t0 + a.tiles_per_chunk) - t0;
+  const int P = a.panels;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    mbar_init(a_full, 1);
+    for (int s = 0; s < kKfStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int s = 0; s < 2; s++) {
+      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_empty[s], kKfEpiWarps);
+    }
+    mbar_init(fin, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kKfTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer ----------------
+      prefetch_tensormap(&tmQh);
+      prefetch_tensormap(&tmRh);
+      mbar_arrive_expect_tx(a_full, 2 * P * kKfATile);
+      for (int p = 0; p < P; p++) {
+        tma_load_2d(sA + (2 * p) * kKfATile, &tmQh, a_full, p * 64, m0);
+        tma_load_2d(sA + (2 * p + 1) * kKfATile, &tmQl, a_full, p * 64, m0);
+      }
+      int j = 0;
+      bool ok = true;
+      for (int t = 0; t < ntiles && ok; t++) {
+        const int n0 = (t0 + t) * kKfBN;
+        for (int p = 0; p < P && ok; p++) {
+          for (int h = 0; h < 2; h++, j++) {  // panel p: hi stage, then lo stage
+            const int s = j % kKfStages;
+            if (!mbar_wait(&empty[s], ((j / kKfStages) & 1) ^ 1)) {
+              report_timeout(111);
+              ok = false;
+              break;
+            }
+            mbar_arrive_expect_tx(&full[s], kKfBTile);
+            tma_load_2d(sB + s * kKfBTile, h == 0 ? &tmRh : &tmRl, &full[s], p * 64, n0);
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---------------- MMA issuer ----------------
+      bool ok = mbar_wait(a_full, 0);
+      if (!ok) report_timeout(112);
+      tc_fence_after();
+      const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+      int j = 0;
+      for (int t = 0; t < ntiles && ok; t++) {
+        const int acc = t & 1;
+        if (!mbar_wait(&acc_empty[acc], ((t >> 1) & 1) ^ 1)) {
+          report_timeout(113);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + acc * kKfBN;
+        for (int p = 0; p < P; p++, j += 2) {
+          // stages j (hi) and j+1 (lo) hold K panel p of the tile
+          const int sh = j % kKfStages, sl = (j + 1) % kKfStages;
+          if (!mbar_wait(&full[sh], (j / kKfStages) & 1) || !mbar_wait(&full[sl], ((j + 1) / kKfStages) & 1)) {
+            report_timeout(114);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t bh = b_base + sh * kKfBTile, bl = b_base + sl * kKfBTile;
+          const uint32_t ah = a_base + (2 * p) * kKfATile, al = ah + kKfATile;
+          // per 16-element K step: qh.rh, qh.rl, ql.rh -- the order of the
+          // materialised minus_square kernel, so the FP32 sums are identical
+#pragma unroll
+          for (int ks = 0; ks < 4; ks++) {
+            const uint32_t ko = ks * 32;  // 16 BF16 along the 128-byte row
+            tc_mma<0>(d, umma_desc_sw128(ah + ko), umma_desc_sw128(bh + ko), (p > 0 || ks > 0) ? 1u : 0u);
+            tc_mma<0>(d, umma_desc_sw128(ah + ko), umma_desc_sw128(bl + ko), 1u);
+            tc_mma<0>(d, umma_desc_sw128(al + ko), umma_desc_sw128(bh + ko), 1u);
+          }
+          tc_commit(&empty[sh]);
+          tc_commit(&empty[sl]);
+        }
+        if (ok) tc_commit(&acc_full[acc]);
+      }
+      tc_commit(fin);  // every MMA issued above has completed when fin flips
+    }
+  } else {
+    // ---------------- selection (warps 2..9) ----------------
+    const int quad = warp & 3;             // TMEM lane quadrant this warp may read
+    const int half = (warp - 2) >> 2;      // column half of the 256-column tile
+    const int row = m0 + quad * 32 + lane;
+    const bool row_ok = row < a.Q;
+    const float na = row_ok ? a.norm_q[row] : 0.f;
+    const float* qrow = a.q32 + (long long)(row_ok ? row : 0) * a.ldq;
+    const float inf = __int_as_float(0x7f800000);
+    float bd[K];
+    int bi[K];
+#pragma unroll
+    for (int u = 0; u < K; u++) {
+      bd[u] = inf;
+      bi[u] = 0x7fffffff;
+    }
+    bool ok = true;
+    const int qblock = m0 / kKfBM;
+    float prior = __int_as_float(0x7f800000);  // bound from earlier chunks' lists
+    for (int t = 0; t < ntiles; t++) {
+      const int acc = t & 1;
+      if (row_ok && (t & 7) == 0) prior = fminf(prior, knn_prior_bound<K>(a, qblock, chunk, row));
+      if (ok && !mbar_wait(&acc_full[acc], (t >> 1) & 1)) {
+        report_timeout(115);
+        ok = false;
+      }
+      ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
+      if (!ok) break;
+      tc_fence_after();
+      const int tile = t0 + t;
+      const int cbase = tile * kKfBN + half * 128;
+      // band * (|q|^2 + max |r|^2) bounds band * (|q|^2 + |r|^2) over the
+      // tile (FP32 addition is monotonic), so v >= lim rules out both the
+      // exact recompute and an insertion (which needs v < thr)
+      const float blim = a.band * (na + a.tile_nrmax[tile]);
+      float thr = fminf(bd[K - 1], prior);
+      float lim = fmaxf(thr, blim);
+      const uint32_t taddr = tmem + acc * kKfBN + half * 128 + ((uint32_t)(quad * 32) << 16);
+#pragma unroll 1
+      for (int c = 0; c < 4; c++) {
+        uint32_t r[32];
+        tmem_ld32(taddr + c * 32, r);
+        if (c == 3) {
+          // the accumulator is in registers: hand it back to the MMA warp
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[acc]);
+        }
+        // Hot pass: the distance of each of the 32 columns and a bit per
+        // column that may enter the list.  The insertion code exists once,
+        // below, so the loop body stays small enough for the instruction cache.
+        const float4* nb4 = reinterpret_cast<const float4*>(a.norm_r + cbase + c * 32);
+        uint32_t mask = 0;
+#pragma unroll
+        for (int q4 = 0; q4 < 8; q4++) {
+          const float4 nb = __ldg(nb4 + q4);
+          const float nbv[4] = {nb.x, nb.y, nb.z, nb.w};
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int jj = q4 * 4 + e;
+            const float v = __fmaf_rn(-2.0f, __uint_as_float(r[jj]), na + nbv[e]);
+            r[jj] = __float_as_uint(v);
+            mask |= (v < lim ? 1u : 0u) << jj;
+          }
+        }
+        // Rare pass, in increasing column order.
+        while (mask) {
+          const int j = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const int col = cbase + c * 32 + j;
+          float v = __uint_as_float(pick32(r, j));
+          const float nsum = na + a.norm_r[col];
+          if (v < a.band * nsum) v = exact_minus_square(qrow, a.r32, a.ldr, col, a.D, 1);
+          if (v < thr) {
+            topk_insert<K>(bd, bi, v, col);
+            thr = fminf(bd[K - 1], prior);
+            lim = fmaxf(thr, blim);
+          }
+        }
+      }
+    }
+    if (row_ok) {
+      const long long base = ((long long)row * (2 * a.chunks) + 2 * chunk + half) * K;
+#pragma unroll
+      for (int u = 0; u < K; u += 4) {
+        *reinterpret_cast<float4*>(a.part_d + base + u) = make_float4(bd[u], bd[u + 1], bd[u + 2], bd[u + 3]);
+        *reinterpret_cast<int4*>(a.part_i + base + u) = make_int4(bi[u], bi[u + 1], bi[u + 2], bi[u + 3]);
+      }
+    }
+    // publish: every selection thread's lists, then the unit's ready flag
+    __threadfence();
+    asm volatile("bar.sync 1, %0;" ::"r"(kKfEpiWarps * 32) : "memory");
+    if (warp == 2 && lane == 0 && ok) st_release_gpu(a.ready + (long long)qblock * a.chunks + chunk, 1u);
+  }
+
+  // every MMA has completed before TMEM is released
+  if (warp == 0) {
+    if (!mbar_wait(fin, 0)) report_timeout(116);
+    tc_fence_after();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kKfTmemCols) : "memory");
+  }
+}
+
+// Insert (v, i) into a list sorted by (distance, index); for merging lists
+// whose indices arrive in no particular order.
+template <int K>
+__device__ __forceinline__ void topk_insert_lex(float (&bd)[K], int (&bi)[K], float v, int i) {
+#pragma unroll
+  for (int t = K - 1; t > 0; t--) {
+    const bool shift = lex_less(v, i, bd[t - 1], bi[t - 1]);
+    const bool place = !shift && lex_less(v, i, bd[t], bi[t]);
+    bd[t] = shift ? bd[t - 1] : (place ? v : bd[t]);
+    bi[t] = shift ? bi[t - 1] : (place ? i : bi[t]);
+  }
+  if (lex_less(v, i, bd[0], bi[0])) {
+    bd[0] = v;
+    bi[0] = i;
+  }
+}
+
+// One warp per query: merges its `lists` sorted lists of K candidates into
+// the kout smallest by (distance, index), writes their square roots and
+// indices (-1 where fewer than kout references exist).
+template <int K>
+__global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict__ part_d,
+                                                        const int32_t* __restrict__ part_i, int rows, int lists,
+                                                        float* __restrict__ out_d, int32_t* __restrict__ out_i,
+                                                        long long ldo, int kout) {
+  const int lane = threadIdx.x & 31;
+  const float inf = __int_as_float(0x7f800000);
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
+    float bd[K];
+    int bi[K];
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+      bd[t] = inf;
+      bi[t] = 0x7fffffff;
+    }
+    for (int l = lane; l < lists; l += 32) {
+      const float* ld = part_d + ((long long)r * lists + l) * K;
+      const int32_t* li = part_i + ((long long)r * lists + l) * K;
+      for (int e = 0; e < K; e++) {
+        const float v = ld[e];
+        const int ix = li[e];
+        if (!lex_less(v, ix, bd[K - 1], bi[K - 1])) break;  // the list is sorted
+        topk_insert_lex<K>(bd, bi, v, ix);
+      }
+    }
+    // warp merge of the lanes' sorted lists
+    for (int t = 0; t < kout; t++) {
+      float v = bd[0];
+      int ix = bi[0];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, ix, o);
+        if (lex_less(v2, i2, v, ix)) {
+          v = v2;
+          ix = i2;
+        }
+      }
+      if (bd[0] == v && bi[0] == ix) {
+#pragma unroll
+        for (int u = 0; u < K - 1; u++) {
+          bd[u] = bd[u + 1];
+          bi[u] = bi[u + 1];
+        }
+        bd[K - 1] = inf;
+        bi[K - 1] = 0x7fffffff;
+      }
+      if (lane == 0) {
+        out_d[(long long)r * ldo + t] = sqrtf(fmaxf(v, 0.f));
+        out_i[(long long)r * ldo + t] = ix == 0x7fffffff ? -1 : ix;
+      }
+    }
+  }
+}
+
+// Per 256-reference tile: the largest |r|^2 among its valid references.
+__global__ void tile_max_kernel(const float* __restrict__ nr, int R, int tiles, float* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tiles; t += (gridDim.x * blockDim.x) >> 5) {
+    float m = -__int_as_float(0x7f800000);
+    for (int c = t * kKfBN + lane; c < min(R, (t + 1) * kKfBN); c += 32) m = fmaxf(m, nr[c]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) out[t] = m;
+  }
+}
+
+}  // namespace simd2

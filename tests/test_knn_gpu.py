@@ -63,3 +63,47 @@ def test_knn_ties_keep_lower_index(cuda):
     dist, idx = s2.knn(torch.from_numpy(q).to(cuda), torch.from_numpy(r).to(cuda), 6)
     want_d, want_i, _ = oracle.knn(q, r, 6)
     np.testing.assert_array_equal(idx.cpu().numpy(), want_i)
+
+
+@pytest.mark.parametrize("shape", [(300, 1000, 128, 16), (129, 257, 37, 5), (64, 4096, 128, 32), (1, 3, 8, 3),
+                                   (1000, 5000, 64, 8), (257, 70001, 100, 16), (130, 512, 128, 4),
+                                   (4096, 65536, 128, 16)])
+def test_knn_fused_matches_materialised(cuda, shape):
+    """The fused kernel (selection in the MMA epilogue) and the materialised
+    path (distance blocks, then selection) return identical bits.  The last
+    shape runs the fused grid in two waves, so second-wave units prune with
+    the lists of finished earlier chunks."""
+    Q, R, D, k = shape
+    q, r = datagen.point_cloud(Q, R, D, seed=Q * 7 + R, dup_frac=0.05)
+    Qt, Rt = torch.from_numpy(q).to(cuda), torch.from_numpy(r).to(cuda)
+    d1, i1 = s2.knn(Qt, Rt, min(k, R), mode="fused")
+    d2, i2 = s2.knn(Qt, Rt, min(k, R), mode="materialised")
+    assert torch.equal(i1, i2)
+    assert torch.equal(d1.view(torch.int32), d2.view(torch.int32))
+    assert s2.device_status() == 0
+
+
+def test_knn_fused_ties_and_fewer_refs_than_k(cuda):
+    """Duplicated references across reference tiles and chunks keep the lower
+    index first; with R < k the tail is +inf / -1, in both modes."""
+    rng = np.random.default_rng(5)
+    base = rng.standard_normal((300, 24)).astype(np.float32)
+    r = np.concatenate([base] * 4)  # copies 300 apart: different 256-wide tiles
+    q = base[:40] + np.float32(0.25)
+    Qt, Rt = torch.from_numpy(q).to(cuda), torch.from_numpy(r).to(cuda)
+    d, i = s2.knn(Qt, Rt, 8, mode="fused")
+    _, want_i, _ = oracle.knn(q, r, 8)
+    np.testing.assert_array_equal(i.cpu().numpy(), want_i)
+    small = torch.from_numpy(base[:5]).to(cuda)
+    d, i = s2.knn(Qt, small, 8, mode="fused")
+    assert torch.all(i[:, 5:] == -1) and torch.all(torch.isinf(d[:, 5:]))
+    d2, i2 = s2.knn(Qt, small, 8, mode="materialised")
+    assert torch.equal(i, i2) and torch.equal(d.view(torch.int32), d2.view(torch.int32))
+
+
+def test_knn_fused_rejects_wide_points(cuda):
+    q = torch.zeros(4, 200, device=cuda)
+    with pytest.raises(s2.Simd2Error):
+        s2.knn(q, q, 2, mode="fused")
+    d, i = s2.knn(q, q, 2)  # auto falls back to the materialised path
+    assert torch.all(d == 0)
