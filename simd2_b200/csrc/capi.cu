@@ -1503,8 +1503,12 @@ int knn_fused_launch(const CUtensorMap& mqh, const CUtensorMap& mql, const CUten
   count_launch();
   if (ev) cudaEventRecord(ev->second, stream);
   SIMD2_CUDA_TRY(cudaGetLastError());
-  knn_merge_kernel<KT><<<grid_for((long long)args.Q * 32), 256, 0, stream>>>(args.part_d, args.part_i, args.Q,
-                                                                            2 * args.chunks, od, oi, ldo, kout);
+  const int lists = 2 * args.chunks;
+  const int G = lists <= 2 ? 2 : lists <= 4 ? 4 : lists <= 8 ? 8 : lists <= 16 ? 16 : 32;
+  const int grid = grid_for((long long)(args.Q + 32 / G - 1) / (32 / G) * 32);
+  auto merge = G == 2 ? knn_merge_kernel<KT, 2> : G == 4 ? knn_merge_kernel<KT, 4> : G == 8 ? knn_merge_kernel<KT, 8>
+             : G == 16 ? knn_merge_kernel<KT, 16> : knn_merge_kernel<KT, 32>;
+  merge<<<grid, 256, 0, stream>>>(args.part_d, args.part_i, args.Q, lists, od, oi, ldo, kout);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;

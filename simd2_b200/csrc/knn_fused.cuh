@@ -364,17 +364,28 @@ __device__ __forceinline__ void topk_insert_lex(float (&bd)[K], int (&bi)[K], fl
   }
 }
 
-// One warp per query: merges its `lists` sorted lists of K candidates into
-// the kout smallest by (distance, index), writes their square roots and
-// indices (-1 where fewer than kout references exist).
-template <int K>
+// Merges each query's `lists` sorted lists of K candidates into the kout
+// smallest by (distance, index), writes their square roots and indices (-1
+// where fewer than kout references exist).
+// G = lanes per query (a power of two, 32 / G queries per warp).  When
+// lists <= G, lane l of a group loads list l whole into registers (16-byte
+// loads) and the group takes kout rounds of a (distance, index) argmin over
+// the lanes' heads, the winner shifting its list by one.  Otherwise each lane
+// first folds lists l, l+G, ... into one sorted list by insertion.
+template <int K, int G>
 __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict__ part_d,
                                                         const int32_t* __restrict__ part_i, int rows, int lists,
                                                         float* __restrict__ out_d, int32_t* __restrict__ out_i,
                                                         long long ldo, int kout) {
   const int lane = threadIdx.x & 31;
+  const int sub = lane & (G - 1);
   const float inf = __int_as_float(0x7f800000);
-  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
+  constexpr int kGroups = 32 / G;  // queries per warp
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  // the loop bound is uniform across the warp, so every lane takes the shuffles
+  for (int r0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kGroups; r0 < rows; r0 += nwarps * kGroups) {
+    const int r = r0 + lane / G;
+    const bool live = r < rows;
     float bd[K];
     int bi[K];
 #pragma unroll
@@ -382,22 +393,35 @@ __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict_
       bd[t] = inf;
       bi[t] = 0x7fffffff;
     }
-    for (int l = lane; l < lists; l += 32) {
-      const float* ld = part_d + ((long long)r * lists + l) * K;
-      const int32_t* li = part_i + ((long long)r * lists + l) * K;
-      for (int e = 0; e < K; e++) {
-        const float v = ld[e];
-        const int ix = li[e];
-        if (!lex_less(v, ix, bd[K - 1], bi[K - 1])) break;  // the list is sorted
-        topk_insert_lex<K>(bd, bi, v, ix);
+    if (live && lists <= G) {
+      if (sub < lists) {
+        const float4* ld = reinterpret_cast<const float4*>(part_d + ((long long)r * lists + sub) * K);
+        const int4* li = reinterpret_cast<const int4*>(part_i + ((long long)r * lists + sub) * K);
+#pragma unroll
+        for (int u = 0; u < K / 4; u++) {
+          const float4 v = ld[u];
+          const int4 w = li[u];
+          bd[4 * u] = v.x, bd[4 * u + 1] = v.y, bd[4 * u + 2] = v.z, bd[4 * u + 3] = v.w;
+          bi[4 * u] = w.x, bi[4 * u + 1] = w.y, bi[4 * u + 2] = w.z, bi[4 * u + 3] = w.w;
+        }
+      }
+    } else if (live) {
+      for (int l = sub; l < lists; l += G) {
+        const float* ld = part_d + ((long long)r * lists + l) * K;
+        const int32_t* li = part_i + ((long long)r * lists + l) * K;
+        for (int e = 0; e < K; e++) {
+          const float v = ld[e];
+          const int ix = li[e];
+          if (!lex_less(v, ix, bd[K - 1], bi[K - 1])) break;  // the list is sorted
+          topk_insert_lex<K>(bd, bi, v, ix);
+        }
       }
     }
-    // warp merge of the lanes' sorted lists
     for (int t = 0; t < kout; t++) {
       float v = bd[0];
       int ix = bi[0];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
+      for (int o = G / 2; o > 0; o >>= 1) {
         const float v2 = __shfl_xor_sync(0xffffffffu, v, o);
         const int i2 = __shfl_xor_sync(0xffffffffu, ix, o);
         if (lex_less(v2, i2, v, ix)) {
@@ -414,7 +438,7 @@ __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict_
         bd[K - 1] = inf;
         bi[K - 1] = 0x7fffffff;
       }
-      if (lane == 0) {
+      if (sub == 0 && live) {
         out_d[(long long)r * ldo + t] = sqrtf(fmaxf(v, 0.f));
         out_i[(long long)r * ldo + t] = ix == 0x7fffffff ? -1 : ix;
       }
