@@ -61,9 +61,11 @@ def parse_args():
     p.add_argument("--batched-count", type=int, default=4096)
     p.add_argument("--knn-q", type=int, default=16384)
     p.add_argument("--knn-r", type=int, default=65536)
-    p.add_argument("--workload", choices=("sweep", "batched", "knn"), default="sweep",
+    p.add_argument("--workload", choices=("sweep", "batched", "knn", "rowpanel"), default="sweep",
                    help="sweep: the nine-semiring srgemm line (default); batched: only the batched closure "
-                        "(used for profiling runs)")
+                        "(used for profiling runs); knn: the k-NN modes; rowpanel: one or_and closure with "
+                        "X's rows split across the ranks")
+    p.add_argument("--rowpanel-n", type=int, default=16384)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -418,6 +420,46 @@ def main():
                          "distance_kernel_ms": kt.by_kind.get("tensor", (0, 0, 0))[0] / args.steps}
         if rank == 0:
             print(json.dumps(out), flush=True)
+        return 0
+
+    if args.workload == "rowpanel":
+        from simd2_b200.shard import closure_rowpanel, max_over_ranks, panel_bounds
+        n = args.rowpanel_n
+        rng = np.random.default_rng(44)
+        m = 2 * n  # or_and reachability closure, edge probability 2/n
+        x = np.zeros((n, n), np.uint8)
+        x[rng.integers(0, n, m), rng.integers(0, n, m)] = 1
+        np.fill_diagonal(x, 1)
+        P, bounds = panel_bounds(n, world)
+        start, stop = bounds[rank]
+        base = torch.zeros((P, n), dtype=torch.uint8, device=dev)
+        base[: stop - start] = torch.from_numpy(x[start:stop]).to(dev)
+        del x
+        block = base.clone()
+        closure_rowpanel("or_and", block, n)  # warm-up (same collective sequence on every rank)
+        times, its = [], 0
+        for _ in range(max(args.steps, 1)):
+            block.copy_(base)
+            barrier()
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            its = closure_rowpanel("or_and", block, n)
+            ev1.record()
+            torch.cuda.synchronize()
+            barrier()
+            times.append(ev0.elapsed_time(ev1))
+        ms = sorted(times)[len(times) // 2]
+        if world > 1:
+            ms = max_over_ranks(ms, device=dev)
+        if rank == 0:
+            print(json.dumps({"workload": f"or_and closure n={n}, rows split over {world} rank(s)", "ms": ms,
+                              "iters": its, "gops": 2.0 * n ** 3 * its / ms / 1e6, "n_gpus": world,
+                              "how": "closure_rowpanel: all-gather of the row blocks, simd2_closure_panel_step, "
+                                     "all-reduce(MAX) of the change flag per squaring; CUDA events, median "
+                                     "of steps, max over ranks"}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
         return 0
 
     if args.workload == "batched":

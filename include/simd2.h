@@ -226,6 +226,18 @@ int simd2_compare_update(float* prev, float* cur, int M, int N, simd2_conv mode,
                          cudaStream_t stream);
 int simd2_compare_update_i32(int32_t* prev, int32_t* cur, int M, int N, int* changed_out, cudaStream_t stream);
 
+/* One repeated-squaring step for the rows one rank owns when an n x n
+ * closure is split into row panels across GPUs (the multi-GPU form of the
+ * loop in apps/apsp/cuASR/apsp_cuASR.cu:37-54):
+ *   out = panel (+) panel (x) full
+ * panel: this rank's `rows` rows of X (pitch ldp); full: all n rows of X
+ * (pitch ldf, e.g. gathered from the ranks); out: rows x n (pitch ldo, not
+ * aliasing panel).  ORs 1 into the device int *changed when any element of
+ * out differs from panel (conv as in simd2_closure).  float* for the float
+ * semirings, uint8_t* 0/1 for SIMD2_OR_AND.  Asynchronous on stream. */
+int simd2_closure_panel_step(simd2_op op, int rows, int n, const void* panel, int ldp, const void* full, int ldf,
+                             void* out, int ldo, simd2_conv conv, int* changed, cudaStream_t stream);
+
 /* Reserve the per-(device, stream) workspace for srgemm calls up to
  * M x N x K so that later calls (e.g. inside stream capture) allocate
  * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */

@@ -56,6 +56,7 @@ def lib() -> ctypes.CDLL:
         L.simd2_srgemm_orand_u8.argtypes = [I, I, I, P, I, P, I, P, I, P, I, I, P]
         L.simd2_closure.argtypes = [I, I, P, I, I, I, ctypes.POINTER(I), P]
         L.simd2_closure_orand_u8.argtypes = [I, P, I, I, ctypes.POINTER(I), P]
+        L.simd2_closure_panel_step.argtypes = [I, I, I, P, I, P, I, P, I, I, P, P]
         L.simd2_reserve_workspace.argtypes = [I, I, I, I, P, ctypes.POINTER(ctypes.c_size_t)]
         L.simd2_release_workspaces.argtypes = []
         L.simd2_device_status.argtypes = []
@@ -236,6 +237,27 @@ def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", 
         return it.value
     _check(rc, f"closure({op})")
     return it.value
+
+
+def closure_panel_step(op: str, panel: torch.Tensor, full: torch.Tensor, out: torch.Tensor, changed: torch.Tensor,
+                       conv: str = "exact", stream=None) -> None:
+    """out = panel (+) panel (x) full for a row panel of a distributed closure.
+
+    ``panel`` (rows x n) holds this rank's rows of X, ``full`` (>= n rows x n)
+    all rows; ``changed`` is a device int32 tensor of one element that
+    becomes nonzero when ``out`` differs from ``panel``.  Asynchronous."""
+    rows, n = panel.shape
+    if full.shape[1] != n or full.shape[0] < n or out.shape != panel.shape:
+        raise ValueError("panel step: panel rows x n, full >= n x n, out like panel")
+    want = torch.uint8 if op == "or_and" else torch.float32
+    if panel.dtype != want or full.dtype != want or out.dtype != want:
+        raise TypeError(f"{op} panel step takes {want} tensors")
+    if changed.dtype != torch.int32 or changed.numel() < 1 or changed.device != panel.device:
+        raise TypeError("changed must be an int32 tensor on the panel's device")
+    rc = lib().simd2_closure_panel_step(OP_ID[op], rows, n, panel.data_ptr(), _mat(panel, "panel"), full.data_ptr(),
+                                        _mat(full, "full"), out.data_ptr(), _mat(out, "out"), CONV[conv],
+                                        changed.data_ptr(), _stream(stream))
+    _check(rc, f"closure_panel_step({op})")
 
 
 class BatchedClosure:

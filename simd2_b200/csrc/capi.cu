@@ -1127,6 +1127,29 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
   return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
+int simd2_closure_panel_step(simd2_op op, int rows, int n, const void* panel, int ldp, const void* full, int ldf,
+                             void* out, int ldo, simd2_conv conv, int* changed, cudaStream_t stream) {
+  if (rows < 0 || n < 0 || (int)op < 0 || (int)op > 8) return SIMD2_ERR_INVALID_ARG;
+  if (conv < SIMD2_CONV_EXACT || conv > SIMD2_CONV_APLP) return SIMD2_ERR_INVALID_ARG;
+  if (rows == 0 || n == 0) return SIMD2_OK;
+  if (!panel || !full || !out || !changed || ldp < n || ldf < n || ldo < n) return SIMD2_ERR_INVALID_ARG;
+  if (out == panel) return SIMD2_ERR_INVALID_ARG;  // the epilogue compares out with panel
+  int rc = check_device();
+  if (rc) return rc;
+  if (op == SIMD2_OR_AND) {
+    const TcPlan plan = tc_plan_u8(rows, n, n);
+    void* p = nullptr;
+    if ((rc = get_workspace(stream, plan.total, &p))) return rc;
+    const auto* P = static_cast<const uint8_t*>(panel);
+    return srgemm_tc_orand<uint8_t>(rows, n, n, P, ldp, static_cast<const uint8_t*>(full), ldf, P, ldp,
+                                    static_cast<uint8_t*>(out), ldo, 1, changed, static_cast<uint8_t*>(p), plan,
+                                    stream);
+  }
+  const auto* P = static_cast<const float*>(panel);
+  return srgemm_f32_ws(op, rows, n, n, P, ldp, static_cast<const float*>(full), ldf, P, ldp,
+                       static_cast<float*>(out), ldo, 1, changed, conv, nullptr, stream);
+}
+
 int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t stream, size_t* bytes_out) {
   if (M < 0 || N < 0 || K < 0 || (int)op < 0 || (int)op > 8) return SIMD2_ERR_INVALID_ARG;
   const Plan plan = make_plan(M, N, K, true);
