@@ -238,6 +238,19 @@ int simd2_compare_update_i32(int32_t* prev, int32_t* cur, int M, int N, int* cha
 int simd2_closure_panel_step(simd2_op op, int rows, int n, const void* panel, int ldp, const void* full, int ldf,
                              void* out, int ldo, simd2_conv conv, int* changed, cudaStream_t stream);
 
+/* Closure with a predecessor matrix, for path reconstruction (the
+ * Floyd-Warshall baselines' pred output, apps/maxrp/baseline/lib/apsp.cpp:
+ * 11-25 and main.cpp:80-94).  X (n x n, pitch ldx) is closed in place as by
+ * simd2_closure (exact convergence); P (int32, pitch ldp) ends with
+ * P[i][j] = the vertex before j on the best i -> j path found, -1 where there
+ * is none and on the diagonal.  init_pred = 1 fills P from X first (i where
+ * X[i][j] is an edge, i.e. not the add identity, and i != j; else -1);
+ * init_pred = 0 takes the caller's P.  Per step, an element that strictly
+ * improves through the lowest such k takes P[k][j].  Semirings with a min or
+ * max add (min_plus, max_plus, max_min, max_mul, min_mul, min_max). */
+int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ldp, int init_pred, int max_iter,
+                       int* iters_out, cudaStream_t stream);
+
 /* Reserve the per-(device, stream) workspace for srgemm calls up to
  * M x N x K so that later calls (e.g. inside stream capture) allocate
  * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */

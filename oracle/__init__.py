@@ -74,6 +74,8 @@ def lib():
         _lib.oracle_closure_f32.restype = I
         _lib.oracle_closure_u8.argtypes = [I, P, I, I]
         _lib.oracle_closure_u8.restype = I
+        _lib.oracle_closure_pred_f32.argtypes = [I, I, P, P, I, I]
+        _lib.oracle_closure_pred_f32.restype = I
         _lib.oracle_knn.argtypes = [P, I, P, I, I, I, P, P, P, I]
     return _lib
 
@@ -165,6 +167,29 @@ def closure(op: str, X, max_iter=500, tol_mode=0, threads=None):
     Xc = np.array(X, np.float32, copy=True)
     it = lib().oracle_closure_f32(OP_ID[op], Xc.shape[0], _ptr(Xc), max_iter, tol_mode, _threads(threads))
     return Xc, it
+
+
+def closure_pred(op: str, X, P=None, max_iter=500):
+    """Closure with a predecessor matrix: returns (X, P int32, iterations).
+    P=None initialises it from X (i for an edge, -1 otherwise and on the diagonal)."""
+    Xc = np.array(X, np.float32, copy=True)
+    n = Xc.shape[0]
+    Pc = np.zeros((n, n), np.int32) if P is None else np.array(P, np.int32, copy=True)
+    it = lib().oracle_closure_pred_f32(OP_ID[op], n, _ptr(Xc), _ptr(Pc), int(P is None), max_iter)
+    return Xc, Pc, it
+
+
+def path(P, i, j):
+    """Vertices of the recorded path i -> j from a predecessor matrix ([] when none)."""
+    if i == j:
+        return [i]
+    out = [j]
+    while j != i:
+        j = int(P[i][j])
+        if j < 0 or len(out) > len(P):
+            return []
+        out.append(j)
+    return out[::-1]
 
 
 def knn(query, ref, k, threads=None):

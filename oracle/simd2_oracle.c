@@ -18,6 +18,8 @@
  *   - repeated-squaring closure    apps/apsp/cuASR/apsp_cuASR.cu:42-54 with the
  *       change test of kernel/converge.cuh:6-14 (float), :61-69 (int) and
  *       the APLP variant :32-43.
+ *   - closure with predecessors    apps/maxrp/baseline/lib/apsp.cpp:11-25 (pred
+ *       rule), restated for repeated squaring (oracle_closure_pred_f32).
  *   - k-NN selection               apps/pld/baseline/test.cpp:132-182 (knn_c) with
  *       the modified insertion sort of apps/pld/emulation/knncuda.cu:171-221
  *       (ties keep the lower reference index).
@@ -260,6 +262,83 @@ int oracle_closure_f32(int op, int n, float* X, int max_iter, int tol_mode, int 
     }
   }
   free(Xn);
+  return it;
+}
+
+/* Closure with a predecessor matrix (the Floyd-Warshall baselines' pred,
+ * apps/maxrp/baseline/lib/apsp.cpp:11-25, initial values main.cpp:80-94),
+ * by repeated squaring: per step and (i, j), best = addop over k = 0..n-1 of
+ * mulop(X[i][k], X[k][j]) with the host_srgemm accumulation, witness k* = the
+ * k of the last replacement (the lowest k attaining best, as replacements
+ * need a strictly better product); X'[i][j] = addop(best, X[i][j]);
+ * P'[i][j] = P[k*][j] when best is strictly better than X[i][j], else
+ * P[i][j].  init_pred: P[i][j] = i for i != j and X[i][j] not the add
+ * identity, else -1.  Returns the step count (the final unchanged step
+ * included).  Min/max-add semirings only; single-threaded. */
+int oracle_closure_pred_f32(int op, int n, float* X, int32_t* P, int init_pred, int max_iter) {
+  const int is_min = (op == OP_MIN_PLUS || op == OP_MIN_MUL || op == OP_MIN_MAX);
+  const float ident = is_min ? INFINITY : -INFINITY;
+  size_t nn = (size_t)n * n;
+  if (init_pred)
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        uint32_t a, b;
+        memcpy(&a, &X[(size_t)i * n + j], 4);
+        memcpy(&b, &ident, 4);
+        P[(size_t)i * n + j] = (i != j && a != b) ? i : -1;
+      }
+  float* Xn = (float*)malloc(nn * sizeof(float) + 1);
+  int32_t* Pn = (int32_t*)malloc(nn * sizeof(int32_t) + 1);
+  float* best = (float*)malloc((size_t)n * sizeof(float) + 1);
+  int* kb = (int*)malloc((size_t)n * sizeof(int) + 1);
+  int it = 0, changed = 1;
+  while (changed && it < max_iter) {
+    it++;
+    changed = 0;
+    for (int i = 0; i < n; i++) {
+      for (int j = 0; j < n; j++) {
+        best[j] = ident;
+        kb[j] = -1;
+      }
+      for (int k = 0; k < n; k++) {
+        const float av = X[(size_t)i * n + k];
+        const float* b = X + (size_t)k * n;
+        for (int j = 0; j < n; j++) {
+          const float bv = b[j];
+          float p;
+          switch (op) {
+            case OP_MIN_PLUS: case OP_MAX_PLUS: p = av + bv; break;
+            case OP_MAX_MIN: p = (bv < av) ? bv : av; break;
+            case OP_MIN_MAX: p = (av < bv) ? bv : av; break;
+            default: p = av * bv; break; /* max_mul, min_mul */
+          }
+          const int repl = is_min ? (p < best[j]) : (best[j] < p);
+          if (repl) {
+            best[j] = p;
+            kb[j] = k;
+          }
+        }
+      }
+      for (int j = 0; j < n; j++) {
+        const size_t x = (size_t)i * n + j;
+        const float cv = X[x], bv = best[j];
+        const float xn = is_min ? s_min(bv, cv) : s_max(bv, cv);
+        const int improved = is_min ? (bv < cv) : (cv < bv);
+        Xn[x] = xn;
+        Pn[x] = improved ? P[(size_t)kb[j] * n + j] : P[x];
+        uint32_t a, b2;
+        memcpy(&a, &xn, 4);
+        memcpy(&b2, &cv, 4);
+        if (a != b2) changed = 1;
+      }
+    }
+    memcpy(X, Xn, nn * sizeof(float));
+    memcpy(P, Pn, nn * sizeof(int32_t));
+  }
+  free(Xn);
+  free(Pn);
+  free(best);
+  free(kb);
   return it;
 }
 

@@ -57,6 +57,7 @@ def lib() -> ctypes.CDLL:
         L.simd2_closure.argtypes = [I, I, P, I, I, I, ctypes.POINTER(I), P]
         L.simd2_closure_orand_u8.argtypes = [I, P, I, I, ctypes.POINTER(I), P]
         L.simd2_closure_panel_step.argtypes = [I, I, I, P, I, P, I, P, I, I, P, P]
+        L.simd2_closure_pred.argtypes = [I, I, P, I, P, I, I, I, ctypes.POINTER(I), P]
         L.simd2_reserve_workspace.argtypes = [I, I, I, I, P, ctypes.POINTER(ctypes.c_size_t)]
         L.simd2_release_workspaces.argtypes = []
         L.simd2_device_status.argtypes = []
@@ -237,6 +238,43 @@ def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", 
         return it.value
     _check(rc, f"closure({op})")
     return it.value
+
+
+def closure_pred(op: str, X: torch.Tensor, P: torch.Tensor | None = None, max_iter: int = 500, stream=None):
+    """Closure of X in place with a predecessor matrix: returns (steps, P).
+
+    P[i][j] is the vertex before j on the best i -> j path (-1: none, and on
+    the diagonal).  P=None starts from the edges of X (i where X[i][j] is not
+    the add identity); a given int32 P is taken as the starting state and
+    updated in place.  Semirings with a min or max add."""
+    n = X.shape[0]
+    if X.shape != (n, n) or X.dtype != torch.float32:
+        raise ValueError("closure_pred needs a square float32 matrix")
+    init = P is None
+    if init:
+        P = torch.empty((n, n), dtype=torch.int32, device=X.device)
+    elif P.shape != (n, n) or P.dtype != torch.int32:
+        raise ValueError("P must be an n x n int32 tensor")
+    it = ctypes.c_int(0)
+    rc = lib().simd2_closure_pred(OP_ID[op], n, X.data_ptr(), _mat(X, "X"), P.data_ptr(), _mat(P, "P"), int(init),
+                                  max_iter, ctypes.byref(it), _stream(stream))
+    _check(rc, f"closure_pred({op})")
+    return it.value, P
+
+
+def path(P, i: int, j: int):
+    """Vertices of the recorded i -> j path from a predecessor matrix (host
+    array or tensor); [] when there is none."""
+    if i == j:
+        return [i]
+    Ph = P.cpu().numpy() if isinstance(P, torch.Tensor) else P
+    out = [j]
+    while j != i:
+        j = int(Ph[i][j])
+        if j < 0 or len(out) > len(Ph):
+            return []
+        out.append(j)
+    return out[::-1]
 
 
 def closure_panel_step(op: str, panel: torch.Tensor, full: torch.Tensor, out: torch.Tensor, changed: torch.Tensor,

@@ -22,6 +22,7 @@
 #include "mlp.cuh"
 #include "knn.cuh"
 #include "knn_fused.cuh"
+#include "pred.cuh"
 
 namespace simd2 {
 namespace {
@@ -1148,6 +1149,71 @@ int simd2_closure_panel_step(simd2_op op, int rows, int n, const void* panel, in
   const auto* P = static_cast<const float*>(panel);
   return srgemm_f32_ws(op, rows, n, n, P, ldp, static_cast<const float*>(full), ldf, P, ldp,
                        static_cast<float*>(out), ldo, 1, changed, conv, nullptr, stream);
+}
+
+int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ldp, int init_pred, int max_iter,
+                       int* iters_out, cudaStream_t stream) {
+  if (iters_out) *iters_out = 0;
+  if ((int)op < 0 || (int)op > 8) return SIMD2_ERR_INVALID_ARG;
+  if (op == SIMD2_PLUS_MUL || op == SIMD2_MINUS_SQUARE || op == SIMD2_OR_AND) return SIMD2_ERR_UNSUPPORTED;
+  if (n < 0 || max_iter < 0 || (n > 0 && (!X || !P || ldx < n || ldp < n))) return SIMD2_ERR_INVALID_ARG;
+  if (n == 0) return SIMD2_OK;
+  int rc = check_device();
+  if (rc) return rc;
+  if (init_pred) {
+    pred_init_kernel<<<grid_for((long long)n * n), 256, 0, stream>>>(n, X, ldx, P, ldp, add_identity(op));
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+  }
+  if (max_iter == 0) return SIMD2_OK;
+  // Workspace: [X' n x n][P' n x n][change flag]
+  const size_t nn = (size_t)n * n;
+  const size_t x_off = 0, p_off = align_up(nn * 4, kAlign), f_off = p_off + align_up(nn * 4, kAlign);
+  void* w = nullptr;
+  if ((rc = get_workspace(stream, f_off + kAlign, &w))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(w);
+  float* bufx[2] = {X, reinterpret_cast<float*>(ws + x_off)};
+  int32_t* bufp[2] = {P, reinterpret_cast<int32_t*>(ws + p_off)};
+  long long ldx_[2] = {ldx, n}, ldp_[2] = {ldp, n};
+  int* flag = reinterpret_cast<int*>(ws + f_off);
+  const dim3 grid((n + kPredBN - 1) / kPredBN, (n + kPredBM - 1) / kPredBM);
+  int cur = 0, it = 0, changed = 1;
+  while (changed && it < max_iter) {
+    it++;
+    SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), stream));
+    const int nx = cur ^ 1;
+    switch (op) {
+#define SIMD2_PRED_CASE(OPV)                                                                                         \
+  case OPV:                                                                                                           \
+    pred_step_kernel<OPV><<<grid, 256, 0, stream>>>(n, bufx[cur], ldx_[cur], bufp[cur], ldp_[cur], bufx[nx],       \
+                                                    ldx_[nx], bufp[nx], ldp_[nx], flag);                             \
+    break;
+      SIMD2_PRED_CASE(SIMD2_MIN_PLUS)
+      SIMD2_PRED_CASE(SIMD2_MAX_PLUS)
+      SIMD2_PRED_CASE(SIMD2_MAX_MIN)
+      SIMD2_PRED_CASE(SIMD2_MAX_MUL)
+      SIMD2_PRED_CASE(SIMD2_MIN_MUL)
+      SIMD2_PRED_CASE(SIMD2_MIN_MAX)
+#undef SIMD2_PRED_CASE
+      default: return SIMD2_ERR_UNSUPPORTED;
+    }
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    int h = 0;
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+    changed = h != 0;
+    cur = nx;
+  }
+  if (cur != 0) {
+    SIMD2_CUDA_TRY(cudaMemcpy2DAsync(X, (size_t)ldx * 4, bufx[1], (size_t)n * 4, (size_t)n * 4, n,
+                                     cudaMemcpyDeviceToDevice, stream));
+    SIMD2_CUDA_TRY(cudaMemcpy2DAsync(P, (size_t)ldp * 4, bufp[1], (size_t)n * 4, (size_t)n * 4, n,
+                                     cudaMemcpyDeviceToDevice, stream));
+  }
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (iters_out) *iters_out = it;
+  return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
 int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t stream, size_t* bytes_out) {
