@@ -363,33 +363,60 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     } else {
       // Sums: a 32 x 32 chunk is transposed through shared memory (the stage
       // ring is idle now) and written row by row: lane l handles column l, so
-      // every store instruction covers 32 consecutive floats of one row.
+      // every store instruction covers 32 consecutive floats of one row.  The
+      // chunk's C values (one column per lane, 32 independent loads) and the
+      // warp's 32 row norms are fetched before the TMEM read, so their latency
+      // overlaps it instead of being paid row by row.
       uint32_t* tile = reinterpret_cast<uint32_t*>(smem) + warp * (32 * 33);
+      const bool msq = ep.op == SIMD2_MINUS_SQUARE;
+      const float na_lane = (msq && row0 + lane < M) ? ep.norm_a[row0 + lane] : 0.f;
+      const int rows_here = min(32, M - row0);
 #pragma unroll 1
       for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+        const int col = n0 + c0 + lane;
+        const bool col_ok = col < N;
+        float cv[32];
+        if (ep.do_epilogue) {
+          const float* Cc = static_cast<const float*>(ep.C) + col;
+#pragma unroll
+          for (int rr = 0; rr < 32; rr++)
+            cv[rr] = (col_ok && rr < rows_here) ? Cc[(long long)(row0 + rr) * ep.ldc] : 0.f;
+        }
+        const float nb = (msq && col_ok) ? ep.norm_b[col] : 0.f;
         uint32_t r[32];
         tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
 #pragma unroll
         for (int j = 0; j < 32; j++) tile[lane * 33 + j] = r[j];
         __syncwarp();
-        const int col = n0 + c0 + lane;
-        const bool col_ok = col < N;
-        const float nb = (ep.op == SIMD2_MINUS_SQUARE && col_ok) ? ep.norm_b[col] : 0.f;
-#pragma unroll 4
-        for (int rr = 0; rr < 32; rr++) {
-          const int row = row0 + rr;
-          if (row >= M) break;
-          const uint32_t x = tile[rr * 33 + lane];
-          if (!col_ok) continue;
-          float v = __uint_as_float(x);
-          if (ep.op == SIMD2_MINUS_SQUARE) {
-            const float nsum = ep.norm_a[row] + nb;
-            v = __fmaf_rn(-2.0f, v, nsum);
-            if (v < ep.band * nsum)
-              v = exact_minus_square(ep.A32 + (long long)row * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows);
+        if (msq) {
+          // distances in place; rows inside the cancellation band are
+          // recomputed exactly in a separate, rarely taken loop (one copy of
+          // the recompute code)
+          uint32_t band = 0;
+#pragma unroll
+          for (int rr = 0; rr < 32; rr++) {
+            const float nsum = __shfl_sync(0xffffffffu, na_lane, rr) + nb;
+            const float v = __fmaf_rn(-2.0f, __uint_as_float(tile[rr * 33 + lane]), nsum);
+            tile[rr * 33 + lane] = __float_as_uint(v);
+            band |= (v < ep.band * nsum && rr < rows_here && col_ok ? 1u : 0u) << rr;
           }
-          if (ep.do_epilogue) v = __fadd_rn(v, static_cast<const float*>(ep.C)[(long long)row * ep.ldc + col]);
-          static_cast<float*>(ep.D)[(long long)row * ep.ldd + col] = v;
+          while (band) {
+            const int rr = __ffs(band) - 1;
+            band &= band - 1;
+            tile[rr * 33 + lane] = __float_as_uint(exact_minus_square(
+                ep.A32 + (long long)(row0 + rr) * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows));
+          }
+        }
+        if (col_ok) {
+          float* Dc = static_cast<float*>(ep.D) + col;
+#pragma unroll
+          for (int rr = 0; rr < 32; rr++) {
+            if (rr < rows_here) {
+              float v = __uint_as_float(tile[rr * 33 + lane]);
+              if (ep.do_epilogue) v = __fadd_rn(v, cv[rr]);
+              Dc[(long long)(row0 + rr) * ep.ldd] = v;
+            }
+          }
         }
         __syncwarp();
       }
