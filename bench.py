@@ -203,9 +203,9 @@ def run_reference_arm(args):
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
-def traffic_from_profile():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "srgemm_simt_kernel_min_plus_4096.md")
+def traffic_from_profile(name="srgemm_simt_kernel_min_plus_4096.md"):
+    """DRAM bytes per launch of a kernel from its committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
             m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
@@ -634,7 +634,9 @@ def main():
                                 "achieved": tc_equiv / (tc_ms / 1e3) / 1e12 if tc_ms > 0 else None,
                                 "peak": bf16_peak, "unit": "TFLOP/s (BF16-equivalent)",
                                 "frac": (tc_equiv / (tc_ms / 1e3) / 1e12) / bf16_peak if tc_ms > 0 else None,
-                                "peak_source": f"{peak_kind} bf16_tflops (cuBLAS burst)", "timed_launches": tc_n},
+                                "peak_source": f"{peak_kind} bf16_tflops (cuBLAS burst)", "timed_launches": tc_n,
+                                "traffic": traffic_from_profile("tc_gemm_kernel_plus_mul_4096.md"),
+                                "traffic_of": "one plus_mul 4096^3 launch with C (ncu dram read + write)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
