@@ -332,6 +332,37 @@ def extra_measurements(args, dev):
                 "selection inside the BF16 hi/lo distance MMA's epilogue, then a per-query merge" if mode == "fused"
                 else "BF16 hi/lo minus_square blocks of 1 GiB written, then top-k + sqrt")}
     del Q, R
+    # --- very sparse inputs: semiring SpGEMM and the hybrid sparse/dense closure
+    sp = {}
+    xs = datagen.er_graph(16384, 4 / 16384, seed=1)
+    Xs = torch.from_numpy(xs).to(dev)
+    As = s2.csr_from_dense(Xs, "min_plus")
+    s2.spgemm("min_plus", As, As, 16384, C=As)  # warm-up
+    ev0.record()
+    Ds = s2.spgemm("min_plus", As, As, 16384, C=As)
+    ev1.record()
+    torch.cuda.synchronize()
+    sp["spgemm_step_ms"] = ev0.elapsed_time(ev1)
+    sp["nnz_in"], sp["nnz_out"] = int(As[1].numel()), int(Ds[1].numel())
+    s2.srgemm("min_plus", Xs, Xs, Xs, do_epilogue=True)
+    ev0.record()
+    s2.srgemm("min_plus", Xs, Xs, Xs, do_epilogue=True)
+    ev1.record()
+    torch.cuda.synchronize()
+    sp["dense_step_ms"] = ev0.elapsed_time(ev1)
+    t0 = time.perf_counter()
+    _, sp["hybrid_closure_iters"] = s2.closure_sparse("min_plus", As)
+    torch.cuda.synchronize()
+    sp["hybrid_closure_ms"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    sp["dense_closure_iters"] = s2.closure("min_plus", Xs)
+    torch.cuda.synchronize()
+    sp["dense_closure_ms"] = (time.perf_counter() - t0) * 1e3
+    sp["how"] = ("ER n=16384, average degree 4, min_plus: one X (+) X(x)X step as CSR SpGEMM vs the dense srgemm "
+                 "(CUDA events); closure as sparse steps until density 1/32 then the dense gated closure, vs the dense "
+                 "closure throughout (wall clock)")
+    del Xs, As, Ds
+    cfg4["sparse_er16384_deg4"] = sp
     A = torch.randn((8192, 8192), device=dev)
     B = torch.randn((8192, 8192), device=dev)
     s2.srgemm("plus_mul", A, B)

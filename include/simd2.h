@@ -251,6 +251,42 @@ int simd2_closure_panel_step(simd2_op op, int rows, int n, const void* panel, in
 int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ldp, int init_pred, int max_iter,
                        int* iters_out, cudaStream_t stream);
 
+/* Semiring SpGEMM on CSR matrices, for inputs too sparse for the dense
+ * kernels -- the regime that density_verification/sp_gemm_comp.cu measures
+ * with cuSPARSE SpGEMM (plus-times) against dense GEMM.
+ *   D = A (x) B [(+) C],   A: M x K, B: K x N, C and D: M x N
+ * An absent entry is the add identity, which must annihilate the multiply:
+ * SIMD2_MIN_PLUS, SIMD2_MAX_PLUS, SIMD2_MAX_MIN, SIMD2_MIN_MAX and
+ * SIMD2_PLUS_MUL (others: SIMD2_ERR_UNSUPPORTED).  CSR with int32 offsets
+ * (rows + 1, starting at 0) and columns strictly increasing within a row;
+ * float values.  D stores every column reached through stored entries, in
+ * increasing order, with the value host_srgemm (kernel/host_srgemm.h:17-49)
+ * gives the dense matrices: products combined in increasing k from the add
+ * identity, then C -- bit-identical, plus_mul included.  N <= 2^20.
+ *
+ * Two calls, as cuSPARSE's SpGEMM: simd2_spgemm_nnz checks the structures
+ * (SIMD2_ERR_INVALID_ARG for malformed CSR), writes D_rowptr (M + 1 ints)
+ * and returns the entry count in *nnz_out (synchronous); the caller then
+ * allocates D_cols / D_vals of that size and calls simd2_spgemm_compute with
+ * the same A, B, C (asynchronous).  C_rowptr = NULL: no C term. */
+int simd2_spgemm_nnz(simd2_op op, int M, int N, int K, const int* A_rowptr, const int* A_cols, int A_nnz,
+                     const int* B_rowptr, const int* B_cols, int B_nnz, const int* C_rowptr, const int* C_cols,
+                     int C_nnz, int* D_rowptr, long long* nnz_out, cudaStream_t stream);
+int simd2_spgemm_compute(simd2_op op, int M, int N, int K, const int* A_rowptr, const int* A_cols,
+                         const float* A_vals, int A_nnz, const int* B_rowptr, const int* B_cols, const float* B_vals,
+                         int B_nnz, const int* C_rowptr, const int* C_cols, const float* C_vals, int C_nnz,
+                         const int* D_rowptr, int* D_cols, float* D_vals, long long D_nnz, cudaStream_t stream);
+
+/* Closure X <- X (+) X (x) X of an n x n CSR matrix, in place, until
+ * unchanged (the loop of apps/apsp/cuASR/apsp_cuASR.cu:37-54 on sparse
+ * storage; exact convergence).  cols / vals hold `capacity` entries, the
+ * first *nnz_inout of them in use; on return *nnz_inout is the closed
+ * matrix's count.  When a step needs more than `capacity` entries the call
+ * returns SIMD2_ERR_SCRATCH_LIMIT with X as of the previous step and the
+ * needed count in *nnz_inout.  Semirings as simd2_spgemm_nnz. */
+int simd2_closure_sparse(simd2_op op, int n, int* rowptr, int* cols, float* vals, long long capacity,
+                         long long* nnz_inout, int max_iter, int* iters_out, cudaStream_t stream);
+
 /* Reserve the per-(device, stream) workspace for srgemm calls up to
  * M x N x K so that later calls (e.g. inside stream capture) allocate
  * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */

@@ -27,6 +27,7 @@ STATUS = {
     0: "ok", 1: "invalid argument", 2: "unsupported operation", 3: "CUDA runtime error",
     4: "workspace allocation failed", 5: "device-side wait timed out",
     6: "closure did not converge within max_iter", 7: "no sm_100 device",
+    8: "scratch or capacity limit exceeded",
 }
 
 
@@ -58,6 +59,10 @@ def lib() -> ctypes.CDLL:
         L.simd2_closure_orand_u8.argtypes = [I, P, I, I, ctypes.POINTER(I), P]
         L.simd2_closure_panel_step.argtypes = [I, I, I, P, I, P, I, P, I, I, P, P]
         L.simd2_closure_pred.argtypes = [I, I, P, I, P, I, I, I, ctypes.POINTER(I), P]
+        LL = ctypes.c_longlong
+        L.simd2_spgemm_nnz.argtypes = [I, I, I, I, P, P, I, P, P, I, P, P, I, P, ctypes.POINTER(LL), P]
+        L.simd2_spgemm_compute.argtypes = [I, I, I, I, P, P, P, I, P, P, P, I, P, P, P, I, P, P, P, LL, P]
+        L.simd2_closure_sparse.argtypes = [I, I, P, P, P, LL, ctypes.POINTER(LL), I, ctypes.POINTER(I), P]
         L.simd2_reserve_workspace.argtypes = [I, I, I, I, P, ctypes.POINTER(ctypes.c_size_t)]
         L.simd2_release_workspaces.argtypes = []
         L.simd2_device_status.argtypes = []
@@ -275,6 +280,93 @@ def path(P, i: int, j: int):
             return []
         out.append(j)
     return out[::-1]
+
+
+SPARSE_IDENTITY = {"min_plus": float("inf"), "max_plus": float("-inf"), "max_min": float("-inf"),
+                   "min_max": float("inf"), "plus_mul": 0.0}
+
+
+def csr_from_dense(X: torch.Tensor, op: str):
+    """(rowptr, cols, vals) of the entries of X that are not the add identity of ``op``."""
+    mask = X != SPARSE_IDENTITY[op]
+    counts = mask.sum(1, dtype=torch.int32)
+    rowptr = torch.zeros(X.shape[0] + 1, dtype=torch.int32, device=X.device)
+    rowptr[1:] = torch.cumsum(counts, 0, dtype=torch.int32)
+    cols = mask.nonzero()[:, 1].to(torch.int32).contiguous()
+    return rowptr, cols, X[mask].to(torch.float32).contiguous()
+
+
+def csr_to_dense(csr, n_cols: int, op: str) -> torch.Tensor:
+    """Dense matrix with the add identity of ``op`` where ``csr`` stores nothing."""
+    rowptr, cols, vals = csr
+    rows = rowptr.numel() - 1
+    X = torch.full((rows, n_cols), SPARSE_IDENTITY[op], dtype=torch.float32, device=vals.device)
+    r = torch.repeat_interleave(torch.arange(rows, device=vals.device), (rowptr[1:] - rowptr[:-1]).long())
+    X[r, cols.long()] = vals
+    return X
+
+
+def _csr(t, name):
+    rowptr, cols, vals = t
+    for x, dt in ((rowptr, torch.int32), (cols, torch.int32), (vals, torch.float32)):
+        if x.dtype != dt or not x.is_cuda or not x.is_contiguous():
+            raise TypeError(f"{name}: CSR needs contiguous CUDA int32 rowptr / cols and float32 vals")
+    if cols.numel() != vals.numel():
+        raise ValueError(f"{name}: cols and vals differ in length")
+    return rowptr, cols, vals
+
+
+def spgemm(op: str, A, B, n_cols: int, C=None, stream=None):
+    """D = A (x) B [(+) C] on CSR matrices (rowptr, cols, vals); returns D as CSR.
+
+    ``n_cols`` is the column count of B (and C, D).  Absent entries are the add
+    identity (``SPARSE_IDENTITY``); columns come out sorted; values equal the
+    dense srgemm's bit for bit."""
+    ap, aj, av = _csr(A, "A")
+    bp, bj, bv = _csr(B, "B")
+    cp = cj = cv = None
+    if C is not None:
+        cp, cj, cv = _csr(C, "C")
+    M, K = ap.numel() - 1, bp.numel() - 1
+    dp = torch.empty(M + 1, dtype=torch.int32, device=av.device)
+    nnz = ctypes.c_longlong(0)
+    s = _stream(stream)
+    ptr = lambda t: t.data_ptr() if t is not None else None
+    rc = lib().simd2_spgemm_nnz(OP_ID[op], M, n_cols, K, ap.data_ptr(), aj.data_ptr(), aj.numel(), bp.data_ptr(),
+                                bj.data_ptr(), bj.numel(), ptr(cp), ptr(cj), cj.numel() if cj is not None else 0,
+                                dp.data_ptr(), ctypes.byref(nnz), s)
+    _check(rc, f"spgemm_nnz({op})")
+    dj = torch.empty(nnz.value, dtype=torch.int32, device=av.device)
+    dv = torch.empty(nnz.value, dtype=torch.float32, device=av.device)
+    rc = lib().simd2_spgemm_compute(OP_ID[op], M, n_cols, K, ap.data_ptr(), aj.data_ptr(), av.data_ptr(), aj.numel(),
+                                    bp.data_ptr(), bj.data_ptr(), bv.data_ptr(), bj.numel(), ptr(cp), ptr(cj), ptr(cv),
+                                    cj.numel() if cj is not None else 0, dp.data_ptr(), ptr(dj), ptr(dv), nnz.value, s)
+    _check(rc, f"spgemm_compute({op})")
+    return dp, dj, dv
+
+
+def closure_sparse(op: str, X, capacity: int | None = None, max_iter: int = 500, stream=None):
+    """Closure of a square CSR matrix (rowptr, cols, vals): returns (closed CSR, steps).
+
+    ``capacity`` bounds the stored entries (default n * n); the arrays are
+    copied into buffers of that size, closed in place and trimmed."""
+    rowptr, cols, vals = _csr(X, "X")
+    n = rowptr.numel() - 1
+    cap = n * n if capacity is None else int(capacity)
+    nnz0 = cols.numel()
+    if cap < nnz0:
+        raise ValueError("capacity below the matrix's entry count")
+    rp = rowptr.clone()
+    cj = torch.empty(max(cap, 1), dtype=torch.int32, device=vals.device)
+    cv = torch.empty(max(cap, 1), dtype=torch.float32, device=vals.device)
+    cj[:nnz0] = cols
+    cv[:nnz0] = vals
+    nnz = ctypes.c_longlong(nnz0)
+    it = ctypes.c_int(0)
+    rc = lib().simd2_closure_sparse(OP_ID[op], n, rp.data_ptr(), cj.data_ptr(), cv.data_ptr(), cap,
+                                    ctypes.byref(nnz), max_iter, ctypes.byref(it), _stream(stream))
+    _check(rc, f"closure_sparse({op}) [entries {nnz.value}]")
+    return (rp, cj[: nnz.value].clone(), cv[: nnz.value].clone()), it.value
 
 
 def closure_panel_step(op: str, panel: torch.Tensor, full: torch.Tensor, out: torch.Tensor, changed: torch.Tensor,

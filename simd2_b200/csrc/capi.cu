@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <atomic>
 #include <type_traits>
@@ -23,6 +24,7 @@
 #include "knn.cuh"
 #include "knn_fused.cuh"
 #include "pred.cuh"
+#include "spgemm.cuh"
 
 namespace simd2 {
 namespace {
@@ -100,13 +102,16 @@ std::pair<cudaEvent_t, cudaEvent_t>* prof_slot(long long ops, int kind = kProfSi
 // workspace: one growable device buffer per (device, stream)
 // ---------------------------------------------------------------------------
 std::mutex g_ws_mu;
-std::map<std::pair<int, cudaStream_t>, std::pair<void*, size_t>> g_ws;
+// (device, stream, slot) -> growable buffer.  Slot 0 is the workspace of
+// every entry point; slot 1 holds the dense matrix of the sparse closure's
+// dense phase while that phase's own calls use slot 0.
+std::map<std::tuple<int, cudaStream_t, int>, std::pair<void*, size_t>> g_ws;
 
-int get_workspace(cudaStream_t stream, size_t bytes, void** out) {
+int get_workspace_slot(cudaStream_t stream, int slot, size_t bytes, void** out) {
   int dev = 0;
   SIMD2_CUDA_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(g_ws_mu);
-  auto& e = g_ws[{dev, stream}];
+  auto& e = g_ws[{dev, stream, slot}];
   if (e.second < bytes) {
     if (e.first) {
       cudaStreamSynchronize(stream);
@@ -124,6 +129,8 @@ int get_workspace(cudaStream_t stream, size_t bytes, void** out) {
   *out = e.first;
   return SIMD2_OK;
 }
+
+int get_workspace(cudaStream_t stream, size_t bytes, void** out) { return get_workspace_slot(stream, 0, bytes, out); }
 
 // ---------------------------------------------------------------------------
 // TMA descriptors
@@ -1216,6 +1223,303 @@ int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ld
   return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
+}  // extern "C"
+
+namespace simd2 {
+namespace {
+
+bool spgemm_op(int op) {
+  return op == SIMD2_MIN_PLUS || op == SIMD2_MAX_PLUS || op == SIMD2_MAX_MIN || op == SIMD2_MIN_MAX ||
+         op == SIMD2_PLUS_MUL;
+}
+
+struct SpPlan {
+  int grid;            // persistent CTAs
+  size_t smem;         // bitmap bytes
+  size_t acc_off, cnt_off, ctr_off, flag_off, tot_off, total;
+};
+
+SpPlan sp_plan(int M, int N, size_t base) {
+  SpPlan p{};
+  const size_t bitmap = (size_t)((N + 31) / 32) * 4;
+  p.smem = bitmap;
+  int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / std::max<size_t>(bitmap, 1)));
+  long long g = std::min<long long>((long long)M, 148LL * per_sm);
+  // the accumulator slices stay below 1 GiB
+  g = std::min<long long>(g, std::max<long long>(1, (1LL << 30) / (4LL * std::max(N, 1))));
+  p.grid = (int)std::max<long long>(1, g);
+  size_t off = base;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
+  p.acc_off = take((size_t)p.grid * N * 4);
+  p.cnt_off = take((size_t)std::max(M, 1) * 4);
+  p.ctr_off = take(16);
+  p.flag_off = take(16);
+  p.tot_off = take(16);
+  p.total = off;
+  return p;
+}
+
+template <bool COUNT>
+int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t stream) {
+  auto pick = [&](auto kern) -> int {
+    if (plan.smem > (48u << 10))
+      SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
+    kern<<<plan.grid, kSpThreads, plan.smem, stream>>>(args);
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    return SIMD2_OK;
+  };
+  switch (op) {
+    case SIMD2_MIN_PLUS: return pick(spgemm_rows_kernel<SIMD2_MIN_PLUS, COUNT>);
+    case SIMD2_MAX_PLUS: return pick(spgemm_rows_kernel<SIMD2_MAX_PLUS, COUNT>);
+    case SIMD2_MAX_MIN: return pick(spgemm_rows_kernel<SIMD2_MAX_MIN, COUNT>);
+    case SIMD2_MIN_MAX: return pick(spgemm_rows_kernel<SIMD2_MIN_MAX, COUNT>);
+    case SIMD2_PLUS_MUL: return pick(spgemm_rows_kernel<SIMD2_PLUS_MUL, COUNT>);
+    default: return SIMD2_ERR_UNSUPPORTED;
+  }
+}
+
+int sp_check_args(int op, int M, int N, int K, const int* ap, const int* aj, int a_nnz, const int* bp,
+                  const int* bj, int b_nnz, const int* cp, const int* cj, int c_nnz) {
+  if ((int)op < 0 || op > 8) return SIMD2_ERR_INVALID_ARG;
+  if (!spgemm_op(op)) return SIMD2_ERR_UNSUPPORTED;
+  if (M < 0 || N < 0 || K < 0 || N > (1 << 20) || a_nnz < 0 || b_nnz < 0 || c_nnz < 0) return SIMD2_ERR_INVALID_ARG;
+  if (!ap || !bp || (a_nnz > 0 && !aj) || (b_nnz > 0 && !bj)) return SIMD2_ERR_INVALID_ARG;
+  if (cp && c_nnz > 0 && !cj) return SIMD2_ERR_INVALID_ARG;
+  return SIMD2_OK;
+}
+
+constexpr int kSpOverflow = -1;  // internal: the result needs more than 2^31 - 1 entries
+
+// Validates the structures, counts the result's row nonzeros, forms D's
+// offsets.  On kSpOverflow, *nnz_out still holds the exact count.
+int spgemm_count(int op, int M, int N, int K, const int* ap, const int* aj, int a_nnz, const int* bp, const int* bj,
+                 int b_nnz, const int* cp, const int* cj, int c_nnz, int* dp, long long* nnz_out, uint8_t* ws,
+                 const SpPlan& plan, cudaStream_t stream) {
+  int* flag = reinterpret_cast<int*>(ws + plan.flag_off);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, 8, stream));
+  csr_check_kernel<<<grid_for(M), 256, 0, stream>>>(M, K, ap, aj, a_nnz, flag);
+  csr_check_kernel<<<grid_for(K), 256, 0, stream>>>(K, N, bp, bj, b_nnz, flag);
+  count_launch();
+  count_launch();
+  if (cp) {
+    csr_check_kernel<<<grid_for(M), 256, 0, stream>>>(M, N, cp, cj, c_nnz, flag);
+    count_launch();
+  }
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  int bad = 0;
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(&bad, flag, 4, cudaMemcpyDeviceToHost, stream));
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (bad) return SIMD2_ERR_INVALID_ARG;
+  SpArgs a{};
+  a.M = M, a.N = N, a.K = K, a.a_nnz = a_nnz, a.b_nnz = b_nnz, a.c_nnz = c_nnz;
+  a.ap = ap, a.aj = aj, a.bp = bp, a.bj = bj, a.cp = cp, a.cj = cj;
+  a.row_nnz = reinterpret_cast<int*>(ws + plan.cnt_off);
+  a.acc = reinterpret_cast<float*>(ws + plan.acc_off);
+  a.next_row = reinterpret_cast<int*>(ws + plan.ctr_off);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(a.next_row, 0, 4, stream));
+  int rc = spgemm_launch<true>(op, a, plan, stream);
+  if (rc) return rc;
+  long long* tot = reinterpret_cast<long long*>(ws + plan.tot_off);
+  offsets_scan_kernel<<<1, 1024, 0, stream>>>(a.row_nnz, M, dp, flag + 1, tot);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  int over = 0;
+  long long total = 0;
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(&total, tot, 8, cudaMemcpyDeviceToHost, stream));
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(&over, flag + 1, 4, cudaMemcpyDeviceToHost, stream));
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  *nnz_out = total;
+  return over ? kSpOverflow : SIMD2_OK;
+}
+
+int spgemm_fill(int op, int M, int N, int K, const int* ap, const int* aj, const float* av, int a_nnz, const int* bp,
+                const int* bj, const float* bv, int b_nnz, const int* cp, const int* cj, const float* cv, int c_nnz,
+                const int* dp, int* dj, float* dv, long long d_cap, uint8_t* ws, const SpPlan& plan,
+                cudaStream_t stream) {
+  SpArgs a{};
+  a.M = M, a.N = N, a.K = K, a.a_nnz = a_nnz, a.b_nnz = b_nnz, a.c_nnz = c_nnz, a.d_cap = d_cap;
+  a.ap = ap, a.aj = aj, a.av = av, a.bp = bp, a.bj = bj, a.bv = bv, a.cp = cp, a.cj = cj, a.cv = cv;
+  a.dp = dp, a.dj = dj, a.dv = dv;
+  a.acc = reinterpret_cast<float*>(ws + plan.acc_off);
+  a.next_row = reinterpret_cast<int*>(ws + plan.ctr_off);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(a.next_row, 0, 4, stream));
+  return spgemm_launch<false>(op, a, plan, stream);
+}
+
+}  // namespace
+}  // namespace simd2
+
+extern "C" {
+
+int simd2_spgemm_nnz(simd2_op op, int M, int N, int K, const int* A_rowptr, const int* A_cols, int A_nnz,
+                     const int* B_rowptr, const int* B_cols, int B_nnz, const int* C_rowptr, const int* C_cols,
+                     int C_nnz, int* D_rowptr, long long* nnz_out, cudaStream_t stream) {
+  using namespace simd2;
+  if (!nnz_out || !D_rowptr) return SIMD2_ERR_INVALID_ARG;
+  *nnz_out = 0;
+  int rc = sp_check_args(op, M, N, K, A_rowptr, A_cols, A_nnz, B_rowptr, B_cols, B_nnz, C_rowptr, C_cols, C_nnz);
+  if (rc) return rc;
+  if ((rc = check_device())) return rc;
+  const SpPlan plan = sp_plan(M, N, 0);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, plan.total, &p))) return rc;
+  if (M == 0) {
+    SIMD2_CUDA_TRY(cudaMemsetAsync(D_rowptr, 0, 4, stream));
+    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+    return SIMD2_OK;
+  }
+  rc = spgemm_count(op, M, N, K, A_rowptr, A_cols, A_nnz, B_rowptr, B_cols, B_nnz, C_rowptr, C_cols, C_nnz,
+                    D_rowptr, nnz_out, static_cast<uint8_t*>(p), plan, stream);
+  return rc == kSpOverflow ? SIMD2_ERR_SCRATCH_LIMIT : rc;  // int32 offsets cannot hold the result
+}
+
+int simd2_spgemm_compute(simd2_op op, int M, int N, int K, const int* A_rowptr, const int* A_cols,
+                         const float* A_vals, int A_nnz, const int* B_rowptr, const int* B_cols, const float* B_vals,
+                         int B_nnz, const int* C_rowptr, const int* C_cols, const float* C_vals, int C_nnz,
+                         const int* D_rowptr, int* D_cols, float* D_vals, long long D_nnz, cudaStream_t stream) {
+  using namespace simd2;
+  int rc = sp_check_args(op, M, N, K, A_rowptr, A_cols, A_nnz, B_rowptr, B_cols, B_nnz, C_rowptr, C_cols, C_nnz);
+  if (rc) return rc;
+  if ((A_nnz > 0 && !A_vals) || (B_nnz > 0 && !B_vals) || (C_rowptr && C_nnz > 0 && !C_vals) || !D_rowptr ||
+      D_nnz < 0 || (D_nnz > 0 && (!D_cols || !D_vals)))
+    return SIMD2_ERR_INVALID_ARG;
+  if (M == 0 || D_nnz == 0) return SIMD2_OK;
+  if ((rc = check_device())) return rc;
+  const SpPlan plan = sp_plan(M, N, 0);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, plan.total, &p))) return rc;
+  return spgemm_fill(op, M, N, K, A_rowptr, A_cols, A_vals, A_nnz, B_rowptr, B_cols, B_vals, B_nnz, C_rowptr, C_cols,
+                     C_vals, C_nnz, D_rowptr, D_cols, D_vals, D_nnz, static_cast<uint8_t*>(p), plan, stream);
+}
+
+int simd2_closure_sparse(simd2_op op, int n, int* rowptr, int* cols, float* vals, long long capacity,
+                         long long* nnz_inout, int max_iter, int* iters_out, cudaStream_t stream) {
+  using namespace simd2;
+  if (iters_out) *iters_out = 0;
+  if (!nnz_inout || n < 0 || max_iter < 0 || capacity < 0 || *nnz_inout < 0 || *nnz_inout > capacity ||
+      capacity > 0x7fffffffLL)
+    return SIMD2_ERR_INVALID_ARG;
+  int rc = sp_check_args(op, n, n, n, rowptr, cols, (int)*nnz_inout, rowptr, cols, (int)*nnz_inout, rowptr, cols,
+                         (int)*nnz_inout);
+  if (rc) return rc;
+  if (op == SIMD2_PLUS_MUL) return SIMD2_ERR_UNSUPPORTED;  // a closure needs an idempotent add
+  if (n == 0 || max_iter == 0) return SIMD2_OK;
+  if ((*nnz_inout > 0 && !vals) || (capacity > 0 && (!cols || !vals))) return SIMD2_ERR_INVALID_ARG;
+  if ((rc = check_device())) return rc;
+  // Workspace: [spgemm plan][D offsets n+1][D columns capacity][D values capacity]
+  const SpPlan plan0 = sp_plan(n, n, 0);
+  const size_t dp_off = plan0.total;
+  const size_t dj_off = dp_off + align_up((size_t)(n + 1) * 4, kAlign);
+  const size_t dv_off = dj_off + align_up((size_t)capacity * 4 + 4, kAlign);
+  const size_t total = dv_off + align_up((size_t)capacity * 4 + 4, kAlign);
+  void* p = nullptr;
+  if ((rc = get_workspace(stream, total, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  int* dp = reinterpret_cast<int*>(ws + dp_off);
+  int* dj = reinterpret_cast<int*>(ws + dj_off);
+  float* dv = reinterpret_cast<float*>(ws + dv_off);
+  int* flag = reinterpret_cast<int*>(ws + plan0.flag_off);
+  const float ident = add_identity(op);
+  long long nnz = *nnz_inout;
+  int it = 0;
+  bool changed = true, dense = false;
+  while (changed && it < max_iter) {
+    // Closures fill in: once X is denser than 1/32 (or a step would pass the
+    // int32 offsets), the dense gated closure takes over from X.
+    if (nnz * 32 > (long long)n * n) {
+      dense = true;
+      break;
+    }
+    long long nn = 0;
+    rc = spgemm_count(op, n, n, n, rowptr, cols, (int)nnz, rowptr, cols, (int)nnz, rowptr, cols, (int)nnz, dp, &nn,
+                      ws, plan0, stream);
+    if (rc == kSpOverflow || (rc == SIMD2_OK && nn * 32 > (long long)n * n && nn > capacity)) {
+      dense = true;
+      break;
+    }
+    if (rc) return rc;
+    if (nn > capacity) {
+      *nnz_inout = nn;  // what the next step needs
+      if (iters_out) *iters_out = it;
+      return SIMD2_ERR_SCRATCH_LIMIT;
+    }
+    it++;
+    rc = spgemm_fill(op, n, n, n, rowptr, cols, vals, (int)nnz, rowptr, cols, vals, (int)nnz, rowptr, cols, vals,
+                     (int)nnz, dp, dj, dv, nn, ws, plan0, stream);
+    if (rc) return rc;
+    // X' holds X's structure plus any new entries: equal counts mean equal
+    // structure, and then the values decide
+    if (nn != nnz) {
+      changed = true;
+    } else {
+      SIMD2_CUDA_TRY(cudaMemsetAsync(flag + 2, 0, 4, stream));
+      values_differ_kernel<<<grid_for(nn), 256, 0, stream>>>(vals, dv, nn, flag + 2);
+      count_launch();
+      SIMD2_CUDA_TRY(cudaGetLastError());
+      int h = 0;
+      SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag + 2, 4, cudaMemcpyDeviceToHost, stream));
+      SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+      changed = h != 0;
+    }
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(rowptr, dp, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, stream));
+    if (nn > 0) {
+      SIMD2_CUDA_TRY(cudaMemcpyAsync(cols, dj, (size_t)nn * 4, cudaMemcpyDeviceToDevice, stream));
+      SIMD2_CUDA_TRY(cudaMemcpyAsync(vals, dv, (size_t)nn * 4, cudaMemcpyDeviceToDevice, stream));
+    }
+    nnz = nn;
+  }
+  if (dense) {
+    // dense phase: X into an n x n matrix (second workspace slot), the gated
+    // dense closure for the remaining steps, then back to CSR
+    void* q = nullptr;
+    if ((rc = get_workspace_slot(stream, 1, (size_t)n * n * 4 + 64, &q))) return rc;
+    float* Xd = static_cast<float*>(q);
+    fill_kernel<float><<<grid_for((long long)n * n), 256, 0, stream>>>(Xd, n, n, n, ident);
+    csr_scatter_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, rowptr, cols, vals, Xd, n);
+    count_launch();
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    int it2 = 0;
+    const int rc2 = closure_f32(op, n, Xd, n, max_iter - it, SIMD2_CONV_EXACT, &it2, stream);
+    if (rc2 && rc2 != SIMD2_ERR_NOT_CONVERGED) return rc2;
+    it += it2;
+    changed = rc2 == SIMD2_ERR_NOT_CONVERGED;
+    // the closure's workspace (slot 0) may have moved: take it again
+    if ((rc = get_workspace(stream, total, &p))) return rc;
+    ws = static_cast<uint8_t*>(p);
+    int* counts = reinterpret_cast<int*>(ws + plan0.cnt_off);
+    flag = reinterpret_cast<int*>(ws + plan0.flag_off);
+    long long* tot = reinterpret_cast<long long*>(ws + plan0.tot_off);
+    SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, 8, stream));
+    dense_row_count_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, n, Xd, n, ident, counts);
+    // offsets go to the workspace first: the caller's rowptr still describes
+    // X if the result does not fit
+    int* dp2 = reinterpret_cast<int*>(ws + dp_off);
+    offsets_scan_kernel<<<1, 1024, 0, stream>>>(counts, n, dp2, flag + 1, tot);
+    count_launch();
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    long long nn = 0;
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(&nn, tot, 8, cudaMemcpyDeviceToHost, stream));
+    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (nn > capacity) {
+      *nnz_inout = nn;
+      if (iters_out) *iters_out = it;
+      return SIMD2_ERR_SCRATCH_LIMIT;
+    }
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(rowptr, dp2, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, stream));
+    dense_to_csr_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, n, Xd, n, ident, dp2, cols, vals);
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    nnz = nn;
+  }
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  *nnz_inout = nnz;
+  if (iters_out) *iters_out = it;
+  return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
+}
+
 int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t stream, size_t* bytes_out) {
   if (M < 0 || N < 0 || K < 0 || (int)op < 0 || (int)op > 8) return SIMD2_ERR_INVALID_ARG;
   const Plan plan = make_plan(M, N, K, true);
@@ -1232,7 +1536,7 @@ int simd2_release_workspaces(void) {
   std::lock_guard<std::mutex> lk(g_ws_mu);
   cudaDeviceSynchronize();
   for (auto it = g_ws.begin(); it != g_ws.end();) {
-    if (it->first.first == dev) {
+    if (std::get<0>(it->first) == dev) {
       cudaFree(it->second.first);
       it = g_ws.erase(it);
     } else {

@@ -1,0 +1,305 @@
+// spgemm.cuh -- semiring SpGEMM on CSR matrices, for inputs too sparse for
+// the dense kernels (the regime of density_verification/sp_gemm_comp.cu,
+// which times cuSPARSE SpGEMM against dense GEMM as the density falls).
+//
+// D = A (x) B [(+) C] where an absent entry is the semiring's add identity.
+// That is exact only where the add identity annihilates the multiply on the
+// stored values: min_plus (+inf), max_plus (-inf), max_min (-inf), min_max
+// (+inf), plus_mul (0).  The result stores every column reached through a
+// stored A[i][k] and B[k][j] (or stored in C), in increasing column order.
+//
+// Row-wise (Gustavson) accumulation.  Persistent CTAs take rows from an
+// atomic counter; a CTA keeps, for its current row, a bitmap of touched
+// columns in shared memory and the running values in its own slice of a
+// global scratch array (N floats per CTA, L2-resident for the sizes used).
+// The row's A entries are visited in increasing k; for each k the threads
+// spread over B's row k (distinct columns, so no two threads meet on one
+// column) and a barrier separates consecutive k.  Every output therefore
+// receives its products in increasing k -- the host_srgemm order
+// (kernel/host_srgemm.h:17-49) -- starting from the add identity, then the C
+// term: bit-identical to the dense contract, plus_mul included.  The bitmap is
+// scanned in word order to write the row's columns sorted.
+//
+// Two passes share the kernel: COUNT writes the row's nonzero count (no
+// values, no barriers per k), FILL writes columns and values at the offsets
+// the host formed from the counts.
+#pragma once
+#include "common.cuh"
+
+namespace simd2 {
+
+constexpr int kSpThreads = 128;
+
+template <int OP>
+struct SpOps;
+template <>
+struct SpOps<SIMD2_MIN_PLUS> {
+  __device__ static float ident() { return __int_as_float(0x7f800000); }
+  __device__ static float mul(float a, float b) { return __fadd_rn(a, b); }
+  __device__ static float add(float d, float p) { return (p < d) ? p : d; }
+};
+template <>
+struct SpOps<SIMD2_MAX_PLUS> {
+  __device__ static float ident() { return __int_as_float(0xff800000); }
+  __device__ static float mul(float a, float b) { return __fadd_rn(a, b); }
+  __device__ static float add(float d, float p) { return (d < p) ? p : d; }
+};
+template <>
+struct SpOps<SIMD2_MAX_MIN> {
+  __device__ static float ident() { return __int_as_float(0xff800000); }
+  __device__ static float mul(float a, float b) { return (b < a) ? b : a; }
+  __device__ static float add(float d, float p) { return (d < p) ? p : d; }
+};
+template <>
+struct SpOps<SIMD2_MIN_MAX> {
+  __device__ static float ident() { return __int_as_float(0x7f800000); }
+  __device__ static float mul(float a, float b) { return (a < b) ? b : a; }
+  __device__ static float add(float d, float p) { return (p < d) ? p : d; }
+};
+template <>
+struct SpOps<SIMD2_PLUS_MUL> {
+  __device__ static float ident() { return 0.f; }
+  __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+  __device__ static float add(float d, float p) { return __fadd_rn(d, p); }
+};
+
+struct SpArgs {
+  int M, N, K;
+  int a_nnz, b_nnz, c_nnz;  // entries in the column / value arrays (reads are clamped to them)
+  long long d_cap;          // FILL: entries in dj / dv (writes are clamped to them)
+  const int* ap;  // A: M + 1 offsets, columns (the k of B's rows), values
+  const int* aj;
+  const float* av;
+  const int* bp;  // B: K + 1 offsets, columns < N, values
+  const int* bj;
+  const float* bv;
+  const int* cp;  // optional C (epilogue), M + 1 offsets; null when absent
+  const int* cj;
+  const float* cv;
+  const int* dp;  // FILL: output offsets (M + 1)
+  int* dj;        // FILL: output columns
+  float* dv;      // FILL: output values
+  int* row_nnz;   // COUNT: per-row nonzero count
+  float* acc;     // gridDim.x * N floats of scratch (FILL)
+  int* next_row;  // atomic row counter, zero before the launch
+};
+
+// Exclusive prefix sum of x over the block (kSpThreads threads); total in *total.
+__device__ __forceinline__ int block_exclusive_scan(int x, int* s_warp, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int v = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) s_warp[warp] = v;
+  __syncthreads();
+  int base = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kSpThreads / 32; w++) {
+    const int t = s_warp[w];
+    if (w < warp) base += t;
+    tot += t;
+  }
+  __syncthreads();
+  *total = tot;
+  return base + v - x;
+}
+
+template <int OP, bool COUNT>
+__global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
+  using O = SpOps<OP>;
+  extern __shared__ uint32_t bitmap[];  // ceil(N / 32) words
+  __shared__ int s_row;
+  __shared__ int s_warp[kSpThreads / 32];
+  const int words = (a.N + 31) >> 5;
+  float* acc = a.acc + (size_t)blockIdx.x * a.N;
+  const float ident = O::ident();
+  while (true) {
+    if (threadIdx.x == 0) s_row = atomicAdd(a.next_row, 1);
+    for (int w = threadIdx.x; w < words; w += kSpThreads) bitmap[w] = 0u;
+    __syncthreads();
+    const int r = s_row;
+    if (r >= a.M) break;
+    // Offsets and indices are validated by the host pass before any launch;
+    // the clamps keep every access inside the arrays whatever they hold.
+    const int e1 = min(a.ap[r + 1], a.a_nnz);
+    for (int e = max(a.ap[r], 0); e < e1; e++) {
+      const int k = a.aj[e];
+      if ((unsigned)k >= (unsigned)a.K) continue;  // uniform across the block
+      const float av = COUNT ? 0.f : a.av[e];
+      const int f1 = min(a.bp[k + 1], a.b_nnz);
+      for (int f = max(a.bp[k], 0) + threadIdx.x; f < f1; f += kSpThreads) {
+        const int j = a.bj[f];
+        if ((unsigned)j >= (unsigned)a.N) continue;
+        const uint32_t bit = 1u << (j & 31);
+        const uint32_t old = atomicOr(&bitmap[j >> 5], bit);
+        if constexpr (!COUNT) acc[j] = O::add((old & bit) ? acc[j] : ident, O::mul(av, a.bv[f]));
+      }
+      if constexpr (!COUNT) __syncthreads();  // the next k sees this k's values, in order
+    }
+    if (a.cp) {
+      // epilogue: D = D (+) C over C's stored entries (the host_srgemm order)
+      const int g1 = min(a.cp[r + 1], a.c_nnz);
+      for (int f = max(a.cp[r], 0) + threadIdx.x; f < g1; f += kSpThreads) {
+        const int j = a.cj[f];
+        if ((unsigned)j >= (unsigned)a.N) continue;
+        const uint32_t bit = 1u << (j & 31);
+        const uint32_t old = atomicOr(&bitmap[j >> 5], bit);
+        if constexpr (!COUNT) acc[j] = O::add((old & bit) ? acc[j] : ident, a.cv[f]);
+      }
+    }
+    __syncthreads();
+    if constexpr (COUNT) {
+      int cnt = 0;
+      for (int w = threadIdx.x; w < words; w += kSpThreads) cnt += __popc(bitmap[w]);
+      int total;
+      block_exclusive_scan(cnt, s_warp, &total);
+      if (threadIdx.x == 0) a.row_nnz[r] = total;
+    } else {
+      // columns in increasing order: word w's set bits land after all set bits of words < w
+      long long out = a.dp[r];
+      const long long out_end = min((long long)a.dp[r + 1], a.d_cap);
+      for (int w0 = 0; w0 < words; w0 += kSpThreads) {
+        const int w = w0 + threadIdx.x;
+        uint32_t bits = w < words ? bitmap[w] : 0u;
+        int total;
+        long long pos = out + block_exclusive_scan(__popc(bits), s_warp, &total);
+        while (bits) {
+          const int b = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const int j = (w << 5) + b;
+          if (pos >= 0 && pos < out_end) {
+            a.dj[pos] = j;
+            a.dv[pos] = acc[j];
+          }
+          pos++;
+        }
+        out += total;
+      }
+    }
+    __syncthreads();  // bitmap and s_row are reused for the next row
+  }
+}
+
+// CSR structure check: rowptr[0] == 0, rowptr[rows] == nnz, offsets
+// nondecreasing, columns in [0, ncols) and strictly increasing within a row.
+// Sets *bad on any violation.
+__global__ void csr_check_kernel(int rows, int ncols, const int* __restrict__ rp, const int* __restrict__ cj, int nnz,
+                                 int* __restrict__ bad) {
+  int b = 0;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (tid == 0 && (rp[0] != 0 || rp[rows] != nnz)) b = 1;
+  for (long long r = tid; r < rows; r += stride) {
+    const int s0 = rp[r], s1 = rp[r + 1];
+    if (s1 < s0 || s0 < 0 || s1 > nnz) {
+      b = 1;
+      continue;
+    }
+    int prev = -1;
+    for (int e = s0; e < s1; e++) {
+      const int j = cj[e];
+      if (j <= prev || j >= ncols) b = 1;
+      prev = j;
+    }
+  }
+  if (b) atomicOr(bad, 1);
+}
+
+// Exclusive prefix sum of counts[0..n) into out[0..n], one block; *total
+// receives the exact sum, *overflow is set when it exceeds INT32 range.
+__global__ void __launch_bounds__(1024) offsets_scan_kernel(const int* __restrict__ counts, int n,
+                                                            int* __restrict__ out, int* __restrict__ overflow,
+                                                            long long* __restrict__ total) {
+  __shared__ long long s_part[32];
+  __shared__ long long s_base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_base = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < n; c0 += 1024) {
+    const int i = c0 + threadIdx.x;
+    long long v = i < n ? counts[i] : 0;
+    const long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    if (lane == 31) s_part[warp] = v;
+    __syncthreads();
+    long long wb = 0, tot = 0;
+    for (int w = 0; w < 32; w++) {
+      if (w < warp) wb += s_part[w];
+      tot += s_part[w];
+    }
+    const long long excl = s_base + wb + v - x;
+    if (i < n) out[i] = excl > 0x7fffffffLL ? 0x7fffffff : (int)excl;
+    __syncthreads();
+    if (threadIdx.x == 0) s_base += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[n] = s_base > 0x7fffffffLL ? 0x7fffffff : (int)s_base;
+    if (s_base > 0x7fffffffLL) *overflow = 1;
+    *total = s_base;
+  }
+}
+
+// out = 1 when the two value arrays (same structure) differ bitwise.
+__global__ void values_differ_kernel(const float* __restrict__ x, const float* __restrict__ y, long long n,
+                                     int* __restrict__ out) {
+  int d = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    if (__float_as_uint(x[t]) != __float_as_uint(y[t])) d = 1;
+  if (__any_sync(0xffffffffu, d) && (threadIdx.x & 31) == 0) atomicOr(out, 1);
+}
+
+// Dense [rows][ld] <- CSR entries (the rest was filled with the identity
+// before); one warp per row.
+__global__ void csr_scatter_kernel(int rows, const int* __restrict__ rp, const int* __restrict__ cj,
+                                   const float* __restrict__ cv, float* __restrict__ X, long long ld) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5)
+    for (int e = rp[r] + lane; e < rp[r + 1]; e += 32) X[(long long)r * ld + cj[e]] = cv[e];
+}
+
+// Entries of each dense row that differ bitwise from the identity; one warp per row.
+__global__ void dense_row_count_kernel(int rows, int cols, const float* __restrict__ X, long long ld, float ident,
+                                       int* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t id = __float_as_uint(ident);
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
+    int c = 0;
+    for (int j = lane; j < cols; j += 32) c += __float_as_uint(X[(long long)r * ld + j]) != id;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) counts[r] = c;
+  }
+}
+
+// CSR <- dense rows (entries that are not the identity, increasing column),
+// at the offsets rp; one warp per row, ballot compaction.
+__global__ void dense_to_csr_kernel(int rows, int cols, const float* __restrict__ X, long long ld, float ident,
+                                    const int* __restrict__ rp, int* __restrict__ cj, float* __restrict__ cv) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t id = __float_as_uint(ident);
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
+    int pos = rp[r];
+    for (int j0 = 0; j0 < cols; j0 += 32) {
+      const int j = j0 + lane;
+      const float v = j < cols ? X[(long long)r * ld + j] : ident;
+      const bool keep = j < cols && __float_as_uint(v) != id;
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int at = pos + __popc(m & ((1u << lane) - 1));
+        cj[at] = j;
+        cv[at] = v;
+      }
+      pos += __popc(m);
+    }
+  }
+}
+
+}  // namespace simd2
