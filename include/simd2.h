@@ -287,6 +287,22 @@ int simd2_spgemm_compute(simd2_op op, int M, int N, int K, const int* A_rowptr, 
 int simd2_closure_sparse(simd2_op op, int n, int* rowptr, int* cols, float* vals, long long capacity,
                          long long* nnz_inout, int max_iter, int* iters_out, cudaStream_t stream);
 
+/* Minimum spanning forest of an undirected weighted graph from its minimax
+ * closure.  The reference's mst app (apps/mst/cuASR/mst_cuASR.cu) computes
+ * the min_max closure D[u][v] = min over u-v paths of the largest edge
+ * weight; an edge belongs to the spanning forest that Kruskal builds in
+ * (weight, u, v) order exactly when it is chosen from the edges with
+ * w(u, v) == D[u][v], which this entry scans for on the GPU before a
+ * union-find on the host.
+ * W: n x n device matrix (pitch ldw), +inf where there is no edge; the
+ * undirected weight of {u, v} is min(W[u][v], W[v][u]); the diagonal is
+ * ignored.  Outputs in HOST memory: edges[2e], edges[2e+1] (u < v) and
+ * weights[e] for e < *count_out (at most n - 1; fewer when the graph is
+ * disconnected), in Kruskal order; *total_out the weight sum (FP64);
+ * *iters_out the closure's step count.  Synchronous. */
+int simd2_mst(int n, const float* W, int ldw, int* edges, float* weights, int* count_out, double* total_out,
+              int* iters_out, cudaStream_t stream);
+
 /* Reserve the per-(device, stream) workspace for srgemm calls up to
  * M x N x K so that later calls (e.g. inside stream capture) allocate
  * nothing.  Returns the bytes now reserved in *bytes_out (may be NULL). */

@@ -192,6 +192,36 @@ def path(P, i, j):
     return out[::-1]
 
 
+def mst(W):
+    """Kruskal over every edge of the undirected graph W (weight of {u, v} =
+    min(W[u][v], W[v][u]), +inf = none) in (weight, u, v) order: (edges
+    [m, 2] with u < v in Kruskal order, weights [m])."""
+    W = np.asarray(W, np.float32)
+    n = W.shape[0]
+    S = np.minimum(W, W.T)
+    iu, ju = np.triu_indices(n, 1)
+    w = S[iu, ju]
+    keep = np.isfinite(w)
+    iu, ju, w = iu[keep], ju[keep], w[keep]
+    order = np.lexsort((ju, iu, w))
+    parent = list(range(n))
+
+    def find(v):
+        while parent[v] != v:
+            parent[v] = parent[parent[v]]
+            v = parent[v]
+        return v
+
+    edges, weights = [], []
+    for e in order:
+        a, b = find(int(iu[e])), find(int(ju[e]))
+        if a != b:
+            parent[b] = a
+            edges.append((int(iu[e]), int(ju[e])))
+            weights.append(w[e])
+    return np.array(edges, np.int32).reshape(-1, 2), np.array(weights, np.float32)
+
+
 def knn(query, ref, k, threads=None):
     """k nearest references per query: (dist[Q,k] float32, idx[Q,k] int32, sqdist[Q,k] float64)."""
     query = np.ascontiguousarray(query, dtype=np.float32)

@@ -63,6 +63,8 @@ def lib() -> ctypes.CDLL:
         L.simd2_spgemm_nnz.argtypes = [I, I, I, I, P, P, I, P, P, I, P, P, I, P, ctypes.POINTER(LL), P]
         L.simd2_spgemm_compute.argtypes = [I, I, I, I, P, P, P, I, P, P, P, I, P, P, P, I, P, P, P, LL, P]
         L.simd2_closure_sparse.argtypes = [I, I, P, P, P, LL, ctypes.POINTER(LL), I, ctypes.POINTER(I), P]
+        L.simd2_mst.argtypes = [I, P, I, P, P, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(I), P]
         L.simd2_reserve_workspace.argtypes = [I, I, I, I, P, ctypes.POINTER(ctypes.c_size_t)]
         L.simd2_release_workspaces.argtypes = []
         L.simd2_device_status.argtypes = []
@@ -367,6 +369,25 @@ def closure_sparse(op: str, X, capacity: int | None = None, max_iter: int = 500,
                                     ctypes.byref(nnz), max_iter, ctypes.byref(it), _stream(stream))
     _check(rc, f"closure_sparse({op}) [entries {nnz.value}]")
     return (rp, cj[: nnz.value].clone(), cv[: nnz.value].clone()), it.value
+
+
+def mst(W: torch.Tensor, stream=None):
+    """Minimum spanning forest of the undirected graph W (+inf = no edge, the
+    weight of {u, v} is min(W[u][v], W[v][u])): returns (edges [m, 2] int32
+    numpy with u < v, weights [m] float32 numpy, total weight, closure steps)."""
+    import numpy as np
+    n = W.shape[0]
+    if W.shape != (n, n) or W.dtype != torch.float32:
+        raise ValueError("mst needs a square float32 matrix")
+    edges = np.zeros((max(n - 1, 1), 2), np.int32)
+    weights = np.zeros(max(n - 1, 1), np.float32)
+    cnt, it = ctypes.c_int(0), ctypes.c_int(0)
+    tot = ctypes.c_double(0)
+    rc = lib().simd2_mst(n, W.data_ptr() if n else None, _mat(W, "W") if n else 1,
+                         edges.ctypes.data_as(ctypes.c_void_p), weights.ctypes.data_as(ctypes.c_void_p),
+                         ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(it), _stream(stream))
+    _check(rc, "mst")
+    return edges[: cnt.value].copy(), weights[: cnt.value].copy(), tot.value, it.value
 
 
 def closure_panel_step(op: str, panel: torch.Tensor, full: torch.Tensor, out: torch.Tensor, changed: torch.Tensor,

@@ -25,6 +25,7 @@
 #include "knn_fused.cuh"
 #include "pred.cuh"
 #include "spgemm.cuh"
+#include "mst.cuh"
 
 namespace simd2 {
 namespace {
@@ -1518,6 +1519,93 @@ int simd2_closure_sparse(simd2_op op, int n, int* rowptr, int* cols, float* vals
   *nnz_inout = nnz;
   if (iters_out) *iters_out = it;
   return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
+}
+
+int simd2_mst(int n, const float* W, int ldw, int* edges, float* weights, int* count_out, double* total_out,
+              int* iters_out, cudaStream_t stream) {
+  using namespace simd2;
+  if (count_out) *count_out = 0;
+  if (total_out) *total_out = 0.0;
+  if (iters_out) *iters_out = 0;
+  if (n < 0 || !count_out || (n > 1 && (!W || ldw < n || !edges || !weights))) return SIMD2_ERR_INVALID_ARG;
+  if (n <= 1) return SIMD2_OK;
+  int rc = check_device();
+  if (rc) return rc;
+  // slot 1: [S n x n][D n x n][count]; slot 2: the candidates; the closure uses slot 0
+  const size_t nn = (size_t)n * n;
+  const size_t d_off = align_up(nn * 4, kAlign), c_off = d_off + align_up(nn * 4, kAlign);
+  void* p = nullptr;
+  if ((rc = get_workspace_slot(stream, 1, c_off + kAlign, &p))) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  float* S = reinterpret_cast<float*>(ws);
+  float* D = reinterpret_cast<float*>(ws + d_off);
+  int* count = reinterpret_cast<int*>(ws + c_off);
+  mst_symmetrize_kernel<<<grid_for((long long)nn), 256, 0, stream>>>(n, W, ldw, S);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(D, S, nn * 4, cudaMemcpyDeviceToDevice, stream));
+  int it = 0;
+  rc = closure_f32(SIMD2_MIN_MAX, n, D, n, 500, SIMD2_CONV_EXACT, &it, stream);
+  if (rc) return rc;
+  if (iters_out) *iters_out = it;
+  SIMD2_CUDA_TRY(cudaMemsetAsync(count, 0, 4, stream));
+  mst_candidates_kernel<true><<<grid_for((long long)nn), 256, 0, stream>>>(n, S, D, count, 0, nullptr, nullptr);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  int m = 0;
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(&m, count, 4, cudaMemcpyDeviceToHost, stream));
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  std::vector<int> uv(2 * (size_t)m + 2);
+  std::vector<float> wv((size_t)m + 1);
+  if (m > 0) {
+    const size_t w_off = align_up((size_t)m * 8, kAlign);
+    void* q = nullptr;
+    if ((rc = get_workspace_slot(stream, 2, w_off + (size_t)m * 4 + kAlign, &q))) return rc;
+    int* cuv = static_cast<int*>(q);
+    float* cw = reinterpret_cast<float*>(static_cast<uint8_t*>(q) + w_off);
+    SIMD2_CUDA_TRY(cudaMemsetAsync(count, 0, 4, stream));
+    mst_candidates_kernel<false><<<grid_for((long long)nn), 256, 0, stream>>>(n, S, D, count, m, cuv, cw);
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(uv.data(), cuv, (size_t)m * 8, cudaMemcpyDeviceToHost, stream));
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(wv.data(), cw, (size_t)m * 4, cudaMemcpyDeviceToHost, stream));
+    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  }
+  // Kruskal over the candidates in (weight, u, v) order, union-find with
+  // path halving and union by size
+  std::vector<int> order(m);
+  for (int e = 0; e < m; e++) order[e] = e;
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    if (wv[a] != wv[b]) return wv[a] < wv[b];
+    if (uv[2 * a] != uv[2 * b]) return uv[2 * a] < uv[2 * b];
+    return uv[2 * a + 1] < uv[2 * b + 1];
+  });
+  std::vector<int> parent(n), size(n, 1);
+  for (int v = 0; v < n; v++) parent[v] = v;
+  auto find = [&](int v) {
+    while (parent[v] != v) {
+      parent[v] = parent[parent[v]];
+      v = parent[v];
+    }
+    return v;
+  };
+  int taken = 0;
+  double total = 0.0;
+  for (int e : order) {
+    int a = find(uv[2 * e]), b = find(uv[2 * e + 1]);
+    if (a == b) continue;
+    if (size[a] < size[b]) std::swap(a, b);
+    parent[b] = a;
+    size[a] += size[b];
+    edges[2 * taken] = uv[2 * e];
+    edges[2 * taken + 1] = uv[2 * e + 1];
+    weights[taken] = wv[e];
+    total += wv[e];
+    taken++;
+  }
+  *count_out = taken;
+  if (total_out) *total_out = total;
+  return SIMD2_OK;
 }
 
 int simd2_reserve_workspace(simd2_op op, int M, int N, int K, cudaStream_t stream, size_t* bytes_out) {
