@@ -566,11 +566,14 @@ def main():
         bo = sum(host_out[op].numel() * host_out[op].element_size() for op in SWEEP_OPS)
 
         def e2e_step(free_ev):
+            # Every semiring has its own device buffers; the only reuse is the
+            # same semiring's buffers one step later, so H2D of op j waits for
+            # nothing but the D2H of op j in the previous step.
             for j, op in enumerate(SWEEP_OPS):
                 slot = slots[j % 2][op]
                 with torch.cuda.stream(s_in):
-                    if free_ev[j % 2] is not None:
-                        s_in.wait_event(free_ev[j % 2])
+                    if free_ev.get(op) is not None:
+                        s_in.wait_event(free_ev[op])
                     for hx, dx in zip(host[op], slot[:3]):
                         dx.copy_(hx, non_blocking=True)
                     in_ev = torch.cuda.Event()
@@ -585,9 +588,9 @@ def main():
                     host_out[op].copy_(slot[3], non_blocking=True)
                     f_ev = torch.cuda.Event()
                     f_ev.record(s_out)
-                free_ev[j % 2] = f_ev
+                free_ev[op] = f_ev
 
-        free = [None, None]
+        free = {}
         for _ in range(2):
             e2e_step(free)
         torch.cuda.synchronize()
@@ -603,8 +606,8 @@ def main():
             dist.all_reduce(et, op=dist.ReduceOp.MAX)
         e2e = {"value": ops_per_step * e2e_steps * world / float(et.item()) / 1e9, "unit": "Gop/s",
                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
-               "how": "pinned host buffers; per semiring H2D(A,B,C) -> srgemm -> D2H(D), two buffer sets on "
-                      "three streams; wall clock around synchronize"}
+               "how": "pinned host buffers; per semiring H2D(A,B,C) -> srgemm -> D2H(D) on three streams "
+                      "(copy in, compute, copy out), device buffers per semiring; wall clock around synchronize"}
 
     clocks = clk.summary()
     peaks, peak_kind = measured_peaks()

@@ -482,6 +482,14 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
 // ---------------------------------------------------------------------------
 // tensor-core paths
 // ---------------------------------------------------------------------------
+// TMA box width (elements along K) and swizzle of the tensor-core operand tiles.
+template <int KIND>
+constexpr int tc_box_k() { return TcCfg<KIND>::kBK; }
+template <int KIND>
+constexpr CUtensorMapSwizzle tc_swizzle() {
+  return TcCfg<KIND>::kRowBytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+}
+
 template <int KIND>
 int launch_tc(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
               const CUtensorMap& b1, const TcEpilogue& ep, cudaStream_t stream) {
@@ -570,12 +578,13 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   SIMD2_CUDA_TRY(cudaGetLastError());
   CUtensorMap ma0, ma1, mb0, mb1;
   const auto BF = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-  const auto SW = CU_TENSOR_MAP_SWIZZLE_128B;
+  const auto SW = tc_swizzle<0>();
+  constexpr int BX = tc_box_k<0>();
   int rc;
-  if ((rc = make_map_2d(&ma0, BF, 2, ahi, M, Kp, Kp, 64, kTcBM, SW))) return rc;
-  if ((rc = make_map_2d(&ma1, BF, 2, alo, M, Kp, Kp, 64, kTcBM, SW))) return rc;
-  if ((rc = make_map_2d(&mb0, BF, 2, ws + plan.b0, N, Kp, Kp, 64, kTcBN, SW))) return rc;
-  if ((rc = make_map_2d(&mb1, BF, 2, ws + plan.b1, N, Kp, Kp, 64, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&ma0, BF, 2, ahi, M, Kp, Kp, BX, kTcBM, SW))) return rc;
+  if ((rc = make_map_2d(&ma1, BF, 2, alo, M, Kp, Kp, BX, kTcBM, SW))) return rc;
+  if ((rc = make_map_2d(&mb0, BF, 2, ws + plan.b0, N, Kp, Kp, BX, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&mb1, BF, 2, ws + plan.b1, N, Kp, Kp, BX, kTcBN, SW))) return rc;
   TcEpilogue ep{};
   ep.op = op;
   ep.do_epilogue = do_epilogue;
@@ -2146,15 +2155,16 @@ extern "C" int simd2_knn_ex(const float* query, int Q, int ldq, const float* ref
   for (int i = 0; i < 4; i++) count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   const auto BF = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-  const auto SW = CU_TENSOR_MAP_SWIZZLE_128B;
+  const auto SW = tc_swizzle<0>();
+  constexpr int BX = tc_box_k<0>();
   CUtensorMap mb0, mb1;
-  if ((rc = make_map_2d(&mb0, BF, 2, r_hi, R, Dp, Dp, 64, kTcBN, SW))) return rc;
-  if ((rc = make_map_2d(&mb1, BF, 2, r_lo, R, Dp, Dp, 64, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&mb0, BF, 2, r_hi, R, Dp, Dp, BX, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&mb1, BF, 2, r_lo, R, Dp, Dp, BX, kTcBN, SW))) return rc;
   for (int q0 = 0; q0 < Q; q0 += Qc) {
     const int rows = std::min(Qc, Q - q0);
     CUtensorMap ma0, ma1;
-    if ((rc = make_map_2d(&ma0, BF, 2, q_hi + (size_t)q0 * Dp, rows, Dp, Dp, 64, kTcBM, SW))) return rc;
-    if ((rc = make_map_2d(&ma1, BF, 2, q_lo + (size_t)q0 * Dp, rows, Dp, Dp, 64, kTcBM, SW))) return rc;
+    if ((rc = make_map_2d(&ma0, BF, 2, q_hi + (size_t)q0 * Dp, rows, Dp, Dp, BX, kTcBM, SW))) return rc;
+    if ((rc = make_map_2d(&ma1, BF, 2, q_lo + (size_t)q0 * Dp, rows, Dp, Dp, BX, kTcBM, SW))) return rc;
     TcEpilogue ep{};
     ep.op = SIMD2_MINUS_SQUARE;
     ep.do_epilogue = 0;

@@ -10,7 +10,8 @@
 //                    cancellation band (small distance relative to the norms).
 //
 // One CTA computes a 128 x 256 tile of D with 4 warps:
-//   warp 0 lane 0  -- TMA producer (2D tiled loads, no multicast, 128-byte swizzle),
+//   warp 0 lane 0  -- TMA producer (2D tiled loads, no multicast; 64-byte
+//                     swizzled rows for BF16, 128-byte for INT8),
 //   warp 1 lane 0  -- MMA issuer (tcgen05.mma, cta_group::1, M=128 N=256),
 //   warps 0..3     -- epilogue: tcgen05.ld of the TMEM accumulator (warp w reads
 //                     TMEM lanes 32w..32w+31 = tile rows), fused (+) C, stores.
@@ -24,17 +25,19 @@ namespace simd2 {
 constexpr int kTcBM = 128;
 constexpr int kTcBN = 256;
 constexpr int kTcThreads = 128;
-constexpr int kTcRowBytes = 128;  // one 128-byte swizzle row of K per operand row
-
 template <int KIND>
 struct TcCfg;
-// BF16 hi/lo: BK = 64 elements, two A tiles and two B tiles per stage.
+// BF16 hi/lo: BK = 32 elements (64-byte swizzled rows), two A tiles and two B
+// tiles per stage, 4 stages of 48 KiB: three stages stay in flight while one
+// feeds the tensor cores (two 96 KiB stages of 128-byte rows left the TMA
+// latency exposed).
 template <>
 struct TcCfg<0> {
-  static constexpr int kBK = 64;
+  static constexpr int kBK = 32;
+  static constexpr int kRowBytes = 64;
   static constexpr int kNumA = 2;
   static constexpr int kNumB = 2;
-  static constexpr int kStages = 2;
+  static constexpr int kStages = 4;
   static constexpr int kKStep = 16;  // K per tcgen05.mma kind::f16
   // c_format F32 (1), a/b format BF16 (1), K-major A and B, N=256, M=128
   static constexpr uint32_t kIdesc =
@@ -44,6 +47,7 @@ struct TcCfg<0> {
 template <>
 struct TcCfg<1> {
   static constexpr int kBK = 128;
+  static constexpr int kRowBytes = 128;
   static constexpr int kNumA = 1;
   static constexpr int kNumB = 1;
   static constexpr int kStages = 4;
@@ -52,12 +56,14 @@ struct TcCfg<1> {
   static constexpr uint32_t kIdesc = (2u << 4) | ((uint32_t)(kTcBN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
 };
 
-constexpr int kTcATile = kTcBM * kTcRowBytes;  // 16 KiB
-constexpr int kTcBTile = kTcBN * kTcRowBytes;  // 32 KiB
+template <int KIND>
+__host__ __device__ constexpr int tc_a_tile() { return kTcBM * TcCfg<KIND>::kRowBytes; }
+template <int KIND>
+__host__ __device__ constexpr int tc_b_tile() { return kTcBN * TcCfg<KIND>::kRowBytes; }
 
 template <int KIND>
 __host__ __device__ constexpr int tc_stage_bytes() {
-  return TcCfg<KIND>::kNumA * kTcATile + TcCfg<KIND>::kNumB * kTcBTile;
+  return TcCfg<KIND>::kNumA * tc_a_tile<KIND>() + TcCfg<KIND>::kNumB * tc_b_tile<KIND>();
 }
 template <int KIND>
 constexpr size_t tc_smem_bytes() {
@@ -65,18 +71,23 @@ constexpr size_t tc_smem_bytes() {
 }
 
 // Shared-memory matrix descriptor for a K-major operand tile written by TMA
-// with 128-byte swizzle: rows of 128 bytes, 8-row core-matrix groups 1024
-// bytes apart (stride byte offset), leading byte offset unused (1), version 1,
-// layout type 2 = SWIZZLE_128B.  Advancing K inside the 128-byte row moves the
-// start address by the byte offset.
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
+// with a 128- or 64-byte swizzle: rows of row_bytes, 8-row core-matrix groups
+// 8 * row_bytes apart (stride byte offset), leading byte offset unused (1),
+// version 1, layout type 2 = SWIZZLE_128B or 4 = SWIZZLE_64B.  Advancing K
+// inside a row moves the start address by the byte offset.
+__device__ __forceinline__ uint64_t umma_desc_swizzled(uint32_t smem_addr, int row_bytes) {
   uint64_t d = 0;
   d |= (uint64_t)((smem_addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;           // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024u >> 4) << 32; // stride byte offset
-  d |= (uint64_t)1u << 46;           // descriptor version (sm_100)
-  d |= (uint64_t)2u << 61;           // SWIZZLE_128B
+  d |= (uint64_t)1u << 16;                             // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)((8u * row_bytes) >> 4) << 32;        // stride byte offset
+  d |= (uint64_t)1u << 46;                             // descriptor version (sm_100)
+  d |= (uint64_t)(row_bytes == 128 ? 2u : 4u) << 61;   // SWIZZLE_128B / SWIZZLE_64B
   return d;
+}
+
+// The descriptor for 128-byte swizzled rows (8-row groups 1024 bytes apart).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
+  return umma_desc_swizzled(smem_addr, 128);
 }
 
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -225,10 +236,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_arrive_expect_tx(&full[s], kStage);
       const int kx = kt * Cfg::kBK;
       tma_load_2d(st, &tmA0, &full[s], kx, m0);
-      if constexpr (Cfg::kNumA == 2) tma_load_2d(st + kTcATile, &tmA1, &full[s], kx, m0);
-      uint8_t* sb = st + Cfg::kNumA * kTcATile;
+      if constexpr (Cfg::kNumA == 2) tma_load_2d(st + tc_a_tile<KIND>(), &tmA1, &full[s], kx, m0);
+      uint8_t* sb = st + Cfg::kNumA * tc_a_tile<KIND>();
       tma_load_2d(sb, &tmB0, &full[s], kx, n0);
-      if constexpr (Cfg::kNumB == 2) tma_load_2d(sb + kTcBTile, &tmB1, &full[s], kx, n0);
+      if constexpr (Cfg::kNumB == 2) tma_load_2d(sb + tc_b_tile<KIND>(), &tmB1, &full[s], kx, n0);
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
@@ -241,19 +252,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
       tc_fence_after();
       const uint32_t st = smem_u32(smem + s * kStage);
-      const uint32_t a0 = st, a1 = st + kTcATile;
-      const uint32_t b0 = st + Cfg::kNumA * kTcATile, b1 = b0 + kTcBTile;
+      const uint32_t a0 = st, a1 = st + tc_a_tile<KIND>();
+      const uint32_t b0 = st + Cfg::kNumA * tc_a_tile<KIND>(), b1 = b0 + tc_b_tile<KIND>();
+      constexpr int RB = Cfg::kRowBytes;
 #pragma unroll
       for (int ks = 0; ks < Cfg::kBK / Cfg::kKStep; ks++) {
-        const uint32_t koff = ks * Cfg::kKStep * (KIND == 0 ? 2 : 1);  // bytes along the 128-byte row
+        const uint32_t koff = ks * Cfg::kKStep * (KIND == 0 ? 2 : 1);  // bytes along the swizzled row
         const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
         if constexpr (KIND == 0) {
           // hi*hi, hi*lo, lo*hi
-          tc_mma<0>(tmem, umma_desc_sw128(a0 + koff), umma_desc_sw128(b0 + koff), acc0);
-          tc_mma<0>(tmem, umma_desc_sw128(a0 + koff), umma_desc_sw128(b1 + koff), 1u);
-          tc_mma<0>(tmem, umma_desc_sw128(a1 + koff), umma_desc_sw128(b0 + koff), 1u);
+          tc_mma<0>(tmem, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
+          tc_mma<0>(tmem, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b1 + koff, RB), 1u);
+          tc_mma<0>(tmem, umma_desc_swizzled(a1 + koff, RB), umma_desc_swizzled(b0 + koff, RB), 1u);
         } else {
-          tc_mma<1>(tmem, umma_desc_sw128(a0 + koff), umma_desc_sw128(b0 + koff), acc0);
+          tc_mma<1>(tmem, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
         }
       }
       tc_commit(&empty[s]);  // stage s is free once these MMAs have read it
