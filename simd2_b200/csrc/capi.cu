@@ -507,7 +507,11 @@ int launch_tc(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1,
   const int tiles_n = (N + kTcBN - 1) / kTcBN;
   auto* ev = prof_slot(2LL * M * N * K, kProfTensor);
   if (ev) cudaEventRecord(ev->first, stream);
-  kern<<<tiles_m * tiles_n, kTcThreads, smem, stream>>>(a0, a1, b0, b1, M, N, K, ep, tiles_m, tiles_n);
+  // persistent: at most one CTA per SM (shared memory and TMEM hold one)
+  int sms = 148;
+  SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int grid = std::min(tiles_m * tiles_n, sms);
+  kern<<<grid, kTcThreads, smem, stream>>>(a0, a1, b0, b1, M, N, K, ep, tiles_m, tiles_n);
   count_launch();
   if (ev) cudaEventRecord(ev->second, stream);
   SIMD2_CUDA_TRY(cudaGetLastError());

@@ -195,6 +195,7 @@ __global__ void __launch_bounds__(kKfThreads, 1)
         }
       }
     }
+    __syncwarp();  // lanes 1..31 wait here, off the issue slots, while lane 0 runs the loop
   } else if (warp == 1) {
     if (lane == 0) {
       // ---------------- MMA issuer ----------------
@@ -239,6 +240,7 @@ __global__ void __launch_bounds__(kKfThreads, 1)
       }
       tc_commit(fin);  // every MMA issued above has completed when fin flips
     }
+    __syncwarp();
   } else {
     // ---------------- selection (warps 2..9) ----------------
     const int quad = warp & 3;             // TMEM lane quadrant this warp may read

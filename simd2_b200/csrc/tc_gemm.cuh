@@ -9,12 +9,16 @@
 //                    recomputes sum_k (a-b)^2 exactly in FP32 inside the
 //                    cancellation band (small distance relative to the norms).
 //
-// One CTA computes a 128 x 256 tile of D with 4 warps:
+// Persistent: one CTA per SM walks the 128 x 256 tiles of D (grouped raster)
+// with 6 warps:
 //   warp 0 lane 0  -- TMA producer (2D tiled loads, no multicast; 64-byte
-//                     swizzled rows for BF16, 128-byte for INT8),
-//   warp 1 lane 0  -- MMA issuer (tcgen05.mma, cta_group::1, M=128 N=256),
-//   warps 0..3     -- epilogue: tcgen05.ld of the TMEM accumulator (warp w reads
-//                     TMEM lanes 32w..32w+31 = tile rows), fused (+) C, stores.
+//                     swizzled rows for BF16, 128-byte for INT8) over every
+//                     k-tile of every tile, one ring of stages,
+//   warp 1 lane 0  -- MMA issuer (tcgen05.mma, cta_group::1, M=128 N=256) into
+//                     one of two 256-column TMEM accumulators, so the next
+//                     tile's MMAs run while the previous tile is written out,
+//   warps 2..5     -- epilogue: tcgen05.ld of the accumulator (warp w reads
+//                     TMEM lanes 32(w%4)..+31 = tile rows), fused (+) C, stores.
 // Both operands are K-major in shared memory: A is [M][K] as given, B is
 // stored transposed ([N][K]) by the operand-prep kernel.
 #pragma once
@@ -24,7 +28,8 @@ namespace simd2 {
 
 constexpr int kTcBM = 128;
 constexpr int kTcBN = 256;
-constexpr int kTcThreads = 128;
+constexpr int kTcEpiWarps = 4;
+constexpr int kTcThreads = (2 + kTcEpiWarps) * 32;  // TMA warp, MMA warp, 4 epilogue warps
 template <int KIND>
 struct TcCfg;
 // BF16 hi/lo: BK = 32 elements (64-byte swizzled rows), two A tiles and two B
@@ -67,7 +72,7 @@ __host__ __device__ constexpr int tc_stage_bytes() {
 }
 template <int KIND>
 constexpr size_t tc_smem_bytes() {
-  return (size_t)TcCfg<KIND>::kStages * tc_stage_bytes<KIND>() + 1024 + 256;
+  return (size_t)TcCfg<KIND>::kStages * tc_stage_bytes<KIND>() + (size_t)kTcEpiWarps * 32 * 33 * 4 + 1024 + 256;
 }
 
 // Shared-memory matrix descriptor for a K-major operand tile written by TMA
@@ -181,37 +186,46 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   constexpr int kStage = tc_stage_bytes<KIND>();
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * kStage);
+  uint32_t* epi_smem = reinterpret_cast<uint32_t*>(smem + S * kStage);  // 4 x 32 x 33 words
+  uint64_t* full = reinterpret_cast<uint64_t*>(epi_smem + kTcEpiWarps * 32 * 33);
   uint64_t* empty = full + S;
-  uint64_t* done = empty + S;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* acc_full = empty + S;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* fin = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
 
-  // Grouped raster over (tile_m, tile_n): 8 tile rows per group.
-  const int group = 8;
-  const int per_group = group * tiles_n;
-  const int g = blockIdx.x / per_group;
-  const int first_m = g * group;
-  const int gsize = min(tiles_m - first_m, group);
-  const int local = blockIdx.x - g * per_group;
-  const int m0 = (first_m + local % gsize) * kTcBM;
-  const int n0 = (local / gsize) * kTcBN;
+  const int tiles = tiles_m * tiles_n;
   const int ktiles = (K + Cfg::kBK - 1) / Cfg::kBK;
-
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  // Grouped raster over (tile_m, tile_n): 8 tile rows per group.
+  auto tile_origin = [&](int t, int& m0, int& n0) {
+    const int group = 8;
+    const int per_group = group * tiles_n;
+    const int g = t / per_group;
+    const int first_m = g * group;
+    const int gsize = min(tiles_m - first_m, group);
+    const int local = t - g * per_group;
+    m0 = (first_m + local % gsize) * kTcBM;
+    n0 = (local / gsize) * kTcBN;
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    for (int a = 0; a < 2; a++) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], kTcEpiWarps);
+    }
+    mbar_init(fin, 1);
     fence_mbar_init();
   }
   if (warp == 0) {
-    // 256 TMEM columns: the 128 x 256 FP32/S32 accumulator.
+    // 512 TMEM columns: two 128 x 256 FP32/S32 accumulators.
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(256)
+                 "r"(512)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -220,229 +234,270 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  bool ok = true;
-  if (warp == 0 && lane == 0) {
-    // ---------------- TMA producer ----------------
-    prefetch_tensormap(&tmA0);
-    prefetch_tensormap(&tmB0);
-    for (int kt = 0; kt < ktiles; kt++) {
-      const int s = kt % S;
-      if (!mbar_wait(&empty[s], ((kt / S) & 1) ^ 1)) {
-        report_timeout(101);
-        ok = false;
-        break;
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer: every k-tile of every tile of this CTA ----------------
+      prefetch_tensormap(&tmA0);
+      prefetch_tensormap(&tmB0);
+      int j = 0;  // running stage counter
+      bool ok = true;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        int m0, n0;
+        tile_origin(t, m0, n0);
+        for (int kt = 0; kt < ktiles; kt++, j++) {
+          const int s = j % S;
+          if (!mbar_wait(&empty[s], ((j / S) & 1) ^ 1)) {
+            report_timeout(101);
+            ok = false;
+            break;
+          }
+          uint8_t* st = smem + s * kStage;
+          mbar_arrive_expect_tx(&full[s], kStage);
+          const int kx = kt * Cfg::kBK;
+          tma_load_2d(st, &tmA0, &full[s], kx, m0);
+          if constexpr (Cfg::kNumA == 2) tma_load_2d(st + tc_a_tile<KIND>(), &tmA1, &full[s], kx, m0);
+          uint8_t* sb = st + Cfg::kNumA * tc_a_tile<KIND>();
+          tma_load_2d(sb, &tmB0, &full[s], kx, n0);
+          if constexpr (Cfg::kNumB == 2) tma_load_2d(sb + tc_b_tile<KIND>(), &tmB1, &full[s], kx, n0);
+        }
       }
-      uint8_t* st = smem + s * kStage;
-      mbar_arrive_expect_tx(&full[s], kStage);
-      const int kx = kt * Cfg::kBK;
-      tma_load_2d(st, &tmA0, &full[s], kx, m0);
-      if constexpr (Cfg::kNumA == 2) tma_load_2d(st + tc_a_tile<KIND>(), &tmA1, &full[s], kx, m0);
-      uint8_t* sb = st + Cfg::kNumA * tc_a_tile<KIND>();
-      tma_load_2d(sb, &tmB0, &full[s], kx, n0);
-      if constexpr (Cfg::kNumB == 2) tma_load_2d(sb + tc_b_tile<KIND>(), &tmB1, &full[s], kx, n0);
     }
-  } else if (warp == 1 && lane == 0) {
-    // ---------------- MMA issuer ----------------
-    for (int kt = 0; kt < ktiles; kt++) {
-      const int s = kt % S;
-      if (!mbar_wait(&full[s], (kt / S) & 1)) {
-        report_timeout(102);
-        ok = false;
-        break;
+    __syncwarp();  // lanes 1..31 wait here, off the issue slots, while lane 0 runs the loop
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---------------- MMA issuer: tile lt accumulates into TMEM half lt & 1 ----------------
+      int j = 0;
+      bool ok = true;
+      int lt = 0;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, lt++) {
+        const int acc = lt & 1;
+        if (!mbar_wait(&acc_empty[acc], ((lt >> 1) & 1) ^ 1)) {
+          report_timeout(104);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + acc * kTcBN;
+        for (int kt = 0; kt < ktiles; kt++, j++) {
+          const int s = j % S;
+          if (!mbar_wait(&full[s], (j / S) & 1)) {
+            report_timeout(102);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = smem_u32(smem + s * kStage);
+          const uint32_t a0 = st, a1 = st + tc_a_tile<KIND>();
+          const uint32_t b0 = st + Cfg::kNumA * tc_a_tile<KIND>(), b1 = b0 + tc_b_tile<KIND>();
+          constexpr int RB = Cfg::kRowBytes;
+#pragma unroll
+          for (int ks = 0; ks < Cfg::kBK / Cfg::kKStep; ks++) {
+            const uint32_t koff = ks * Cfg::kKStep * (KIND == 0 ? 2 : 1);  // bytes along the swizzled row
+            const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
+            if constexpr (KIND == 0) {
+              // hi*hi, hi*lo, lo*hi
+              tc_mma<0>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
+              tc_mma<0>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b1 + koff, RB), 1u);
+              tc_mma<0>(d, umma_desc_swizzled(a1 + koff, RB), umma_desc_swizzled(b0 + koff, RB), 1u);
+            } else {
+              tc_mma<1>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
+            }
+          }
+          tc_commit(&empty[s]);  // stage s is free once these MMAs have read it
+        }
+        if (ok) tc_commit(&acc_full[acc]);  // accumulator complete
       }
+      tc_commit(fin);  // every MMA issued above has completed when fin flips
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue warps 2..5: warp w reads TMEM lanes 32 (w % 4) .. ----------------
+    const int quad = warp & 3;
+    uint32_t* epi_tile = epi_smem + (warp - 2) * (32 * 33);
+    bool ok = true;
+    int lt = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, lt++) {
+      const int acc = lt & 1;
+      if (ok && !mbar_wait(&acc_full[acc], (lt >> 1) & 1)) {
+        report_timeout(103);
+        ok = false;
+      }
+      ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld below is warp-collective
+      if (!ok) break;
       tc_fence_after();
-      const uint32_t st = smem_u32(smem + s * kStage);
-      const uint32_t a0 = st, a1 = st + tc_a_tile<KIND>();
-      const uint32_t b0 = st + Cfg::kNumA * tc_a_tile<KIND>(), b1 = b0 + tc_b_tile<KIND>();
-      constexpr int RB = Cfg::kRowBytes;
-#pragma unroll
-      for (int ks = 0; ks < Cfg::kBK / Cfg::kKStep; ks++) {
-        const uint32_t koff = ks * Cfg::kKStep * (KIND == 0 ? 2 : 1);  // bytes along the swizzled row
-        const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
-        if constexpr (KIND == 0) {
-          // hi*hi, hi*lo, lo*hi
-          tc_mma<0>(tmem, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
-          tc_mma<0>(tmem, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b1 + koff, RB), 1u);
-          tc_mma<0>(tmem, umma_desc_swizzled(a1 + koff, RB), umma_desc_swizzled(b0 + koff, RB), 1u);
-        } else {
-          tc_mma<1>(tmem, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
-        }
-      }
-      tc_commit(&empty[s]);  // stage s is free once these MMAs have read it
-    }
-    tc_commit(done);  // accumulator complete
-  }
-  __syncwarp();
-
-  // ---------------- epilogue (all 4 warps) ----------------
-  if (!mbar_wait(done, 0)) {
-    report_timeout(103);
-    ok = false;
-  }
-  tc_fence_after();
-  ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld below is warp-collective
-  // Each warp owns tile rows 32w..32w+31 (its TMEM lanes); tcgen05.ld gives
-  // lane l the 32 accumulators of tile row 32w+l for 32 consecutive columns.
-  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-  const int row0 = m0 + warp * 32;
-  int changed = 0;
-  if (ok) {
-    if constexpr (KIND == 1) {
-      // or_and: 32 flags of one row are 32 contiguous bytes (u8) or 128 bytes
-      // (i32), so each lane writes its own row with 16-byte vector stores.
-      const int row = row0 + lane;
-      const bool u8 = ep.out_u8 != 0;
-      const int esz = u8 ? 1 : 4;
-      const bool vec_ok = ((ep.ldd * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.D) & 15) == 0) &&
-                          (!ep.do_epilogue ||
-                           (((ep.ldc * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.C) & 15) == 0)));
-#pragma unroll 1
-      for (int c0 = 0; c0 < kTcBN; c0 += 32) {
-        uint32_t r[32];
-        tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
-        if (row >= M) continue;
-        const int colb = n0 + c0;
-        if (u8) {
-          const uint8_t* crow = static_cast<const uint8_t*>(ep.C) + (long long)row * ep.ldc;
-          uint8_t* drow = static_cast<uint8_t*>(ep.D) + (long long)row * ep.ldd;
-          if (vec_ok && colb + 32 <= N) {
-            uint32_t w[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++)
-              w[q] = (r[4 * q] != 0u) | ((r[4 * q + 1] != 0u) << 8) | ((r[4 * q + 2] != 0u) << 16) |
-                     ((uint32_t)(r[4 * q + 3] != 0u) << 24);
-            if (ep.do_epilogue) {
-              const uint4 c0v = *reinterpret_cast<const uint4*>(crow + colb);
-              const uint4 c1v = *reinterpret_cast<const uint4*>(crow + colb + 16);
-              const uint32_t cw[8] = {c0v.x, c0v.y, c0v.z, c0v.w, c1v.x, c1v.y, c1v.z, c1v.w};
-#pragma unroll
-              for (int q = 0; q < 8; q++) {
-                // normalise C's bytes to 0/1 before the OR
-                uint32_t cb = cw[q];
-                cb = ((cb & 0x7f7f7f7fu) + 0x7f7f7f7fu | cb) & 0x80808080u;
-                cb >>= 7;
-                const uint32_t v = w[q] | cb;
-                if (ep.changed && v != cb) changed = 1;
-                w[q] = v;
-              }
-            }
-            *reinterpret_cast<uint4*>(drow + colb) = make_uint4(w[0], w[1], w[2], w[3]);
-            *reinterpret_cast<uint4*>(drow + colb + 16) = make_uint4(w[4], w[5], w[6], w[7]);
-          } else {
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-              const int col = colb + j;
-              if (col < N) {
-                uint8_t v = r[j] != 0u;
+      int m0, n0;
+      tile_origin(t, m0, n0);
+      const uint32_t trow = tmem + acc * kTcBN + ((uint32_t)(quad * 32) << 16);
+      const int row0 = m0 + quad * 32;
+      int changed = 0;
+      if (ok) {
+        if constexpr (KIND == 1) {
+          // or_and: 32 flags of one row are 32 contiguous bytes (u8) or 128 bytes
+          // (i32), so each lane writes its own row with 16-byte vector stores.
+          const int row = row0 + lane;
+          const bool u8 = ep.out_u8 != 0;
+          const int esz = u8 ? 1 : 4;
+          const bool vec_ok = ((ep.ldd * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.D) & 15) == 0) &&
+                              (!ep.do_epilogue ||
+                               (((ep.ldc * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.C) & 15) == 0)));
+    #pragma unroll 1
+          for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+            uint32_t r[32];
+            tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
+            if (row >= M) continue;
+            const int colb = n0 + c0;
+            if (u8) {
+              const uint8_t* crow = static_cast<const uint8_t*>(ep.C) + (long long)row * ep.ldc;
+              uint8_t* drow = static_cast<uint8_t*>(ep.D) + (long long)row * ep.ldd;
+              if (vec_ok && colb + 32 <= N) {
+                uint32_t w[8];
+    #pragma unroll
+                for (int q = 0; q < 8; q++)
+                  w[q] = (r[4 * q] != 0u) | ((r[4 * q + 1] != 0u) << 8) | ((r[4 * q + 2] != 0u) << 16) |
+                         ((uint32_t)(r[4 * q + 3] != 0u) << 24);
                 if (ep.do_epilogue) {
-                  const uint8_t cv = crow[col] != 0;
-                  v |= cv;
-                  if (ep.changed && v != cv) changed = 1;
+                  const uint4 c0v = *reinterpret_cast<const uint4*>(crow + colb);
+                  const uint4 c1v = *reinterpret_cast<const uint4*>(crow + colb + 16);
+                  const uint32_t cw[8] = {c0v.x, c0v.y, c0v.z, c0v.w, c1v.x, c1v.y, c1v.z, c1v.w};
+    #pragma unroll
+                  for (int q = 0; q < 8; q++) {
+                    // normalise C's bytes to 0/1 before the OR
+                    uint32_t cb = cw[q];
+                    cb = ((cb & 0x7f7f7f7fu) + 0x7f7f7f7fu | cb) & 0x80808080u;
+                    cb >>= 7;
+                    const uint32_t v = w[q] | cb;
+                    if (ep.changed && v != cb) changed = 1;
+                    w[q] = v;
+                  }
                 }
-                drow[col] = v;
+                *reinterpret_cast<uint4*>(drow + colb) = make_uint4(w[0], w[1], w[2], w[3]);
+                *reinterpret_cast<uint4*>(drow + colb + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+              } else {
+    #pragma unroll
+                for (int j = 0; j < 32; j++) {
+                  const int col = colb + j;
+                  if (col < N) {
+                    uint8_t v = r[j] != 0u;
+                    if (ep.do_epilogue) {
+                      const uint8_t cv = crow[col] != 0;
+                      v |= cv;
+                      if (ep.changed && v != cv) changed = 1;
+                    }
+                    drow[col] = v;
+                  }
+                }
+              }
+            } else {
+              const int32_t* crow = static_cast<const int32_t*>(ep.C) + (long long)row * ep.ldc;
+              int32_t* drow = static_cast<int32_t*>(ep.D) + (long long)row * ep.ldd;
+              if (vec_ok && colb + 32 <= N) {
+    #pragma unroll
+                for (int q = 0; q < 8; q++) {
+                  int4 v = make_int4(r[4 * q] != 0u, r[4 * q + 1] != 0u, r[4 * q + 2] != 0u, r[4 * q + 3] != 0u);
+                  if (ep.do_epilogue) {
+                    const int4 c = *reinterpret_cast<const int4*>(crow + colb + 4 * q);
+                    v.x |= c.x != 0;
+                    v.y |= c.y != 0;
+                    v.z |= c.z != 0;
+                    v.w |= c.w != 0;
+                  }
+                  *reinterpret_cast<int4*>(drow + colb + 4 * q) = v;
+                }
+              } else {
+    #pragma unroll
+                for (int j = 0; j < 32; j++) {
+                  const int col = colb + j;
+                  if (col < N) {
+                    int32_t v = r[j] != 0u;
+                    if (ep.do_epilogue) v |= (crow[col] != 0);
+                    drow[col] = v;
+                  }
+                }
               }
             }
           }
         } else {
-          const int32_t* crow = static_cast<const int32_t*>(ep.C) + (long long)row * ep.ldc;
-          int32_t* drow = static_cast<int32_t*>(ep.D) + (long long)row * ep.ldd;
-          if (vec_ok && colb + 32 <= N) {
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-              int4 v = make_int4(r[4 * q] != 0u, r[4 * q + 1] != 0u, r[4 * q + 2] != 0u, r[4 * q + 3] != 0u);
-              if (ep.do_epilogue) {
-                const int4 c = *reinterpret_cast<const int4*>(crow + colb + 4 * q);
-                v.x |= c.x != 0;
-                v.y |= c.y != 0;
-                v.z |= c.z != 0;
-                v.w |= c.w != 0;
-              }
-              *reinterpret_cast<int4*>(drow + colb + 4 * q) = v;
+          // Sums: a 32 x 32 chunk is transposed through shared memory (the stage
+          // ring is idle now) and written row by row: lane l handles column l, so
+          // every store instruction covers 32 consecutive floats of one row.  The
+          // chunk's C values (one column per lane, 32 independent loads) and the
+          // warp's 32 row norms are fetched before the TMEM read, so their latency
+          // overlaps it instead of being paid row by row.
+          uint32_t* tile = epi_tile;
+          const bool msq = ep.op == SIMD2_MINUS_SQUARE;
+          const float na_lane = (msq && row0 + lane < M) ? ep.norm_a[row0 + lane] : 0.f;
+          const int rows_here = min(32, M - row0);
+    #pragma unroll 1
+          for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+            const int col = n0 + c0 + lane;
+            const bool col_ok = col < N;
+            float cv[32];
+            if (ep.do_epilogue) {
+              const float* Cc = static_cast<const float*>(ep.C) + col;
+    #pragma unroll
+              for (int rr = 0; rr < 32; rr++)
+                cv[rr] = (col_ok && rr < rows_here) ? Cc[(long long)(row0 + rr) * ep.ldc] : 0.f;
             }
-          } else {
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-              const int col = colb + j;
-              if (col < N) {
-                int32_t v = r[j] != 0u;
-                if (ep.do_epilogue) v |= (crow[col] != 0);
-                drow[col] = v;
+            const float nb = (msq && col_ok) ? ep.norm_b[col] : 0.f;
+            uint32_t r[32];
+            tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
+    #pragma unroll
+            for (int j = 0; j < 32; j++) tile[lane * 33 + j] = r[j];
+            __syncwarp();
+            if (msq) {
+              // distances in place; rows inside the cancellation band are
+              // recomputed exactly in a separate, rarely taken loop (one copy of
+              // the recompute code)
+              uint32_t band = 0;
+    #pragma unroll
+              for (int rr = 0; rr < 32; rr++) {
+                const float nsum = __shfl_sync(0xffffffffu, na_lane, rr) + nb;
+                const float v = __fmaf_rn(-2.0f, __uint_as_float(tile[rr * 33 + lane]), nsum);
+                tile[rr * 33 + lane] = __float_as_uint(v);
+                band |= (v < ep.band * nsum && rr < rows_here && col_ok ? 1u : 0u) << rr;
+              }
+              while (band) {
+                const int rr = __ffs(band) - 1;
+                band &= band - 1;
+                tile[rr * 33 + lane] = __float_as_uint(exact_minus_square(
+                    ep.A32 + (long long)(row0 + rr) * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows));
               }
             }
+            if (col_ok) {
+              float* Dc = static_cast<float*>(ep.D) + col;
+    #pragma unroll
+              for (int rr = 0; rr < 32; rr++) {
+                if (rr < rows_here) {
+                  float v = __uint_as_float(tile[rr * 33 + lane]);
+                  if (ep.do_epilogue) v = __fadd_rn(v, cv[rr]);
+                  Dc[(long long)(row0 + rr) * ep.ldd] = v;
+                }
+              }
+            }
+            __syncwarp();
           }
         }
       }
-    } else {
-      // Sums: a 32 x 32 chunk is transposed through shared memory (the stage
-      // ring is idle now) and written row by row: lane l handles column l, so
-      // every store instruction covers 32 consecutive floats of one row.  The
-      // chunk's C values (one column per lane, 32 independent loads) and the
-      // warp's 32 row norms are fetched before the TMEM read, so their latency
-      // overlaps it instead of being paid row by row.
-      uint32_t* tile = reinterpret_cast<uint32_t*>(smem) + warp * (32 * 33);
-      const bool msq = ep.op == SIMD2_MINUS_SQUARE;
-      const float na_lane = (msq && row0 + lane < M) ? ep.norm_a[row0 + lane] : 0.f;
-      const int rows_here = min(32, M - row0);
-#pragma unroll 1
-      for (int c0 = 0; c0 < kTcBN; c0 += 32) {
-        const int col = n0 + c0 + lane;
-        const bool col_ok = col < N;
-        float cv[32];
-        if (ep.do_epilogue) {
-          const float* Cc = static_cast<const float*>(ep.C) + col;
-#pragma unroll
-          for (int rr = 0; rr < 32; rr++)
-            cv[rr] = (col_ok && rr < rows_here) ? Cc[(long long)(row0 + rr) * ep.ldc] : 0.f;
-        }
-        const float nb = (msq && col_ok) ? ep.norm_b[col] : 0.f;
-        uint32_t r[32];
-        tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
-#pragma unroll
-        for (int j = 0; j < 32; j++) tile[lane * 33 + j] = r[j];
-        __syncwarp();
-        if (msq) {
-          // distances in place; rows inside the cancellation band are
-          // recomputed exactly in a separate, rarely taken loop (one copy of
-          // the recompute code)
-          uint32_t band = 0;
-#pragma unroll
-          for (int rr = 0; rr < 32; rr++) {
-            const float nsum = __shfl_sync(0xffffffffu, na_lane, rr) + nb;
-            const float v = __fmaf_rn(-2.0f, __uint_as_float(tile[rr * 33 + lane]), nsum);
-            tile[rr * 33 + lane] = __float_as_uint(v);
-            band |= (v < ep.band * nsum && rr < rows_here && col_ok ? 1u : 0u) << rr;
-          }
-          while (band) {
-            const int rr = __ffs(band) - 1;
-            band &= band - 1;
-            tile[rr * 33 + lane] = __float_as_uint(exact_minus_square(
-                ep.A32 + (long long)(row0 + rr) * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows));
-          }
-        }
-        if (col_ok) {
-          float* Dc = static_cast<float*>(ep.D) + col;
-#pragma unroll
-          for (int rr = 0; rr < 32; rr++) {
-            if (rr < rows_here) {
-              float v = __uint_as_float(tile[rr * 33 + lane]);
-              if (ep.do_epilogue) v = __fadd_rn(v, cv[rr]);
-              Dc[(long long)(row0 + rr) * ep.ldd] = v;
-            }
-          }
-        }
-        __syncwarp();
+
+      if (ep.changed && KIND == 1) {
+        if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
       }
+      // the accumulator half is read out: the MMA warp may reuse it
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[acc]);
     }
   }
-  if (ep.changed && KIND == 1) {
-    if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
-  }
 
+  // every MMA has completed before TMEM is released
+  if (warp == 0) {
+    if (!mbar_wait(fin, 0)) report_timeout(105);
+    tc_fence_after();
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
   }
 }
 
