@@ -78,6 +78,37 @@ struct BatchMaps {
   CUtensorMap b[2];
 };
 
+// One k-tile of the 8 x 4 register tile; ROWS = 4 skips rows ty + 16i for
+// i >= 4 (tile rows 64..127), used when those rows lie past the graph.
+template <int OP, int ROWS>
+__device__ __forceinline__ void batched_mac_ktile(float (&acc)[8][4], const float* As, const float* Bs, int ty,
+                                                  int tx, int cbase, int swz) {
+  constexpr int WN = 2;
+#pragma unroll 2
+  for (int q = 0; q < kBK / 4; q++) {
+    float4 a[ROWS];
+#pragma unroll
+    for (int ii = 0; ii < ROWS; ii++)
+      a[ii] = *reinterpret_cast<const float4*>(As + (ty + 16 * ii) * kBK + ((q ^ swz) << 2));
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      float4 b[WN];
+#pragma unroll
+      for (int c = 0; c < WN; c++)
+        b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (cbase + 32 * c + 2 * tx) * 2);
+#pragma unroll
+      for (int ii = 0; ii < ROWS; ii++) {
+        const float2 ap = h == 0 ? make_float2(a[ii].x, a[ii].y) : make_float2(a[ii].z, a[ii].w);
+#pragma unroll
+        for (int c = 0; c < WN; c++) {
+          acc[ii][2 * c] = Mac<OP>::mac2(acc[ii][2 * c], ap, make_float2(b[c].x, b[c].y));
+          acc[ii][2 * c + 1] = Mac<OP>::mac2(acc[ii][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
+        }
+      }
+    }
+  }
+}
+
 template <int OP>
 __global__ void __launch_bounds__(kSimtThreads, 1)
     closure_batched_kernel(BatchGraph* graphs, const BatchMaps* __restrict__ maps, const int* order, int count,
@@ -158,6 +189,8 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
       for (int t = 0; t < ntiles; t++) {
         const int m0 = (t % tiles_m) * kBM;
         const int n0 = (t / tiles_m) * kBN;
+        const bool half_rows = m0 + 64 >= n;               // uniform over the CTA
+        const bool idle_cols = n0 + 64 >= n && cbase == 64;  // uniform over the warp
         float acc[8][2 * WN];
 #pragma unroll
         for (int i = 0; i < 8; i++)
@@ -175,28 +208,12 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
           }
           const float* As = reinterpret_cast<const float*>(smem + s * kStageBytes);
           const float* Bs = reinterpret_cast<const float*>(smem + s * kStageBytes + kATileBytes);
-#pragma unroll 2
-          for (int q = 0; q < kBK / 4; q++) {
-            float4 a[8];
-#pragma unroll
-            for (int ii = 0; ii < 8; ii++)
-              a[ii] = *reinterpret_cast<const float4*>(As + (ty + 16 * ii) * kBK + ((q ^ swz) << 2));
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              float4 b[WN];
-#pragma unroll
-              for (int c = 0; c < WN; c++)
-                b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (cbase + 32 * c + 2 * tx) * 2);
-#pragma unroll
-              for (int ii = 0; ii < 8; ii++) {
-                const float2 ap = h == 0 ? make_float2(a[ii].x, a[ii].y) : make_float2(a[ii].z, a[ii].w);
-#pragma unroll
-                for (int c = 0; c < WN; c++) {
-                  acc[ii][2 * c] = Mac<OP>::mac2(acc[ii][2 * c], ap, make_float2(b[c].x, b[c].y));
-                  acc[ii][2 * c + 1] = Mac<OP>::mac2(acc[ii][2 * c + 1], ap, make_float2(b[c].z, b[c].w));
-                }
-              }
-            }
+          // Padding halves: rows past the graph are not computed (ROWS = 4), and
+          // the warps of the upper column half sit out a tile whose columns end
+          // by column 64 -- what they would compute is never stored.
+          if (!idle_cols) {
+            if (half_rows) batched_mac_ktile<OP, 4>(acc, As, Bs, ty, tx, cbase, swz);
+            else batched_mac_ktile<OP, 8>(acc, As, Bs, ty, tx, cbase, swz);
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
