@@ -676,6 +676,16 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
         }
+        mp = line["per_semiring_kernel_gops"].get("min_plus") if line.get("per_semiring_kernel_gops") else None
+        if mp:
+            # the reference's one recorded measurement of this path: the cuASR
+            # min_plus srgemm kernel at 4096^3, 27.32 ms on an RTX 3080-class
+            # Ampere board (2 * 4096^3 / 27.32 ms = 5031 Gop/s); another GPU, so
+            # this is context, not vs_baseline
+            line["published_comparison"] = {
+                "kernel": "min_plus srgemm 4096^3, kernel time", "published_gops": 2.0 * 4096 ** 3 / 27.32e-3 / 1e9,
+                "published_hw": "Ampere, RTX 3080 class, SM 1.44 GHz", "this_gops": mp,
+                "ratio": mp / (2.0 * 4096 ** 3 / 27.32e-3 / 1e9)}
         line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
