@@ -211,3 +211,29 @@ def test_selection_fp16_and_fp32_paths(cuda, op):
             got = run_gpu(op, x, y, c, epi, cuda)
             want = oracle.srgemm(op, x, y, c, do_epilogue=epi)
             np.testing.assert_array_equal(bits(got), bits(want), err_msg=f"{op} {name} epi={epi}")
+
+
+@pytest.mark.parametrize("op", ["plus_mul", "minus_square", "or_and"])
+@pytest.mark.parametrize("shape", [(1024, 1024, 2048), (4096, 4096, 256), (130, 300, 700)])
+def test_tensor_core_partial_rounds(cuda, op, shape):
+    """Shapes that leave the persistent tensor-core grid partly idle (fewer
+    tiles than SMs; a 68-tile last round of 4096 x 4096; ragged edges): the
+    oracle's result (or_and exactly) on rows sampled across the output."""
+    M, N, K = shape
+    a, b, c = datagen.semiring_operands(op, M, N, K, seed=M + K)
+    A, B, C = (torch.from_numpy(x).to(cuda) for x in (a, b, c))
+    got = s2.srgemm(op, A, B, C, do_epilogue=True).cpu().numpy()
+    rows = np.unique(np.linspace(0, M - 1, 40).astype(int))
+    if op == "or_and":
+        want = oracle.srgemm(op, a[rows], b, c[rows], do_epilogue=True)
+        assert np.array_equal(got[rows], want)
+        return
+    want = oracle.srgemm_f64(op, a[rows], b, c[rows], do_epilogue=True)
+    g = got[rows].astype(np.float64)
+    if op == "plus_mul":
+        S = np.abs(a[rows]).astype(np.float64) @ np.abs(b).astype(np.float64) + np.abs(c[rows])
+    else:
+        S = ((a[rows].astype(np.float64) ** 2).sum(1)[:, None] + (b.astype(np.float64) ** 2).sum(0)[None, :]) * 2 \
+            + np.abs(c[rows])
+    assert np.all(np.abs(g - want) <= (4 * 2.0 ** -16 + 2 * K * 2.0 ** -24) * S + 1e-6)
+    assert s2.device_status() == 0
