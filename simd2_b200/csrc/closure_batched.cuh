@@ -78,8 +78,8 @@ struct BatchMaps {
   CUtensorMap b[2];
 };
 
-// One k-tile of the 8 x 4 register tile; ROWS = 4 skips rows ty + 16i for
-// i >= 4 (tile rows 64..127), used when those rows lie past the graph.
+// One k-tile of the 8 x 4 register tile; ROWS < 8 skips rows ty + 16i for
+// i >= ROWS (tile rows 16 ROWS..127), used when those rows lie past the graph.
 template <int OP, int ROWS>
 __device__ __forceinline__ void batched_mac_ktile(float (&acc)[8][4], const float* As, const float* Bs, int ty,
                                                   int tx, int cbase, int swz) {
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
       for (int t = 0; t < ntiles; t++) {
         const int m0 = (t % tiles_m) * kBM;
         const int n0 = (t / tiles_m) * kBN;
-        const bool half_rows = m0 + 64 >= n;               // uniform over the CTA
+        const int row_groups = min(8, (n - m0 + 15) / 16);  // 16-row groups holding graph rows
         const bool idle_cols = n0 + 64 >= n && cbase == 64;  // uniform over the warp
         float acc[8][2 * WN];
 #pragma unroll
@@ -208,12 +208,20 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
           }
           const float* As = reinterpret_cast<const float*>(smem + s * kStageBytes);
           const float* Bs = reinterpret_cast<const float*>(smem + s * kStageBytes + kATileBytes);
-          // Padding halves: rows past the graph are not computed (ROWS = 4), and
+          // Padding: 16-row groups past the graph are not computed, and
           // the warps of the upper column half sit out a tile whose columns end
           // by column 64 -- what they would compute is never stored.
           if (!idle_cols) {
-            if (half_rows) batched_mac_ktile<OP, 4>(acc, As, Bs, ty, tx, cbase, swz);
-            else batched_mac_ktile<OP, 8>(acc, As, Bs, ty, tx, cbase, swz);
+            switch (row_groups) {
+              case 1: batched_mac_ktile<OP, 1>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 2: batched_mac_ktile<OP, 2>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 3: batched_mac_ktile<OP, 3>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 4: batched_mac_ktile<OP, 4>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 5: batched_mac_ktile<OP, 5>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 6: batched_mac_ktile<OP, 6>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 7: batched_mac_ktile<OP, 7>(acc, As, Bs, ty, tx, cbase, swz); break;
+              default: batched_mac_ktile<OP, 8>(acc, As, Bs, ty, tx, cbase, swz); break;
+            }
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
