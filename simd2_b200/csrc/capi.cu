@@ -921,7 +921,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
       if (cudaMemcpyAsync(hbuf, flag, sizeof(hbuf), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
         return SIMD2_ERR_CUDA;
     }
-    if (want_dec && step_feat) {
+    if (want_dec && (step_feat || dispatch == 2)) {
       if (cudaMemcpyAsync(hst, obase + occ.stats, sizeof(hst), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
         return SIMD2_ERR_CUDA;
     }
@@ -938,21 +938,33 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   int it = 0;
   int changed = 1;
   int cfg_id = default_cfg;
+  // Closure steps only fill X in: once every (tile, k-tile) block triple is
+  // occupied, no later step can skip anything, so the learned loop stops the
+  // occupancy pass and runs the dense configuration (feature recording keeps it).
+  const unsigned long long all_triples = (unsigned long long)occ.tiles_m * occ.tiles_n * occ.ktiles;
+  bool occ_on = need_occ;
+  auto settle = [&]() {
+    if (dispatch == 2 && !step_feat && hst[0] >= all_triples) {
+      occ_on = false;
+      cfg_id = default_cfg;
+    }
+  };
   if (need_occ) {
     if ((rc = enqueue_occ(cur, ldcur)) || (rc = read_back(false, true))) return rc;
     if (dispatch == 2) cfg_id = hbuf[8];  // decision[0]
     if (step_feat) mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst[0], hst[1], hst[2], sms, step_feat);
+    settle();
   }
   while (changed && it < max_iter) {
     SimtConfig cfg;
     cfg.split = config_split(cfg_id);
-    cfg.skip = config_skip(cfg_id) && can_skip && need_occ;
+    cfg.skip = config_skip(cfg_id) && can_skip && occ_on;
     if (cfg.skip) {
       cfg.occA = obase + occ.occA;
       cfg.occB = obase + occ.occB;
     }
     if (step_cfg) step_cfg[it] = (cfg.skip ? 4 : 0) | (cfg.split == 1 ? 0 : cfg.split == 2 ? 1 : cfg.split == 4 ? 2 : 3);
-    const float step_occ_ms = (need_occ && cfg.skip) ? occ_ms : 0.f;  // a skip step pays for its occupancy pass
+    const float step_occ_ms = (occ_on && cfg.skip) ? occ_ms : 0.f;  // a skip step pays for its occupancy pass
     if (cudaMemsetAsync(flag, 0, sizeof(int), stream) != cudaSuccess) {
       rc = SIMD2_ERR_CUDA;
       break;
@@ -965,7 +977,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     if (rc) break;
     if (step_ms) cudaEventRecord(ev[1], stream);
     it++;
-    const bool next = need_occ && it < max_iter;
+    const bool next = occ_on && it < max_iter;
     if (next && (rc = enqueue_occ(nxt, ldnxt))) break;
     float srg_ms = 0.f;
     if ((rc = read_back(true, next))) break;
@@ -979,6 +991,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
       if (step_feat && changed)
         mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst[0], hst[1], hst[2], sms,
                      step_feat + (size_t)it * kMlpFeat);
+      settle();
     }
     std::swap(cur, nxt);
     std::swap(ldcur, ldnxt);
