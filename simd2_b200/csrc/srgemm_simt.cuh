@@ -147,7 +147,6 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
   uint64_t* empty = full + STAGES;
   __shared__ uint16_t s_klist[SKIP ? kMaxSkipKtiles : 1];
   __shared__ int s_warp_cnt[kSimtWarps];
-  __shared__ int s_kcount;
 
   // Grouped raster: 8 consecutive tile rows share each B' column panel in L2.
   const int tile = blockIdx.x / SPLIT;
