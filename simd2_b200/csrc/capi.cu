@@ -19,6 +19,7 @@
 #include "prep.cuh"
 #include "srgemm_simt.cuh"
 #include "tc_gemm.cuh"
+#include "tc_gemm2.cuh"
 #include "closure_batched.cuh"
 #include "mlp.cuh"
 #include "knn.cuh"
@@ -518,6 +519,55 @@ int launch_tc(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1,
   return SIMD2_OK;
 }
 
+// Pair tiles (256 x 256) from which the SM-pair kernel is used: enough to
+// keep the pairs of the GPU busy; smaller problems run on single SMs.
+constexpr int kTc2MinTiles = 64;
+
+inline bool use_tc2(int M, int N) {
+  return (long long)((M + kTc2BM - 1) / kTc2BM) * ((N + kTcBN - 1) / kTcBN) >= kTc2MinTiles;
+}
+
+// SM-pair launch: clusters of 2 CTAs, one pair per pair of SMs at most.
+template <int KIND>
+int launch_tc2(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
+               const CUtensorMap& b1, const TcEpilogue& ep, cudaStream_t stream) {
+  auto kern = tc_gemm2_kernel<KIND>;
+  const size_t smem = tc2_smem_bytes<KIND>();
+  static int max_pairs[64] = {};
+  int dev = 0;
+  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
+  cudaLaunchConfig_t lc = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  lc.blockDim = dim3(kTcThreads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = stream;
+  if (!max_pairs[dev]) {
+    SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    lc.gridDim = dim3(2 * 74);
+    int clusters = 0;
+    SIMD2_CUDA_TRY(cudaOccupancyMaxActiveClusters(&clusters, kern, &lc));
+    max_pairs[dev] = std::max(1, clusters);
+  }
+  const int tiles_m = (M + kTc2BM - 1) / kTc2BM;
+  const int tiles_n = (N + kTcBN - 1) / kTcBN;
+  const int pairs = std::min(tiles_m * tiles_n, max_pairs[dev]);
+  lc.gridDim = dim3(2 * pairs);
+  auto* ev = prof_slot(2LL * M * N * K, kProfTensor);
+  if (ev) cudaEventRecord(ev->first, stream);
+  SIMD2_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, a0, a1, b0, b1, M, N, K, ep, tiles_m, tiles_n));
+  count_launch();
+  if (ev) cudaEventRecord(ev->second, stream);
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
 struct TcPlan {
   int Kp;
   size_t a0, a1, b0, b1, na, nb, nb64, total;
@@ -585,10 +635,13 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   const auto SW = tc_swizzle<0>();
   constexpr int BX = tc_box_k<0>();
   int rc;
+  // the SM-pair kernel stages B in halves of 128 rows
+  const bool pair = use_tc2(M, N);
+  const int brows = pair ? 128 : kTcBN;
   if ((rc = make_map_2d(&ma0, BF, 2, ahi, M, Kp, Kp, BX, kTcBM, SW))) return rc;
   if ((rc = make_map_2d(&ma1, BF, 2, alo, M, Kp, Kp, BX, kTcBM, SW))) return rc;
-  if ((rc = make_map_2d(&mb0, BF, 2, ws + plan.b0, N, Kp, Kp, BX, kTcBN, SW))) return rc;
-  if ((rc = make_map_2d(&mb1, BF, 2, ws + plan.b1, N, Kp, Kp, BX, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&mb0, BF, 2, ws + plan.b0, N, Kp, Kp, BX, brows, SW))) return rc;
+  if ((rc = make_map_2d(&mb1, BF, 2, ws + plan.b1, N, Kp, Kp, BX, brows, SW))) return rc;
   TcEpilogue ep{};
   ep.op = op;
   ep.do_epilogue = do_epilogue;
@@ -604,6 +657,7 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   ep.ldb32 = ldb;
   ep.K = K;
   ep.band = kMinusSquareBand;
+  if (pair) return launch_tc2<0>(M, N, K, ma0, ma1, mb0, mb1, ep, stream);
   return launch_tc<0>(M, N, K, ma0, ma1, mb0, mb1, ep, stream);
 }
 
@@ -624,8 +678,9 @@ int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, 
   const auto U8 = CU_TENSOR_MAP_DATA_TYPE_UINT8;
   const auto SW = CU_TENSOR_MAP_SWIZZLE_128B;
   int rc;
+  const bool pair = use_tc2(M, N);
   if ((rc = make_map_2d(&ma, U8, 1, a8, M, Kp, Kp, 128, kTcBM, SW))) return rc;
-  if ((rc = make_map_2d(&mb, U8, 1, b8, N, Kp, Kp, 128, kTcBN, SW))) return rc;
+  if ((rc = make_map_2d(&mb, U8, 1, b8, N, Kp, Kp, 128, pair ? 128 : kTcBN, SW))) return rc;
   TcEpilogue ep{};
   ep.op = SIMD2_OR_AND;
   ep.do_epilogue = do_epilogue;
@@ -635,6 +690,7 @@ int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, 
   ep.ldd = ldd;
   ep.out_u8 = sizeof(T) == 1;
   ep.changed = changed;
+  if (pair) return launch_tc2<1>(M, N, K, ma, ma, mb, mb, ep, stream);
   return launch_tc<1>(M, N, K, ma, ma, mb, mb, ep, stream);
 }
 

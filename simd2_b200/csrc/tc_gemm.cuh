@@ -176,6 +176,159 @@ __device__ __forceinline__ float exact_minus_square(const float* a, const float*
   return s;
 }
 
+// Epilogue of one 128 x 256 tile for the 32 rows of one warp: lane l holds
+// row row0 + l of the accumulator in TMEM at trow (lane quadrant and column
+// base included).  Sets changed when an or_and output differs from C.
+template <int KIND>
+__device__ __forceinline__ void tc_tile_epilogue(const TcEpilogue& ep, int M, int N, int n0, int row0, uint32_t trow,
+                                                 uint32_t* epi_tile, int lane, int& changed) {
+  if constexpr (KIND == 1) {
+    // or_and: 32 flags of one row are 32 contiguous bytes (u8) or 128 bytes
+    // (i32), so each lane writes its own row with 16-byte vector stores.
+    const int row = row0 + lane;
+    const bool u8 = ep.out_u8 != 0;
+    const int esz = u8 ? 1 : 4;
+    const bool vec_ok = ((ep.ldd * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.D) & 15) == 0) &&
+                        (!ep.do_epilogue ||
+                         (((ep.ldc * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.C) & 15) == 0)));
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+      uint32_t r[32];
+      tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
+      if (row >= M) continue;
+      const int colb = n0 + c0;
+      if (u8) {
+        const uint8_t* crow = static_cast<const uint8_t*>(ep.C) + (long long)row * ep.ldc;
+        uint8_t* drow = static_cast<uint8_t*>(ep.D) + (long long)row * ep.ldd;
+        if (vec_ok && colb + 32 <= N) {
+          uint32_t w[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++)
+            w[q] = (r[4 * q] != 0u) | ((r[4 * q + 1] != 0u) << 8) | ((r[4 * q + 2] != 0u) << 16) |
+                   ((uint32_t)(r[4 * q + 3] != 0u) << 24);
+          if (ep.do_epilogue) {
+            const uint4 c0v = *reinterpret_cast<const uint4*>(crow + colb);
+            const uint4 c1v = *reinterpret_cast<const uint4*>(crow + colb + 16);
+            const uint32_t cw[8] = {c0v.x, c0v.y, c0v.z, c0v.w, c1v.x, c1v.y, c1v.z, c1v.w};
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+              // normalise C's bytes to 0/1 before the OR
+              uint32_t cb = cw[q];
+              cb = ((cb & 0x7f7f7f7fu) + 0x7f7f7f7fu | cb) & 0x80808080u;
+              cb >>= 7;
+              const uint32_t v = w[q] | cb;
+              if (ep.changed && v != cb) changed = 1;
+              w[q] = v;
+            }
+          }
+          *reinterpret_cast<uint4*>(drow + colb) = make_uint4(w[0], w[1], w[2], w[3]);
+          *reinterpret_cast<uint4*>(drow + colb + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int col = colb + j;
+            if (col < N) {
+              uint8_t v = r[j] != 0u;
+              if (ep.do_epilogue) {
+                const uint8_t cv = crow[col] != 0;
+                v |= cv;
+                if (ep.changed && v != cv) changed = 1;
+              }
+              drow[col] = v;
+            }
+          }
+        }
+      } else {
+        const int32_t* crow = static_cast<const int32_t*>(ep.C) + (long long)row * ep.ldc;
+        int32_t* drow = static_cast<int32_t*>(ep.D) + (long long)row * ep.ldd;
+        if (vec_ok && colb + 32 <= N) {
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            int4 v = make_int4(r[4 * q] != 0u, r[4 * q + 1] != 0u, r[4 * q + 2] != 0u, r[4 * q + 3] != 0u);
+            if (ep.do_epilogue) {
+              const int4 c = *reinterpret_cast<const int4*>(crow + colb + 4 * q);
+              v.x |= c.x != 0;
+              v.y |= c.y != 0;
+              v.z |= c.z != 0;
+              v.w |= c.w != 0;
+            }
+            *reinterpret_cast<int4*>(drow + colb + 4 * q) = v;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int col = colb + j;
+            if (col < N) {
+              int32_t v = r[j] != 0u;
+              if (ep.do_epilogue) v |= (crow[col] != 0);
+              drow[col] = v;
+            }
+          }
+        }
+      }
+    }
+  } else {
+    // Sums: a 32 x 32 chunk is transposed through shared memory (the stage
+    // ring is idle now) and written row by row: lane l handles column l, so
+    // every store instruction covers 32 consecutive floats of one row.  The
+    // chunk's C values (one column per lane, 32 independent loads) and the
+    // warp's 32 row norms are fetched before the TMEM read, so their latency
+    // overlaps it instead of being paid row by row.
+    uint32_t* tile = epi_tile;
+    const bool msq = ep.op == SIMD2_MINUS_SQUARE;
+    const float na_lane = (msq && row0 + lane < M) ? ep.norm_a[row0 + lane] : 0.f;
+    const int rows_here = min(32, M - row0);
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+      const int col = n0 + c0 + lane;
+      const bool col_ok = col < N;
+      float cv[32];
+      if (ep.do_epilogue) {
+        const float* Cc = static_cast<const float*>(ep.C) + col;
+#pragma unroll
+        for (int rr = 0; rr < 32; rr++)
+          cv[rr] = (col_ok && rr < rows_here) ? Cc[(long long)(row0 + rr) * ep.ldc] : 0.f;
+      }
+      const float nb = (msq && col_ok) ? ep.norm_b[col] : 0.f;
+      uint32_t r[32];
+      tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
+#pragma unroll
+      for (int j = 0; j < 32; j++) tile[lane * 33 + j] = r[j];
+      __syncwarp();
+      if (msq) {
+        // distances in place; rows inside the cancellation band are
+        // recomputed exactly in a separate, rarely taken loop (one copy of
+        // the recompute code)
+        uint32_t band = 0;
+#pragma unroll
+        for (int rr = 0; rr < 32; rr++) {
+          const float nsum = __shfl_sync(0xffffffffu, na_lane, rr) + nb;
+          const float v = __fmaf_rn(-2.0f, __uint_as_float(tile[rr * 33 + lane]), nsum);
+          tile[rr * 33 + lane] = __float_as_uint(v);
+          band |= (v < ep.band * nsum && rr < rows_here && col_ok ? 1u : 0u) << rr;
+        }
+        while (band) {
+          const int rr = __ffs(band) - 1;
+          band &= band - 1;
+          tile[rr * 33 + lane] = __float_as_uint(exact_minus_square(
+              ep.A32 + (long long)(row0 + rr) * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows));
+        }
+      }
+      if (col_ok) {
+        float* Dc = static_cast<float*>(ep.D) + col;
+#pragma unroll
+        for (int rr = 0; rr < 32; rr++) {
+          if (rr < rows_here) {
+            float v = __uint_as_float(tile[rr * 33 + lane]);
+            if (ep.do_epilogue) v = __fadd_rn(v, cv[rr]);
+            Dc[(long long)(row0 + rr) * ep.ldd] = v;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
 template <int KIND>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1,
@@ -329,155 +482,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint32_t trow = tmem + acc * kTcBN + ((uint32_t)(quad * 32) << 16);
       const int row0 = m0 + quad * 32;
       int changed = 0;
-      if (ok) {
-        if constexpr (KIND == 1) {
-          // or_and: 32 flags of one row are 32 contiguous bytes (u8) or 128 bytes
-          // (i32), so each lane writes its own row with 16-byte vector stores.
-          const int row = row0 + lane;
-          const bool u8 = ep.out_u8 != 0;
-          const int esz = u8 ? 1 : 4;
-          const bool vec_ok = ((ep.ldd * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.D) & 15) == 0) &&
-                              (!ep.do_epilogue ||
-                               (((ep.ldc * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.C) & 15) == 0)));
-    #pragma unroll 1
-          for (int c0 = 0; c0 < kTcBN; c0 += 32) {
-            uint32_t r[32];
-            tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
-            if (row >= M) continue;
-            const int colb = n0 + c0;
-            if (u8) {
-              const uint8_t* crow = static_cast<const uint8_t*>(ep.C) + (long long)row * ep.ldc;
-              uint8_t* drow = static_cast<uint8_t*>(ep.D) + (long long)row * ep.ldd;
-              if (vec_ok && colb + 32 <= N) {
-                uint32_t w[8];
-    #pragma unroll
-                for (int q = 0; q < 8; q++)
-                  w[q] = (r[4 * q] != 0u) | ((r[4 * q + 1] != 0u) << 8) | ((r[4 * q + 2] != 0u) << 16) |
-                         ((uint32_t)(r[4 * q + 3] != 0u) << 24);
-                if (ep.do_epilogue) {
-                  const uint4 c0v = *reinterpret_cast<const uint4*>(crow + colb);
-                  const uint4 c1v = *reinterpret_cast<const uint4*>(crow + colb + 16);
-                  const uint32_t cw[8] = {c0v.x, c0v.y, c0v.z, c0v.w, c1v.x, c1v.y, c1v.z, c1v.w};
-    #pragma unroll
-                  for (int q = 0; q < 8; q++) {
-                    // normalise C's bytes to 0/1 before the OR
-                    uint32_t cb = cw[q];
-                    cb = ((cb & 0x7f7f7f7fu) + 0x7f7f7f7fu | cb) & 0x80808080u;
-                    cb >>= 7;
-                    const uint32_t v = w[q] | cb;
-                    if (ep.changed && v != cb) changed = 1;
-                    w[q] = v;
-                  }
-                }
-                *reinterpret_cast<uint4*>(drow + colb) = make_uint4(w[0], w[1], w[2], w[3]);
-                *reinterpret_cast<uint4*>(drow + colb + 16) = make_uint4(w[4], w[5], w[6], w[7]);
-              } else {
-    #pragma unroll
-                for (int j = 0; j < 32; j++) {
-                  const int col = colb + j;
-                  if (col < N) {
-                    uint8_t v = r[j] != 0u;
-                    if (ep.do_epilogue) {
-                      const uint8_t cv = crow[col] != 0;
-                      v |= cv;
-                      if (ep.changed && v != cv) changed = 1;
-                    }
-                    drow[col] = v;
-                  }
-                }
-              }
-            } else {
-              const int32_t* crow = static_cast<const int32_t*>(ep.C) + (long long)row * ep.ldc;
-              int32_t* drow = static_cast<int32_t*>(ep.D) + (long long)row * ep.ldd;
-              if (vec_ok && colb + 32 <= N) {
-    #pragma unroll
-                for (int q = 0; q < 8; q++) {
-                  int4 v = make_int4(r[4 * q] != 0u, r[4 * q + 1] != 0u, r[4 * q + 2] != 0u, r[4 * q + 3] != 0u);
-                  if (ep.do_epilogue) {
-                    const int4 c = *reinterpret_cast<const int4*>(crow + colb + 4 * q);
-                    v.x |= c.x != 0;
-                    v.y |= c.y != 0;
-                    v.z |= c.z != 0;
-                    v.w |= c.w != 0;
-                  }
-                  *reinterpret_cast<int4*>(drow + colb + 4 * q) = v;
-                }
-              } else {
-    #pragma unroll
-                for (int j = 0; j < 32; j++) {
-                  const int col = colb + j;
-                  if (col < N) {
-                    int32_t v = r[j] != 0u;
-                    if (ep.do_epilogue) v |= (crow[col] != 0);
-                    drow[col] = v;
-                  }
-                }
-              }
-            }
-          }
-        } else {
-          // Sums: a 32 x 32 chunk is transposed through shared memory (the stage
-          // ring is idle now) and written row by row: lane l handles column l, so
-          // every store instruction covers 32 consecutive floats of one row.  The
-          // chunk's C values (one column per lane, 32 independent loads) and the
-          // warp's 32 row norms are fetched before the TMEM read, so their latency
-          // overlaps it instead of being paid row by row.
-          uint32_t* tile = epi_tile;
-          const bool msq = ep.op == SIMD2_MINUS_SQUARE;
-          const float na_lane = (msq && row0 + lane < M) ? ep.norm_a[row0 + lane] : 0.f;
-          const int rows_here = min(32, M - row0);
-    #pragma unroll 1
-          for (int c0 = 0; c0 < kTcBN; c0 += 32) {
-            const int col = n0 + c0 + lane;
-            const bool col_ok = col < N;
-            float cv[32];
-            if (ep.do_epilogue) {
-              const float* Cc = static_cast<const float*>(ep.C) + col;
-    #pragma unroll
-              for (int rr = 0; rr < 32; rr++)
-                cv[rr] = (col_ok && rr < rows_here) ? Cc[(long long)(row0 + rr) * ep.ldc] : 0.f;
-            }
-            const float nb = (msq && col_ok) ? ep.norm_b[col] : 0.f;
-            uint32_t r[32];
-            tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
-    #pragma unroll
-            for (int j = 0; j < 32; j++) tile[lane * 33 + j] = r[j];
-            __syncwarp();
-            if (msq) {
-              // distances in place; rows inside the cancellation band are
-              // recomputed exactly in a separate, rarely taken loop (one copy of
-              // the recompute code)
-              uint32_t band = 0;
-    #pragma unroll
-              for (int rr = 0; rr < 32; rr++) {
-                const float nsum = __shfl_sync(0xffffffffu, na_lane, rr) + nb;
-                const float v = __fmaf_rn(-2.0f, __uint_as_float(tile[rr * 33 + lane]), nsum);
-                tile[rr * 33 + lane] = __float_as_uint(v);
-                band |= (v < ep.band * nsum && rr < rows_here && col_ok ? 1u : 0u) << rr;
-              }
-              while (band) {
-                const int rr = __ffs(band) - 1;
-                band &= band - 1;
-                tile[rr * 33 + lane] = __float_as_uint(exact_minus_square(
-                    ep.A32 + (long long)(row0 + rr) * ep.lda32, ep.B32, ep.ldb32, col, ep.K, ep.b_rows));
-              }
-            }
-            if (col_ok) {
-              float* Dc = static_cast<float*>(ep.D) + col;
-    #pragma unroll
-              for (int rr = 0; rr < 32; rr++) {
-                if (rr < rows_here) {
-                  float v = __uint_as_float(tile[rr * 33 + lane]);
-                  if (ep.do_epilogue) v = __fadd_rn(v, cv[rr]);
-                  Dc[(long long)(row0 + rr) * ep.ldd] = v;
-                }
-              }
-            }
-            __syncwarp();
-          }
-        }
-      }
-
+      tc_tile_epilogue<KIND>(ep, M, N, n0, row0, trow, epi_tile, lane, changed);
       if (ep.changed && KIND == 1) {
         if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
       }
