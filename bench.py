@@ -664,12 +664,12 @@ def main():
                                         "2 ops per (x),(+) pair = 2 lane-instructions",
                          "share_of_kernel_time": simt_ms / (simt_ms + tc_ms) if simt_ms + tc_ms > 0 else None,
                          "timed_launches": simt_n},
-            "roofline_tensor": {"bound": "tensor", "kernel": "tc_gemm_kernel (plus_mul, minus_square, or_and)",
+            "roofline_tensor": {"bound": "tensor", "kernel": "tc_gemm2_kernel on SM pairs (plus_mul, minus_square, or_and)",
                                 "achieved": tc_equiv / (tc_ms / 1e3) / 1e12 if tc_ms > 0 else None,
                                 "peak": bf16_peak, "unit": "TFLOP/s (BF16-equivalent)",
                                 "frac": (tc_equiv / (tc_ms / 1e3) / 1e12) / bf16_peak if tc_ms > 0 else None,
                                 "peak_source": f"{peak_kind} bf16_tflops (cuBLAS burst)", "timed_launches": tc_n,
-                                "traffic": traffic_from_profile("tc_gemm_kernel_plus_mul_4096.md"),
+                                "traffic": traffic_from_profile("tc_gemm2_kernel_plus_mul_4096.md"),
                                 "traffic_of": "one plus_mul 4096^3 launch with C (ncu dram read + write)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
