@@ -280,44 +280,50 @@ __global__ void __launch_bounds__(kKfThreads, 1)
       float lim = fmaxf(thr, blim);
       const uint32_t taddr = tmem + acc * kKfBN + half * 128 + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
-      for (int c = 0; c < 4; c++) {
-        uint32_t r[32];
-        tmem_ld32(taddr + c * 32, r);
-        if (c == 3) {
+      for (int c2 = 0; c2 < 2; c2++) {
+        // 64 columns per TMEM round trip (tcgen05.ld .x64, one wait)
+        uint32_t r64[64];
+        tmem_ld64(taddr + c2 * 64, r64);
+        if (c2 == 1) {
           // the accumulator is in registers: hand it back to the MMA warp
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&acc_empty[acc]);
         }
-        // Hot pass: the distance of each of the 32 columns and a bit per
-        // column that may enter the list.  The insertion code exists once,
-        // below, so the loop body stays small enough for the instruction cache.
-        const float4* nb4 = reinterpret_cast<const float4*>(a.norm_r + cbase + c * 32);
-        uint32_t mask = 0;
 #pragma unroll
-        for (int q4 = 0; q4 < 8; q4++) {
-          const float4 nb = __ldg(nb4 + q4);
-          const float nbv[4] = {nb.x, nb.y, nb.z, nb.w};
+        for (int h = 0; h < 2; h++) {
+          const int c = 2 * c2 + h;
+          uint32_t(&r)[32] = *reinterpret_cast<uint32_t(*)[32]>(r64 + 32 * h);
+          // Hot pass: the distance of each of the 32 columns and a bit per
+          // column that may enter the list.  The insertion code exists once per
+          // half, below, so the loop body stays small for the instruction cache.
+          const float4* nb4 = reinterpret_cast<const float4*>(a.norm_r + cbase + c * 32);
+          uint32_t mask = 0;
 #pragma unroll
-          for (int e = 0; e < 4; e++) {
-            const int jj = q4 * 4 + e;
-            const float v = __fmaf_rn(-2.0f, __uint_as_float(r[jj]), na + nbv[e]);
-            r[jj] = __float_as_uint(v);
-            mask |= (v < lim ? 1u : 0u) << jj;
+          for (int q4 = 0; q4 < 8; q4++) {
+            const float4 nb = __ldg(nb4 + q4);
+            const float nbv[4] = {nb.x, nb.y, nb.z, nb.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const int jj = q4 * 4 + e;
+              const float v = __fmaf_rn(-2.0f, __uint_as_float(r[jj]), na + nbv[e]);
+              r[jj] = __float_as_uint(v);
+              mask |= (v < lim ? 1u : 0u) << jj;
+            }
           }
-        }
-        // Rare pass, in increasing column order.
-        while (mask) {
-          const int j = __ffs(mask) - 1;
-          mask &= mask - 1;
-          const int col = cbase + c * 32 + j;
-          float v = __uint_as_float(pick32(r, j));
-          const float nsum = na + a.norm_r[col];
-          if (v < a.band * nsum) v = exact_minus_square(qrow, a.r32, a.ldr, col, a.D, 1);
-          if (v < thr) {
-            topk_insert<K>(bd, bi, v, col);
-            thr = fminf(bd[K - 1], prior);
-            lim = fmaxf(thr, blim);
+          // Rare pass, in increasing column order.
+          while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int col = cbase + c * 32 + j;
+            float v = __uint_as_float(pick32(r, j));
+            const float nsum = na + a.norm_r[col];
+            if (v < a.band * nsum) v = exact_minus_square(qrow, a.r32, a.ldr, col, a.D, 1);
+            if (v < thr) {
+              topk_insert<K>(bd, bi, v, col);
+              thr = fminf(bd[K - 1], prior);
+              lim = fmaxf(thr, blim);
+            }
           }
         }
       }
