@@ -162,7 +162,10 @@ typedef enum simd2_dispatch {
  * simd2_mlp_param_count() floats (LEARNED only).  Optional host outputs of
  * max_iter entries: step_configs (config run per step), step_ms (device time
  * of each step), step_features (7 floats per step: the cost-model features).
- * Results are bit-identical for every policy. */
+ * Results are bit-identical for every policy.  LEARNED decides per step only
+ * for n > 1024: a decision (occupancy pass, MLP launch, host round trip) costs
+ * about as much as a whole dense step below that, so smaller closures run the
+ * DENSE path (step_features then stay zero). */
 int simd2_closure_ex(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_conv conv,
                      simd2_dispatch dispatch, int fixed_config, const float* mlp_params,
                      int* iters_out, int* step_configs, float* step_ms, float* step_features,

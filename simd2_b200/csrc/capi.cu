@@ -924,6 +924,15 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     SIMD2_CUDA_TRY(cudaGetDevice(&dev));
     SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   }
+  // A learned step costs an occupancy pass, the MLP launch and a host round
+  // trip (about 25 us together on B200).  Up to n = kLearnedMinN a whole dense
+  // step costs about as much (2n^3 <= 2.1 Gop, under 70 us on 148 SMs), so no
+  // choice can win back its decision and the plain gated path runs instead.
+  if (dispatch == 2 && n <= kLearnedMinN) {
+    dispatch = 0;
+    if (step_feat) std::fill(step_feat, step_feat + (size_t)max_iter * kMlpFeat, 0.f);
+    step_feat = nullptr;
+  }
   const bool can_skip = skip_supported(op) && (n + kBK - 1) / kBK <= kMaxSkipKtiles;
   const bool need_occ = dispatch == 2 || step_feat != nullptr || (dispatch == 1 && config_skip(fixed_cfg) && can_skip);
   // Workspace: [srgemm plan][Xnew n x n][flag + decision][occupancy]
@@ -1256,28 +1265,70 @@ int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ld
     SIMD2_CUDA_TRY(cudaGetLastError());
   }
   if (max_iter == 0) return SIMD2_OK;
-  // Workspace: [X' n x n][P' n x n][change flag]
+  // Workspace: [X' n x n][P' n x n][X^T n x n][B' Kp/2 x 2Np][packed A n x Kp][change flag]
   const size_t nn = (size_t)n * n;
-  const size_t x_off = 0, p_off = align_up(nn * 4, kAlign), f_off = p_off + align_up(nn * 4, kAlign);
+  const int Kp = round_up(n, kBK), Np = round_up(n, kBN);
+  const size_t x_off = 0, p_off = align_up(nn * 4, kAlign), t_off = p_off + align_up(nn * 4, kAlign);
+  const size_t b_off = t_off + align_up(nn * 4, kAlign);
+  const size_t a_off = b_off + align_up((size_t)Kp * Np * 4, kAlign);
+  const size_t f_off = a_off + align_up((size_t)n * Kp * 4, kAlign);
   void* w = nullptr;
   if ((rc = get_workspace(stream, f_off + kAlign, &w))) return rc;
   uint8_t* ws = static_cast<uint8_t*>(w);
   float* bufx[2] = {X, reinterpret_cast<float*>(ws + x_off)};
   int32_t* bufp[2] = {P, reinterpret_cast<int32_t*>(ws + p_off)};
   long long ldx_[2] = {ldx, n}, ldp_[2] = {ldp, n};
+  float* XT = reinterpret_cast<float*>(ws + t_off);
+  float* Bp = reinterpret_cast<float*>(ws + b_off);
+  float* Ap = reinterpret_cast<float*>(ws + a_off);
   int* flag = reinterpret_cast<int*>(ws + f_off);
-  const dim3 grid((n + kPredBN - 1) / kPredBN, (n + kPredBM - 1) / kPredBM);
+  const int tiles = (n + kBM - 1) / kBM;
+  const size_t smem = pred_smem_bytes();
+  const float pad = pad_value(op);
   int cur = 0, it = 0, changed = 1;
   while (changed && it < max_iter) {
     it++;
     SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), stream));
     const int nx = cur ^ 1;
+    float* Xc = bufx[cur];
+    const long long ldc = ldx_[cur];
+    // operands of the step: X^T for the witness search, B' = X with k pairs
+    // interleaved, and A = X itself when its rows suit TMA (else a packed copy)
+    transpose_f32_kernel<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, stream>>>(n, Xc, ldc, XT, n);
+    count_launch();
+    interleave_pairs_kernel<float, 0><<<grid_for((long long)Kp / 2 * Np / 2), 256, 0, stream>>>(Xc, ldc, n, n, Bp, Kp,
+                                                                                               Np, pad);
+    count_launch();
+    const bool pack_a = !a_tma_ok(Xc, ldc) || (n % 4 != 0);
+    const float* a_base = Xc;
+    long long a_pitch = ldc;
+    if (pack_a) {
+      pack_rows_kernel<float, 0><<<grid_for((long long)n * Kp), 256, 0, stream>>>(Xc, ldc, n, n, Ap, Kp, pad);
+      count_launch();
+      a_base = Ap;
+      a_pitch = Kp;
+    }
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    CUtensorMap mA, mB;
+    if ((rc = make_map_f32(&mA, a_base, n, pack_a ? Kp : n, a_pitch, kBK, kBM, CU_TENSOR_MAP_SWIZZLE_128B, true)))
+      return rc;
+    if ((rc = make_map_f32(&mB, Bp, Kp / 2, 2LL * Np, 2LL * Np, 2 * kBN, kBK / 2, CU_TENSOR_MAP_SWIZZLE_NONE, false)))
+      return rc;
     switch (op) {
 #define SIMD2_PRED_CASE(OPV)                                                                                         \
-  case OPV:                                                                                                           \
-    pred_step_kernel<OPV><<<grid, 256, 0, stream>>>(n, bufx[cur], ldx_[cur], bufp[cur], ldp_[cur], bufx[nx],       \
-                                                    ldx_[nx], bufp[nx], ldp_[nx], flag);                             \
-    break;
+  case OPV: {                                                                                                         \
+    static bool configured[64] = {};                                                                                  \
+    int dev = 0;                                                                                                      \
+    SIMD2_CUDA_TRY(cudaGetDevice(&dev));                                                                              \
+    if (dev >= 0 && dev < 64 && !configured[dev]) {                                                                   \
+      SIMD2_CUDA_TRY(cudaFuncSetAttribute(pred_fast_kernel<OPV>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                          (int)smem));                                                                \
+      configured[dev] = true;                                                                                         \
+    }                                                                                                                 \
+    pred_fast_kernel<OPV><<<tiles * tiles, kSimtThreads, smem, stream>>>(                                             \
+        mA, mB, n, Xc, ldc, XT, n, bufp[cur], ldp_[cur], bufx[nx], ldx_[nx], bufp[nx], ldp_[nx], flag, tiles, tiles); \
+    break;                                                                                                            \
+  }
       SIMD2_PRED_CASE(SIMD2_MIN_PLUS)
       SIMD2_PRED_CASE(SIMD2_MAX_PLUS)
       SIMD2_PRED_CASE(SIMD2_MAX_MIN)

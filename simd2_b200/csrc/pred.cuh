@@ -15,16 +15,21 @@
 //   P'[i][j] = best strictly better than X[i][j] ? P[k*][j] : P[i][j]
 // since j's predecessor on the path i -> k* -> j is its predecessor on k* -> j.
 //
-// The step kernel is a plain shared-memory tiled kernel (64 x 64 outputs per
-// 256-thread block, 4 x 4 per thread, K tiles of 16): the witness doubles the
-// accumulator state and adds a select per product, so this path is opt-in
-// and separate from the packed closure kernels.
+// pred_fast_kernel finds k* without a compare per product.  It runs the
+// packed main loop of the CUDA-core srgemm tile (TMA-staged A and k-pair
+// interleaved B', one (x),(+) pair per lane per cycle) into a per-k-tile
+// minimum t, and after each k-tile of 32 keeps, per output, best and the index
+// of the last k-tile where t was strictly better than best.  That k-tile holds
+// k*: every earlier k-tile's products are worse than best (strict record), and
+// no later one is better.  The epilogue re-forms the 32 products of that
+// k-tile for each output whose value improves (X[i][k] from the row, X[k][j]
+// from a transposed copy, both contiguous) and takes the first one equal to
+// best -- the same IEEE operation on the same operands, so the same bits.
 #pragma once
 #include "common.cuh"
+#include "srgemm_simt.cuh"
 
 namespace simd2 {
-
-constexpr int kPredBM = 64, kPredBN = 64, kPredBK = 16;
 
 template <int OP>
 struct PredOps;
@@ -68,83 +73,205 @@ struct PredOps<SIMD2_MIN_MAX> {
   static constexpr bool kMin = true;
 };
 
-// One predecessor-tracking squaring step: X, P (pitch ldx, ldp) -> Xn, Pn
-// (pitch ldxn, ldpn).  *changed |= 1 when any X' element differs bitwise from X.
+// Row stride (uint16 entries) of the per-output k-tile record in shared
+// memory; 160 puts the two half-warps' rows on different banks.
+constexpr int kPredRecStride = 160;
+constexpr int kPredStages = 4;
+
+constexpr size_t pred_smem_bytes() {
+  return simt_smem_bytes(kPredStages) + (size_t)kBM * kPredRecStride * sizeof(uint16_t);
+}
+
+// One predecessor-tracking squaring step on a 128 x 128 output tile per CTA:
+// X, P (pitch ldx, ldp) -> Xn, Pn (pitch ldxn, ldpn).  tmA reads X in k-tiles
+// (NaN beyond n), tmB the k-pair interleaved copy of X, XT is X transposed
+// (pitch ldt).  *changed |= 1 when any X' element differs bitwise from X.
 template <int OP>
-__global__ void __launch_bounds__(256)
-    pred_step_kernel(int n, const float* __restrict__ X, long long ldx, const int32_t* __restrict__ P,
-                     long long ldp, float* __restrict__ Xn, long long ldxn, int32_t* __restrict__ Pn,
-                     long long ldpn, int* __restrict__ changed) {
+__global__ void __launch_bounds__(kSimtThreads, 1)
+    pred_fast_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int n,
+                     const float* __restrict__ X, long long ldx, const float* __restrict__ XT, long long ldt,
+                     const int32_t* __restrict__ P, long long ldp, float* __restrict__ Xn, long long ldxn,
+                     int32_t* __restrict__ Pn, long long ldpn, int* __restrict__ changed, int tiles_m,
+                     int tiles_n) {
   using O = PredOps<OP>;
-  __shared__ float As[kPredBM][kPredBK + 1];
-  __shared__ float Bs[kPredBK][kPredBN];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int i0 = blockIdx.y * kPredBM, j0 = blockIdx.x * kPredBN;
-  const float ident = O::kMin ? __int_as_float(0x7f800000) : __int_as_float(0xff800000);
-  float best[4][4];
-  int kb[4][4];
-#pragma unroll
-  for (int r = 0; r < 4; r++)
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      best[r][c] = ident;
-      kb[r][c] = -1;
+  constexpr int STAGES = kPredStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
+  uint64_t* empty = full + STAGES;
+  uint16_t* rec = reinterpret_cast<uint16_t*>(empty + STAGES);
+
+  // grouped raster: 8 consecutive tile rows share each B' column panel in L2
+  const int tile = blockIdx.x;
+  const int per_group = 8 * tiles_n;
+  const int g = tile / per_group;
+  const int first_m = g * 8;
+  const int gsize = min(tiles_m - first_m, 8);
+  const int local = tile - g * per_group;
+  const int m0 = (first_m + local % gsize) * kBM;
+  const int n0 = (local / gsize) * kBN;
+  const int ktiles = (n + kBK - 1) / kBK;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kSimtWarps);
     }
-  for (int k0 = 0; k0 < n; k0 += kPredBK) {
-    // A tile: rows i0..i0+63, columns k0..k0+15; B tile: rows k0..k0+15, columns j0..j0+63
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const int t = threadIdx.x + 256 * e;
-      const int ar = t >> 4, ac = t & 15;
-      const int gi = i0 + ar, gk = k0 + ac;
-      As[ar][ac] = (gi < n && gk < n) ? X[(long long)gi * ldx + gk] : 0.f;
-      const int br = t >> 6, bc = t & 63;
-      const int gk2 = k0 + br, gj = j0 + bc;
-      Bs[br][bc] = (gk2 < n && gj < n) ? X[(long long)gk2 * ldx + gj] : 0.f;
-    }
-    __syncthreads();
-    const int kmax = min(kPredBK, n - k0);
-    for (int kk = 0; kk < kmax; kk++) {
-      float a[4], b[4];
-#pragma unroll
-      for (int r = 0; r < 4; r++) a[r] = As[ty + 16 * r][kk];
-#pragma unroll
-      for (int c = 0; c < 4; c++) b[c] = Bs[kk][tx + 16 * c];
-#pragma unroll
-      for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-          const float p = O::mul(a[r], b[c]);
-          if (O::better(p, best[r][c])) {
-            best[r][c] = p;
-            kb[r][c] = k0 + kk;
-          }
-        }
-    }
-    __syncthreads();
+    fence_mbar_init();
   }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    prefetch_tensormap(&tmA);
+    prefetch_tensormap(&tmB);
+    for (int i = 0; i < min(STAGES, ktiles); i++) {
+      uint8_t* sa = smem + i * kStageBytes;
+      mbar_arrive_expect_tx(&full[i], kStageBytes);
+      tma_load_2d(sa, &tmA, &full[i], i * kBK, m0);
+      tma_load_2d(sa + kATileBytes, &tmB, &full[i], 2 * n0, i * (kBK / 2));
+    }
+  }
+
+  const int tx = lane & 15;
+  const int ty = (warp & 7) * 2 + (lane >> 4);
+  const int cbase = (warp >> 3) * 64;
+  const int swz = ty & 7;
+  const float ident = Mac<OP>::identity();
+  float best[8][4], t[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) best[i][j] = ident;
+
+  bool ok = true;
+  int issued = min(STAGES, ktiles);
+  for (int kt = 0; kt < ktiles; kt++) {
+    const int s = kt % STAGES;
+    if (threadIdx.x == 0 && kt >= 1 && kt - 1 + STAGES < ktiles) {
+      const int r = kt - 1, rs = r % STAGES;
+      if (mbar_wait(&empty[rs], (r / STAGES) & 1)) {
+        uint8_t* sa = smem + rs * kStageBytes;
+        mbar_arrive_expect_tx(&full[rs], kStageBytes);
+        tma_load_2d(sa, &tmA, &full[rs], (r + STAGES) * kBK, m0);
+        tma_load_2d(sa + kATileBytes, &tmB, &full[rs], 2 * n0, (r + STAGES) * (kBK / 2));
+        issued = r + STAGES + 1;
+      } else {
+        report_timeout(21);
+      }
+    }
+    if (!mbar_wait(&full[s], (kt / STAGES) & 1)) {
+      report_timeout(22);
+      ok = false;
+      break;
+    }
+    const float* As = reinterpret_cast<const float*>(smem + s * kStageBytes);
+    const float* Bs = reinterpret_cast<const float*>(smem + s * kStageBytes + kATileBytes);
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) t[i][j] = ident;
+#pragma unroll 2
+    for (int q = 0; q < kBK / 4; q++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        float2 a[8];
+#pragma unroll
+        for (int ii = 0; ii < 8; ii++)
+          a[ii] = *reinterpret_cast<const float2*>(As + (ty + 16 * ii) * kBK + ((q ^ swz) << 2) + 2 * h);
+        float4 b[2];
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+          b[c] = *reinterpret_cast<const float4*>(Bs + (2 * q + h) * (2 * kBN) + (cbase + 32 * c + 2 * tx) * 2);
+#pragma unroll
+        for (int ii = 0; ii < 8; ii++)
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            t[ii][2 * c] = Mac<OP>::mac2(t[ii][2 * c], a[ii], make_float2(b[c].x, b[c].y));
+            t[ii][2 * c + 1] = Mac<OP>::mac2(t[ii][2 * c + 1], a[ii], make_float2(b[c].z, b[c].w));
+          }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    // strict record: the k-tile where best last improved holds the witness
+#pragma unroll
+    for (int ii = 0; ii < 8; ii++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        if (O::better(t[ii][j], best[ii][j])) {
+          best[ii][j] = t[ii][j];
+          rec[(ty + 16 * ii) * kPredRecStride + cbase + 32 * (j >> 1) + 2 * tx + (j & 1)] = (uint16_t)kt;
+        }
+      }
+  }
+  if (!ok) {
+    // every issued copy lands before this CTA's shared memory is released
+    if (threadIdx.x == 0)
+      for (int i = max(0, issued - STAGES); i < issued; i++) mbar_wait(&full[i % STAGES], (i / STAGES) & 1);
+    return;
+  }
+  __syncwarp();
+
   int ch = 0;
 #pragma unroll
-  for (int r = 0; r < 4; r++) {
-    const int i = i0 + ty + 16 * r;
+  for (int ii = 0; ii < 8; ii++) {
+    const int i = m0 + ty + 16 * ii;
     if (i >= n) continue;
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-      const int j = j0 + tx + 16 * c;
-      if (j >= n) continue;
-      const float cv = X[(long long)i * ldx + j];
-      const float b = best[r][c];
+    for (int j = 0; j < 4; j++) {
+      const int cl = cbase + 32 * (j >> 1) + 2 * tx + (j & 1);
+      const int col = n0 + cl;
+      if (col >= n) continue;
+      const float cv = X[(long long)i * ldx + col];
+      const float b = best[ii][j];
       // host_srgemm epilogue: D = addop(D, C) with D = best
       const float xn = O::kMin ? ((cv < b) ? cv : b) : ((b < cv) ? cv : b);
-      const bool improved = O::better(b, cv);
-      Xn[(long long)i * ldxn + j] = xn;
-      Pn[(long long)i * ldpn + j] = improved ? P[(long long)kb[r][c] * ldp + j] : P[(long long)i * ldp + j];
+      int32_t pv;
+      if (O::better(b, cv)) {
+        const int k0 = (int)rec[(ty + 16 * ii) * kPredRecStride + cl] * kBK;
+        const int k1 = min(k0 + kBK, n);
+        const float* xr = X + (long long)i * ldx;
+        const float* tr = XT + (long long)col * ldt;
+        int ks = -1;
+        for (int k = k0; k < k1; k++)
+          if (O::mul(xr[k], tr[k]) == b) {
+            ks = k;
+            break;
+          }
+        if (ks < 0) {
+          // cannot happen with the precondition (no NaN, no -0.0): the
+          // product that set best is re-formed with the same operation
+          report_error(SIMD2_ERR_INVALID_ARG);
+          ks = i;
+        }
+        pv = P[(long long)ks * ldp + col];
+      } else {
+        pv = P[(long long)i * ldp + col];
+      }
+      Xn[(long long)i * ldxn + col] = xn;
+      Pn[(long long)i * ldpn + col] = pv;
       if (__float_as_uint(xn) != __float_as_uint(cv)) ch = 1;
     }
   }
-  if (__any_sync(0xffffffffu, ch) && (threadIdx.x & 31) == 0) atomicOr(changed, 1);
+  if (__any_sync(0xffffffffu, ch) && lane == 0) atomicOr(changed, 1);
 }
 
+// XT[j][i] = X[i][j] for i, j < n, through 32 x 32 shared-memory tiles.
+__global__ void transpose_f32_kernel(int n, const float* __restrict__ X, long long ldx, float* __restrict__ XT,
+                                     long long ldt) {
+  __shared__ float tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = by + r, j = bx + threadIdx.x;
+    if (i < n && j < n) tile[r][threadIdx.x] = X[(long long)i * ldx + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = bx + r, i = by + threadIdx.x;
+    if (i < n && j < n) XT[(long long)j * ldt + i] = tile[threadIdx.x][r];
+  }
+}
 // P[i][j] = i where X[i][j] is an edge (not the add identity) and i != j, else -1.
 __global__ void pred_init_kernel(int n, const float* __restrict__ X, long long ldx, int32_t* __restrict__ P,
                                  long long ldp, float ident) {

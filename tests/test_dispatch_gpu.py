@@ -116,3 +116,20 @@ def test_learned_dispatch_identical_and_not_slower(cuda):
         t_dense += sum(ra["ms"])
         t_learned += sum(rb["ms"])
     assert t_learned <= 1.05 * t_dense, (t_learned, t_dense)
+
+
+def test_learned_dispatch_small_closure_runs_dense_path(cuda):
+    """At n <= 1024 a per-step decision costs about a dense step, so the learned
+    policy runs the plain path: same bits, same per-step configurations, no
+    features recorded."""
+    params = torch.randn(costmodel.param_count(), generator=torch.Generator().manual_seed(0)).to(cuda)
+    x = datagen.er_graph(512, 0.05, seed=1)
+    want, it_want = oracle.closure("min_plus", x)
+    Xa = torch.from_numpy(x.copy()).to(cuda)
+    Xb = torch.from_numpy(x.copy()).to(cuda)
+    ra = s2.closure_ex("min_plus", Xa, dispatch="dense", record=True)
+    rb = s2.closure_ex("min_plus", Xb, dispatch="learned", mlp_params=params, record=True)
+    assert ra["iters"] == rb["iters"] == it_want
+    assert ra["configs"] == rb["configs"]
+    assert all(f == [0.0] * 7 for f in rb["features"])
+    np.testing.assert_array_equal(bits(Xb.cpu().numpy()), bits(want))

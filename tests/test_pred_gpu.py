@@ -41,6 +41,27 @@ def test_closure_pred_matches_oracle(cuda, op, n):
     np.testing.assert_array_equal(P.cpu().numpy(), want_p)
 
 
+TIE_IDENT = {"min_plus": np.inf, "max_plus": -np.inf, "max_min": -np.inf, "min_max": np.inf}
+
+
+@pytest.mark.parametrize("op", list(TIE_IDENT))
+@pytest.mark.parametrize("n", [300, 512])
+def test_closure_pred_ties(cuda, op, n):
+    """Small integer weights: most (i, j) have many k attaining the best
+    product, within one 32-wide k-tile and across k-tiles, so the witness must
+    be the lowest such k exactly as in the sequential accumulation."""
+    rng = np.random.default_rng(n + len(op))
+    x = np.where(rng.random((n, n)) < 0.2, rng.integers(1, 4, (n, n)), TIE_IDENT[op]).astype(np.float32)
+    if op == "max_plus":  # a DAG: no positive cycles
+        x = np.where(np.triu(np.ones((n, n), bool), 1), x, -np.inf).astype(np.float32)
+    want_x, want_p, want_it = oracle.closure_pred(op, x)
+    X = torch.from_numpy(x).to(cuda)
+    it, P = s2.closure_pred(op, X)
+    assert it == want_it
+    assert np.array_equal(X.cpu().numpy().view(np.uint32), want_x.view(np.uint32))
+    np.testing.assert_array_equal(P.cpu().numpy(), want_p)
+
+
 @pytest.mark.parametrize("family,edges", [("k0", lambda n: []), ("k1", k1_edges), ("kn", kn_edges),
                                           ("dicircle", dicircle_edges)])
 def test_fw_families_1000(cuda, family, edges):
