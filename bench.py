@@ -300,6 +300,36 @@ def extra_measurements(args, dev):
     out["batched_apsp"] = res_b
     del mats
 
+    # --- paths: closure with a predecessor matrix, and the MST from the min_max closure
+    paths = {}
+    xp = torch.from_numpy(datagen.er_graph(4096, 0.05, seed=1)).to(dev)
+
+    def best_ms(fn, reps=3):
+        fn(xp.clone())  # warm-up
+        best = None
+        for _ in range(reps):
+            X = xp.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = fn(X)
+            torch.cuda.synchronize()
+            dt = (time.perf_counter() - t0) * 1e3
+            best = dt if best is None else min(best, dt)
+        return best, r
+
+    pred_ms, (pred_it, _) = best_ms(lambda X: s2.closure_pred("min_plus", X))
+    plain_ms, plain_it = best_ms(lambda X: s2.closure("min_plus", X))
+    paths["closure_pred_er4096"] = {
+        "ms": pred_ms, "iters": pred_it, "gops": 2.0 * 4096 ** 3 * pred_it / pred_ms / 1e6,
+        "plain_closure_ms": plain_ms, "plain_iters": plain_it, "cost_vs_plain": pred_ms / plain_ms,
+        "how": "simd2_closure_pred wall clock (X and P to the fixed point) vs simd2_closure on the same ER graph"}
+    mst_ms, mst_r = best_ms(lambda X: s2.mst(X))
+    paths["mst_er4096"] = {"ms": mst_ms, "edges": int(len(mst_r[0])), "closure_iters": int(mst_r[3]),
+                           "how": "simd2_mst wall clock: min_max closure, candidate scan, host Kruskal over the "
+                                  "candidates"}
+    out["paths"] = paths
+    del xp
+
     # --- dense-contraction workloads at full size (tensor cores)
     cfg4 = {}
     n4 = 16384

@@ -165,7 +165,13 @@ typedef enum simd2_dispatch {
  * Results are bit-identical for every policy.  LEARNED decides per step only
  * for n > 1024: a decision (occupancy pass, MLP launch, host round trip) costs
  * about as much as a whole dense step below that, so smaller closures run the
- * DENSE path (step_features then stay zero). */
+ * DENSE path (step_features then stay zero).  Above that, with SIMD2_CONV_EXACT
+ * and a semiring simd2_spgemm_compute supports, LEARNED first squares X as a
+ * CSR SpGEMM while X holds at most n^2/32 entries and the step forms at most
+ * n^3/256 products (a result past n^2/32 entries is written densely and ends
+ * the opening; sparse steps are recorded as config 8, features zero).  The
+ * dense steps then follow the MLP's per-step choice for n > 2048, and the
+ * DENSE path for 1024 < n <= 2048. */
 int simd2_closure_ex(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_conv conv,
                      simd2_dispatch dispatch, int fixed_config, const float* mlp_params,
                      int* iters_out, int* step_configs, float* step_ms, float* step_features,

@@ -183,6 +183,9 @@ def config_id(split: int, skip: bool) -> int:
 
 
 def config_desc(cfg: int) -> str:
+    """Name of a closure-step configuration; NUM_CONFIGS marks a sparse (SpGEMM) step of the learned policy."""
+    if cfg == NUM_CONFIGS:
+        return "sparse"
     return f"split{1 << (cfg & 3)}{'+skip' if cfg >> 2 else ''}"
 
 

@@ -804,6 +804,10 @@ int dense_split(int n, int sms) {
   return s;
 }
 
+// Defined with the SpGEMM host code below.
+int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, int* steps, bool* changed,
+                           int* step_cfg, float* step_ms, cudaStream_t stream);
+
 // Closure steps enqueued in chunks without a host round trip per step.
 // changed[t] is written by step t; every kernel of step t+1 reads changed[t]
 // as its gate and does nothing when it is 0, so steps enqueued past the fixed
@@ -933,6 +937,29 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     if (step_feat) std::fill(step_feat, step_feat + (size_t)max_iter * kMlpFeat, 0.f);
     step_feat = nullptr;
   }
+  // The learned policy opens with sparse steps while X is sparse (see
+  // closure_sparse_opening; bitwise change test only).
+  int it0 = 0;
+  if (dispatch == 2 && conv == SIMD2_CONV_EXACT) {
+    bool ch = true;
+    if ((rc = closure_sparse_opening(op, n, X, ldx, max_iter, &it0, &ch, step_cfg, step_ms, stream))) return rc;
+    if (step_feat) std::fill(step_feat, step_feat + (size_t)it0 * kMlpFeat, 0.f);
+    if (!ch || it0 == max_iter) {
+      if (iters_out) *iters_out = it0;
+      return ch ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
+    }
+    max_iter -= it0;
+    if (step_cfg) step_cfg += it0;
+    if (step_ms) step_ms += it0;
+    if (step_feat) step_feat += (size_t)it0 * kMlpFeat;
+    // Up to n = kLearnedLoopMinN the MLP's per-step choice (measured on R-MAT
+    // graphs) gains less than its decisions cost: the gated dense path goes on.
+    if (n <= kLearnedLoopMinN) {
+      dispatch = 0;
+      if (step_feat) std::fill(step_feat, step_feat + (size_t)max_iter * kMlpFeat, 0.f);
+      step_feat = nullptr;
+    }
+  }
   const bool can_skip = skip_supported(op) && (n + kBK - 1) / kBK <= kMaxSkipKtiles;
   const bool need_occ = dispatch == 2 || step_feat != nullptr || (dispatch == 1 && config_skip(fixed_cfg) && can_skip);
   // Workspace: [srgemm plan][Xnew n x n][flag + decision][occupancy]
@@ -953,9 +980,11 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   uint8_t* obase = ws + o_off;
 
   if (dispatch != 2 && step_feat == nullptr) {
-    return closure_gated(op, n, X, ldx, max_iter, conv, fixed_cfg, dispatch == 1, can_skip, need_occ, occ, ws,
-                         x_off, reinterpret_cast<int*>(ws + f_off + 256), obase, iters_out, step_cfg, step_ms, sms,
-                         stream);
+    int it2 = 0;
+    rc = closure_gated(op, n, X, ldx, max_iter, conv, fixed_cfg, dispatch == 1, can_skip, need_occ, occ, ws, x_off,
+                       reinterpret_cast<int*>(ws + f_off + 256), obase, &it2, step_cfg, step_ms, sms, stream);
+    if (iters_out) *iters_out = it0 + it2;
+    return rc;
   }
   // Per-step loop (learned dispatch, or feature recording): the occupancy and
   // the cost-model choice for step t+1 are enqueued right after step t's
@@ -1068,7 +1097,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     SIMD2_CUDA_TRY(cudaMemcpy2DAsync(X, ldx * 4, cur, ldcur * 4, (size_t)n * 4, n, cudaMemcpyDeviceToDevice, stream));
   }
   SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
-  if (iters_out) *iters_out = it;
+  if (iters_out) *iters_out = it0 + it;
   return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
@@ -1393,7 +1422,7 @@ SpPlan sp_plan(int M, int N, size_t base) {
   return p;
 }
 
-template <bool COUNT>
+template <bool COUNT, bool DENSE = false>
 int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t stream) {
   auto pick = [&](auto kern) -> int {
     if (plan.smem > (48u << 10))
@@ -1404,11 +1433,11 @@ int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t s
     return SIMD2_OK;
   };
   switch (op) {
-    case SIMD2_MIN_PLUS: return pick(spgemm_rows_kernel<SIMD2_MIN_PLUS, COUNT>);
-    case SIMD2_MAX_PLUS: return pick(spgemm_rows_kernel<SIMD2_MAX_PLUS, COUNT>);
-    case SIMD2_MAX_MIN: return pick(spgemm_rows_kernel<SIMD2_MAX_MIN, COUNT>);
-    case SIMD2_MIN_MAX: return pick(spgemm_rows_kernel<SIMD2_MIN_MAX, COUNT>);
-    case SIMD2_PLUS_MUL: return pick(spgemm_rows_kernel<SIMD2_PLUS_MUL, COUNT>);
+    case SIMD2_MIN_PLUS: return pick(spgemm_rows_kernel<SIMD2_MIN_PLUS, COUNT, DENSE>);
+    case SIMD2_MAX_PLUS: return pick(spgemm_rows_kernel<SIMD2_MAX_PLUS, COUNT, DENSE>);
+    case SIMD2_MAX_MIN: return pick(spgemm_rows_kernel<SIMD2_MAX_MIN, COUNT, DENSE>);
+    case SIMD2_MIN_MAX: return pick(spgemm_rows_kernel<SIMD2_MIN_MAX, COUNT, DENSE>);
+    case SIMD2_PLUS_MUL: return pick(spgemm_rows_kernel<SIMD2_PLUS_MUL, COUNT, DENSE>);
     default: return SIMD2_ERR_UNSUPPORTED;
   }
 }
@@ -1479,6 +1508,163 @@ int spgemm_fill(int op, int M, int N, int K, const int* ap, const int* aj, const
   a.next_row = reinterpret_cast<int*>(ws + plan.ctr_off);
   SIMD2_CUDA_TRY(cudaMemsetAsync(a.next_row, 0, 4, stream));
   return spgemm_launch<false>(op, a, plan, stream);
+}
+
+// FILL pass into a dense M x N matrix D (pitch ldd) that holds the identity.
+int spgemm_fill_dense(int op, int M, int N, int K, const int* ap, const int* aj, const float* av, int a_nnz,
+                      const int* bp, const int* bj, const float* bv, int b_nnz, const int* cp, const int* cj,
+                      const float* cv, int c_nnz, float* D, long long ldd, uint8_t* ws, const SpPlan& plan,
+                      cudaStream_t stream) {
+  SpArgs a{};
+  a.M = M, a.N = N, a.K = K, a.a_nnz = a_nnz, a.b_nnz = b_nnz, a.c_nnz = c_nnz;
+  a.ap = ap, a.aj = aj, a.av = av, a.bp = bp, a.bj = bj, a.bv = bv, a.cp = cp, a.cj = cj, a.cv = cv;
+  a.dense = D, a.ldd = ldd;
+  a.acc = reinterpret_cast<float*>(ws + plan.acc_off);
+  a.next_row = reinterpret_cast<int*>(ws + plan.ctr_off);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(a.next_row, 0, 4, stream));
+  return spgemm_launch<false, true>(op, a, plan, stream);
+}
+
+// Sparse opening of a learned closure: while X is sparse, square it in CSR.
+// A step runs as a semiring SpGEMM when X holds at most n^2/32 entries, the
+// step forms at most n^3/256 products (sum over k of row count x column
+// count; at B200's rates of about 100 G products/s sparse and 17 T MAC/s
+// dense, that is under two thirds of a dense step's time).  A result with
+// more than n^2/32 entries goes straight into X and ends the opening.  X
+// (dense, pitch ldx) is rewritten when any step ran.  *steps: steps run; *changed: false when the last one changed
+// nothing.  Every step gives the dense step's bits (same contract, same order).
+int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, int* steps, bool* changed,
+                           int* step_cfg, float* step_ms, cudaStream_t stream) {
+  *steps = 0;
+  *changed = true;
+  if (!spgemm_op(op) || op == SIMD2_PLUS_MUL || max_iter <= 0 || n < 2) return SIMD2_OK;
+  const long long nn2 = (long long)n * n;
+  const long long cap = nn2 / 32;
+  if (cap < 1 || cap > 0x7fffffffLL) return SIMD2_OK;
+  const float ident = add_identity(op);
+  const SpPlan plan = sp_plan(n, n, 0);
+  // slot 1: [spgemm plan][offsets x2][columns x2][values x2][column counts][products]
+  size_t off = plan.total;
+  auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
+  size_t rp_off[2], cj_off[2], cv_off[2];
+  for (int b = 0; b < 2; b++) {
+    rp_off[b] = take((size_t)(n + 1) * 4);
+    cj_off[b] = take((size_t)cap * 4);
+    cv_off[b] = take((size_t)cap * 4);
+  }
+  const size_t cc_off = take((size_t)n * 4);
+  const size_t pr_off = take(16);
+  void* p = nullptr;
+  int rc = get_workspace_slot(stream, 1, off, &p);
+  if (rc) return rc;
+  uint8_t* ws = static_cast<uint8_t*>(p);
+  int* rp[2] = {reinterpret_cast<int*>(ws + rp_off[0]), reinterpret_cast<int*>(ws + rp_off[1])};
+  int* cj[2] = {reinterpret_cast<int*>(ws + cj_off[0]), reinterpret_cast<int*>(ws + cj_off[1])};
+  float* cv[2] = {reinterpret_cast<float*>(ws + cv_off[0]), reinterpret_cast<float*>(ws + cv_off[1])};
+  int* colcnt = reinterpret_cast<int*>(ws + cc_off);
+  unsigned long long* prod = reinterpret_cast<unsigned long long*>(ws + pr_off);
+  int* counts = reinterpret_cast<int*>(ws + plan.cnt_off);
+  int* flag = reinterpret_cast<int*>(ws + plan.flag_off);
+  long long* tot = reinterpret_cast<long long*>(ws + plan.tot_off);
+
+  // X -> CSR, when sparse enough
+  SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, 8, stream));
+  dense_row_count_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, n, X, ldx, ident, counts);
+  offsets_scan_kernel<<<1, 1024, 0, stream>>>(counts, n, rp[0], flag + 1, tot);
+  count_launch();
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  long long nnz = 0;
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(&nnz, tot, 8, cudaMemcpyDeviceToHost, stream));
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (nnz > cap) return SIMD2_OK;
+  dense_to_csr_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, n, X, ldx, ident, rp[0], cj[0], cv[0]);
+  count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+
+  cudaEvent_t ev[2] = {};
+  if (step_ms)
+    for (auto& e : ev) SIMD2_CUDA_TRY(cudaEventCreate(&e));
+  int cur = 0, it = 0;
+  bool ch = true, in_x = false;  // in_x: the last step wrote X itself
+  const unsigned long long max_products = (unsigned long long)nn2 * (unsigned long long)n / 256ull;
+  while (ch && it < max_iter) {
+    SIMD2_CUDA_TRY(cudaMemsetAsync(colcnt, 0, (size_t)n * 4, stream));
+    SIMD2_CUDA_TRY(cudaMemsetAsync(prod, 0, 8, stream));
+    csr_col_count_kernel<<<grid_for(std::max(nnz, 1LL)), 256, 0, stream>>>(cj[cur], nnz, n, colcnt);
+    csr_products_kernel<<<grid_for(n), 256, 0, stream>>>(n, rp[cur], colcnt, prod);
+    count_launch();
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+    unsigned long long hp = 0;
+    SIMD2_CUDA_TRY(cudaMemcpyAsync(&hp, prod, 8, cudaMemcpyDeviceToHost, stream));
+    SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (hp > max_products) break;
+    const int nx = cur ^ 1;
+    if (step_ms) cudaEventRecord(ev[0], stream);
+    long long nn = 0;
+    rc = spgemm_count(op, n, n, n, rp[cur], cj[cur], (int)nnz, rp[cur], cj[cur], (int)nnz, rp[cur], cj[cur], (int)nnz,
+                      rp[nx], &nn, ws, plan, stream);
+    if (rc && rc != kSpOverflow) return rc;
+    if (rc == kSpOverflow || nn > cap) {
+      // the result is too dense for CSR: this step writes it straight into X
+      // (more entries than X had, so it changed) and the dense loop goes on
+      fill_kernel<float><<<grid_for(nn2), 256, 0, stream>>>(X, ldx, n, n, ident);
+      count_launch();
+      SIMD2_CUDA_TRY(cudaGetLastError());
+      rc = spgemm_fill_dense(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz,
+                             rp[cur], cj[cur], cv[cur], (int)nnz, X, ldx, ws, plan, stream);
+      if (rc) return rc;
+      if (step_ms) {
+        cudaEventRecord(ev[1], stream);
+        cudaEventSynchronize(ev[1]);
+        cudaEventElapsedTime(&step_ms[it], ev[0], ev[1]);
+      }
+      if (step_cfg) step_cfg[it] = kNumConfigs;
+      it++;
+      in_x = true;
+      ch = true;
+      break;
+    }
+    rc = spgemm_fill(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur],
+                     cj[cur], cv[cur], (int)nnz, rp[nx], cj[nx], cv[nx], nn, ws, plan, stream);
+    if (rc) return rc;
+    // X' holds X's structure (C = X) plus new entries: equal counts mean equal structure
+    if (nn != nnz) {
+      ch = true;
+    } else {
+      SIMD2_CUDA_TRY(cudaMemsetAsync(flag + 2, 0, 4, stream));
+      values_differ_kernel<<<grid_for(std::max(nn, 1LL)), 256, 0, stream>>>(cv[cur], cv[nx], nn, flag + 2);
+      count_launch();
+      SIMD2_CUDA_TRY(cudaGetLastError());
+      int h = 0;
+      SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag + 2, 4, cudaMemcpyDeviceToHost, stream));
+      SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+      ch = h != 0;
+    }
+    if (step_ms) {
+      cudaEventRecord(ev[1], stream);
+      cudaEventSynchronize(ev[1]);
+      cudaEventElapsedTime(&step_ms[it], ev[0], ev[1]);
+    }
+    if (step_cfg) step_cfg[it] = kNumConfigs;  // the sparse step
+    it++;
+    cur = nx;
+    nnz = nn;
+  }
+  if (step_ms)
+    for (auto& e : ev) cudaEventDestroy(e);
+  if (it > 0 && !in_x) {
+    fill_kernel<float><<<grid_for(nn2), 256, 0, stream>>>(X, ldx, n, n, ident);
+    csr_scatter_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, rp[cur], cj[cur], cv[cur], X, ldx);
+    count_launch();
+    count_launch();
+    SIMD2_CUDA_TRY(cudaGetLastError());
+  }
+  SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+  *steps = it;
+  *changed = ch;
+  return SIMD2_OK;
 }
 
 }  // namespace

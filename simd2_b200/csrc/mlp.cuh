@@ -23,7 +23,8 @@ constexpr int kMlpW3 = kMlpB2 + kMlpH;
 constexpr int kMlpB3 = kMlpW3 + kMlpH;
 constexpr int kMlpParams = kMlpB3 + 1;  // 1505
 constexpr int kNumConfigs = 8;          // split {1,2,4,8} x skip {0,1}
-constexpr int kLearnedMinN = 1024;      // the learned dispatch decides per step above this n
+constexpr int kLearnedMinN = 1024;      // the learned policy runs the plain path up to this n,
+constexpr int kLearnedLoopMinN = 2048;  // then a sparse opening, and per-step MLP choices above this n
 
 __host__ __device__ inline int config_split(int c) { return 1 << (c & 3); }
 __host__ __device__ inline int config_skip(int c) { return c >> 2; }

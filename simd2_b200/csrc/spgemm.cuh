@@ -22,7 +22,8 @@
 //
 // Two passes share the kernel: COUNT writes the row's nonzero count (no
 // values, no barriers per k), FILL writes columns and values at the offsets
-// the host formed from the counts.
+// the host formed from the counts -- or, with DENSE, the values straight into
+// a dense matrix prefilled with the identity (no offsets needed).
 #pragma once
 #include "common.cuh"
 
@@ -79,6 +80,8 @@ struct SpArgs {
   const int* dp;  // FILL: output offsets (M + 1)
   int* dj;        // FILL: output columns
   float* dv;      // FILL: output values
+  float* dense;   // FILL into a dense matrix (DENSE): D rows of pitch ldd, prefilled with the identity
+  long long ldd;
   int* row_nnz;   // COUNT: per-row nonzero count
   float* acc;     // gridDim.x * N floats of scratch (FILL)
   int* next_row;  // atomic row counter, zero before the launch
@@ -107,7 +110,7 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* s_warp, int* tot
   return base + v - x;
 }
 
-template <int OP, bool COUNT>
+template <int OP, bool COUNT, bool DENSE = false>
 __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
   using O = SpOps<OP>;
   extern __shared__ uint32_t bitmap[];  // ceil(N / 32) words
@@ -157,6 +160,17 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
       int total;
       block_exclusive_scan(cnt, s_warp, &total);
       if (threadIdx.x == 0) a.row_nnz[r] = total;
+    } else if constexpr (DENSE) {
+      // the touched columns straight into the dense row (the rest holds the identity)
+      float* drow = a.dense + (long long)r * a.ldd;
+      for (int w = threadIdx.x; w < words; w += kSpThreads) {
+        uint32_t bits = bitmap[w];
+        while (bits) {
+          const int j = (w << 5) + __ffs(bits) - 1;
+          bits &= bits - 1;
+          drow[j] = acc[j];
+        }
+      }
     } else {
       // columns in increasing order: word w's set bits land after all set bits of words < w
       long long out = a.dp[r];
@@ -263,6 +277,26 @@ __global__ void csr_scatter_kernel(int rows, const int* __restrict__ rp, const i
   const int lane = threadIdx.x & 31;
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5)
     for (int e = rp[r] + lane; e < rp[r + 1]; e += 32) X[(long long)r * ld + cj[e]] = cv[e];
+}
+
+// colcnt[j] += 1 for every stored column j (colcnt zeroed before).
+__global__ void csr_col_count_kernel(const int* __restrict__ cj, long long nnz, int ncols, int* __restrict__ colcnt) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+    const int j = cj[e];
+    if ((unsigned)j < (unsigned)ncols) atomicAdd(&colcnt[j], 1);
+  }
+}
+
+// *out += sum_k rowcnt(k) * colcnt(k): the products a Gustavson A (x) A forms
+// (each stored A[i][k] meets each stored A[k][j]).  *out zeroed before.
+__global__ void csr_products_kernel(int n, const int* __restrict__ rp, const int* __restrict__ colcnt,
+                                    unsigned long long* __restrict__ out) {
+  unsigned long long s = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    s += (unsigned long long)(rp[k + 1] - rp[k]) * (unsigned long long)colcnt[k];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
 }
 
 // Entries of each dense row that differ bitwise from the identity; one warp per row.

@@ -133,3 +133,35 @@ def test_learned_dispatch_small_closure_runs_dense_path(cuda):
     assert ra["configs"] == rb["configs"]
     assert all(f == [0.0] * 7 for f in rb["features"])
     np.testing.assert_array_equal(bits(Xb.cpu().numpy()), bits(want))
+
+
+@pytest.mark.parametrize("case", ["rmat", "components"])
+def test_learned_sparse_opening_identical(cuda, case):
+    """Above n = 1024 the learned policy squares a sparse X as CSR SpGEMM
+    steps (config 8) before the MLP-chosen dense steps: same bits and the
+    same step count as the dense path.  'components' (disjoint 4-cycles)
+    converges while still sparse."""
+    n = 2048
+    if case == "rmat":
+        x = datagen.rmat_graph(n, 3.0, seed=21)
+    else:
+        rng = np.random.default_rng(22)
+        x = np.full((n, n), np.inf, np.float32)
+        np.fill_diagonal(x, 0.0)
+        for b in range(0, n, 4):
+            for t in range(4):
+                x[b + t, b + (t + 1) % 4] = rng.integers(1, 100)
+    params = torch.randn(costmodel.param_count(), generator=torch.Generator().manual_seed(1)).to(cuda)
+    Xa = torch.from_numpy(x.copy()).to(cuda)
+    Xb = torch.from_numpy(x.copy()).to(cuda)
+    ra = s2.closure_ex("min_plus", Xa, dispatch="dense", record=True)
+    rb = s2.closure_ex("min_plus", Xb, dispatch="learned", mlp_params=params, record=True)
+    assert ra["iters"] == rb["iters"]
+    assert torch.equal(Xa.view(torch.int32), Xb.view(torch.int32))
+    assert rb["configs"][0] == s2.NUM_CONFIGS  # the opening ran
+    if case == "components":
+        assert all(c == s2.NUM_CONFIGS for c in rb["configs"])
+    # without recording as well
+    Xc = torch.from_numpy(x.copy()).to(cuda)
+    assert s2.closure_ex("min_plus", Xc, dispatch="learned", mlp_params=params) == ra["iters"]
+    assert torch.equal(Xa.view(torch.int32), Xc.view(torch.int32))
