@@ -1396,24 +1396,31 @@ bool spgemm_op(int op) {
          op == SIMD2_PLUS_MUL;
 }
 
+constexpr int kSpSmemAccMaxN = 16384;
+
 struct SpPlan {
   int grid;            // persistent CTAs
-  size_t smem;         // bitmap bytes
+  size_t smem;         // bitmap bytes (COUNT)
+  bool smem_acc;       // FILL accumulators in shared memory
+  size_t smem_fill;    // FILL: bitmap + accumulators
   size_t acc_off, cnt_off, ctr_off, flag_off, tot_off, total;
 };
 
 SpPlan sp_plan(int M, int N, size_t base) {
   SpPlan p{};
-  const size_t bitmap = (size_t)((N + 31) / 32) * 4;
+  const size_t bitmap = (size_t)sp_bitmap_words(N) * 4;
   p.smem = bitmap;
-  int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / std::max<size_t>(bitmap, 1)));
+  // the FILL pass keeps the row's accumulators in shared memory up to 16384 columns
+  p.smem_acc = N <= kSpSmemAccMaxN;
+  p.smem_fill = bitmap + (p.smem_acc ? (size_t)N * 4 : 0);
+  int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / std::max<size_t>(p.smem_fill, 1)));
   long long g = std::min<long long>((long long)M, 148LL * per_sm);
   // the accumulator slices stay below 1 GiB
   g = std::min<long long>(g, std::max<long long>(1, (1LL << 30) / (4LL * std::max(N, 1))));
   p.grid = (int)std::max<long long>(1, g);
   size_t off = base;
   auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
-  p.acc_off = take((size_t)p.grid * N * 4);
+  p.acc_off = take(p.smem_acc ? 16 : (size_t)p.grid * N * 4);
   p.cnt_off = take((size_t)std::max(M, 1) * 4);
   p.ctr_off = take(16);
   p.flag_off = take(16);
@@ -1422,22 +1429,26 @@ SpPlan sp_plan(int M, int N, size_t base) {
   return p;
 }
 
-template <bool COUNT, bool DENSE = false>
+template <bool COUNT, bool DENSE = false, bool SMEM = false>
 int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t stream) {
+  if constexpr (!COUNT && !SMEM) {
+    if (plan.smem_acc) return spgemm_launch<COUNT, DENSE, true>(op, args, plan, stream);
+  }
+  const size_t smem = SMEM ? plan.smem_fill : plan.smem;
   auto pick = [&](auto kern) -> int {
-    if (plan.smem > (48u << 10))
-      SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
-    kern<<<plan.grid, kSpThreads, plan.smem, stream>>>(args);
+    if (smem > (48u << 10))
+      SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<plan.grid, kSpThreads, smem, stream>>>(args);
     count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
     return SIMD2_OK;
   };
   switch (op) {
-    case SIMD2_MIN_PLUS: return pick(spgemm_rows_kernel<SIMD2_MIN_PLUS, COUNT, DENSE>);
-    case SIMD2_MAX_PLUS: return pick(spgemm_rows_kernel<SIMD2_MAX_PLUS, COUNT, DENSE>);
-    case SIMD2_MAX_MIN: return pick(spgemm_rows_kernel<SIMD2_MAX_MIN, COUNT, DENSE>);
-    case SIMD2_MIN_MAX: return pick(spgemm_rows_kernel<SIMD2_MIN_MAX, COUNT, DENSE>);
-    case SIMD2_PLUS_MUL: return pick(spgemm_rows_kernel<SIMD2_PLUS_MUL, COUNT, DENSE>);
+    case SIMD2_MIN_PLUS: return pick(spgemm_rows_kernel<SIMD2_MIN_PLUS, COUNT, DENSE, SMEM>);
+    case SIMD2_MAX_PLUS: return pick(spgemm_rows_kernel<SIMD2_MAX_PLUS, COUNT, DENSE, SMEM>);
+    case SIMD2_MAX_MIN: return pick(spgemm_rows_kernel<SIMD2_MAX_MIN, COUNT, DENSE, SMEM>);
+    case SIMD2_MIN_MAX: return pick(spgemm_rows_kernel<SIMD2_MIN_MAX, COUNT, DENSE, SMEM>);
+    case SIMD2_PLUS_MUL: return pick(spgemm_rows_kernel<SIMD2_PLUS_MUL, COUNT, DENSE, SMEM>);
     default: return SIMD2_ERR_UNSUPPORTED;
   }
 }

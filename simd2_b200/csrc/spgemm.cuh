@@ -10,15 +10,18 @@
 //
 // Row-wise (Gustavson) accumulation.  Persistent CTAs take rows from an
 // atomic counter; a CTA keeps, for its current row, a bitmap of touched
-// columns in shared memory and the running values in its own slice of a
-// global scratch array (N floats per CTA, L2-resident for the sizes used).
-// The row's A entries are visited in increasing k; for each k the threads
-// spread over B's row k (distinct columns, so no two threads meet on one
-// column) and a barrier separates consecutive k.  Every output therefore
-// receives its products in increasing k -- the host_srgemm order
+// columns in shared memory and the running values next to it in shared
+// memory (N <= 16384) or in its own slice of a global scratch array.
+// For plus_mul the row's A entries are visited in increasing k; for each k
+// the threads spread over B's row k (distinct columns, so no two threads meet
+// on one column) and a barrier separates consecutive k.  Every output
+// therefore receives its products in increasing k -- the host_srgemm order
 // (kernel/host_srgemm.h:17-49) -- starting from the add identity, then the C
-// term: bit-identical to the dense contract, plus_mul included.  The bitmap is
-// scanned in word order to write the row's columns sorted.
+// term: bit-identical to the dense contract.  The min/max adds are
+// order-independent on non-NaN values, so for them each warp takes its own
+// A entries and folds products with atomic min / max on order-preserving
+// keys: the same bits without a barrier per k.  The bitmap is scanned in word
+// order to write the row's columns sorted.
 //
 // Two passes share the kernel: COUNT writes the row's nonzero count (no
 // values, no barriers per k), FILL writes columns and values at the offsets
@@ -110,15 +113,69 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* s_warp, int* tot
   return base + v - x;
 }
 
-template <int OP, bool COUNT, bool DENSE = false>
+// min/max adds fold in any order on non-NaN values, so their FILL runs
+// without the per-k barrier: values live in the scratch as order-preserving
+// unsigned keys (larger float, larger key) folded with atomicMin / atomicMax.
+// -0.0 (excluded by the precondition, and no product of other values is
+// -0.0) is the one value whose key differs from an equal float's.
+template <int OP>
+struct SpKey {
+  static constexpr bool kUnordered = OP != SIMD2_PLUS_MUL;
+  static constexpr bool kMin = OP == SIMD2_MIN_PLUS || OP == SIMD2_MIN_MAX;
+  __device__ static uint32_t key(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  }
+  __device__ static float value(uint32_t k) { return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k); }
+  __device__ static void fold(uint32_t* p, float v) {
+    if (v != v) return;  // a NaN product is dropped, as the dense min / max drops it
+    if constexpr (kMin) atomicMin(p, key(v));
+    else atomicMax(p, key(v));
+  }
+};
+
+// Words of the column bitmap, rounded up so that an accumulator array placed
+// after it in shared memory starts 16-byte aligned.
+__host__ __device__ constexpr int sp_bitmap_words(int n) { return ((n + 31) / 32 + 3) & ~3; }
+
+// SMEM: the row's accumulators live in shared memory after the bitmap (N
+// floats or keys), else in the CTA's slice of the global scratch.
+template <int OP, bool COUNT, bool DENSE = false, bool SMEM = false>
 __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
   using O = SpOps<OP>;
-  extern __shared__ uint32_t bitmap[];  // ceil(N / 32) words
+  using KY = SpKey<OP>;
+  // warp-parallel over k: COUNT always, FILL for the order-independent adds
+  constexpr bool kWarpK = COUNT || KY::kUnordered;
+  extern __shared__ uint32_t sp_smem[];
+  uint32_t* bitmap = sp_smem;  // ceil(N / 32) words
   __shared__ int s_row;
   __shared__ int s_warp[kSpThreads / 32];
   const int words = (a.N + 31) >> 5;
-  float* acc = a.acc + (size_t)blockIdx.x * a.N;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* acc = SMEM ? reinterpret_cast<float*>(sp_smem + sp_bitmap_words(a.N)) : a.acc + (size_t)blockIdx.x * a.N;
+  uint32_t* acck = reinterpret_cast<uint32_t*>(acc);
   const float ident = O::ident();
+  if constexpr (!COUNT && KY::kUnordered) {
+    // the accumulators start at the identity; every row puts back what it touched
+    const uint32_t ik = KY::key(ident);
+    for (int j = threadIdx.x; j < a.N; j += kSpThreads) acck[j] = ik;
+  }
+  // the value of touched column j once the row's folds are done
+  auto result = [&](int j) -> float {
+    if constexpr (KY::kUnordered) {
+      if constexpr (SMEM) {
+        const float v = KY::value(acck[j]);
+        acck[j] = KY::key(ident);
+        return v;
+      } else {
+        const float v = KY::value(__ldcg(acck + j));
+        __stcg(acck + j, KY::key(ident));
+        return v;
+      }
+    } else {
+      return acc[j];
+    }
+  };
   while (true) {
     if (threadIdx.x == 0) s_row = atomicAdd(a.next_row, 1);
     for (int w = threadIdx.x; w < words; w += kSpThreads) bitmap[w] = 0u;
@@ -128,29 +185,49 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
     // Offsets and indices are validated by the host pass before any launch;
     // the clamps keep every access inside the arrays whatever they hold.
     const int e1 = min(a.ap[r + 1], a.a_nnz);
-    for (int e = max(a.ap[r], 0); e < e1; e++) {
-      const int k = a.aj[e];
-      if ((unsigned)k >= (unsigned)a.K) continue;  // uniform across the block
-      const float av = COUNT ? 0.f : a.av[e];
-      const int f1 = min(a.bp[k + 1], a.b_nnz);
-      for (int f = max(a.bp[k], 0) + threadIdx.x; f < f1; f += kSpThreads) {
-        const int j = a.bj[f];
-        if ((unsigned)j >= (unsigned)a.N) continue;
-        const uint32_t bit = 1u << (j & 31);
-        const uint32_t old = atomicOr(&bitmap[j >> 5], bit);
-        if constexpr (!COUNT) acc[j] = O::add((old & bit) ? acc[j] : ident, O::mul(av, a.bv[f]));
+    if constexpr (kWarpK) {
+      // one warp per A entry (k), its lanes over B's row k; no order between k
+      for (int e = max(a.ap[r], 0) + warp; e < e1; e += kSpThreads / 32) {
+        const int k = a.aj[e];
+        if ((unsigned)k >= (unsigned)a.K) continue;  // uniform across the warp
+        const float av = COUNT ? 0.f : a.av[e];
+        const int f1 = min(a.bp[k + 1], a.b_nnz);
+        for (int f = max(a.bp[k], 0) + lane; f < f1; f += 32) {
+          const int j = a.bj[f];
+          if ((unsigned)j >= (unsigned)a.N) continue;
+          atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+          if constexpr (!COUNT) KY::fold(acck + j, O::mul(av, a.bv[f]));
+        }
       }
-      if constexpr (!COUNT) __syncthreads();  // the next k sees this k's values, in order
+    } else {
+      for (int e = max(a.ap[r], 0); e < e1; e++) {
+        const int k = a.aj[e];
+        if ((unsigned)k >= (unsigned)a.K) continue;  // uniform across the block
+        const float av = a.av[e];
+        const int f1 = min(a.bp[k + 1], a.b_nnz);
+        for (int f = max(a.bp[k], 0) + threadIdx.x; f < f1; f += kSpThreads) {
+          const int j = a.bj[f];
+          if ((unsigned)j >= (unsigned)a.N) continue;
+          const uint32_t bit = 1u << (j & 31);
+          const uint32_t old = atomicOr(&bitmap[j >> 5], bit);
+          acc[j] = O::add((old & bit) ? acc[j] : ident, O::mul(av, a.bv[f]));
+        }
+        __syncthreads();  // the next k sees this k's values, in order
+      }
     }
     if (a.cp) {
-      // epilogue: D = D (+) C over C's stored entries (the host_srgemm order)
+      // epilogue: D = D (+) C over C's stored entries (after all products in
+      // the ordered fill, the host_srgemm order)
       const int g1 = min(a.cp[r + 1], a.c_nnz);
       for (int f = max(a.cp[r], 0) + threadIdx.x; f < g1; f += kSpThreads) {
         const int j = a.cj[f];
         if ((unsigned)j >= (unsigned)a.N) continue;
         const uint32_t bit = 1u << (j & 31);
         const uint32_t old = atomicOr(&bitmap[j >> 5], bit);
-        if constexpr (!COUNT) acc[j] = O::add((old & bit) ? acc[j] : ident, a.cv[f]);
+        if constexpr (!COUNT) {
+          if constexpr (KY::kUnordered) KY::fold(acck + j, a.cv[f]);
+          else acc[j] = O::add((old & bit) ? acc[j] : ident, a.cv[f]);
+        }
       }
     }
     __syncthreads();
@@ -168,7 +245,7 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
         while (bits) {
           const int j = (w << 5) + __ffs(bits) - 1;
           bits &= bits - 1;
-          drow[j] = acc[j];
+          drow[j] = result(j);
         }
       }
     } else {
@@ -184,16 +261,17 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
           const int b = __ffs(bits) - 1;
           bits &= bits - 1;
           const int j = (w << 5) + b;
+          const float v = result(j);
           if (pos >= 0 && pos < out_end) {
             a.dj[pos] = j;
-            a.dv[pos] = acc[j];
+            a.dv[pos] = v;
           }
           pos++;
         }
         out += total;
       }
     }
-    __syncthreads();  // bitmap and s_row are reused for the next row
+    __syncthreads();  // bitmap, s_row and the scratch are reused for the next row
   }
 }
 

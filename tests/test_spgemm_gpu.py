@@ -30,7 +30,7 @@ def to_csr(x, op, dev):
 
 
 @pytest.mark.parametrize("op", OPS)
-@pytest.mark.parametrize("shape", [(1, 1, 1), (37, 61, 50), (300, 400, 200), (130, 70, 257)])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (37, 61, 50), (300, 400, 200), (130, 70, 257), (20, 20000, 30)])
 @pytest.mark.parametrize("with_c", [False, True])
 def test_spgemm_matches_dense_oracle(cuda, op, shape, with_c):
     M, N, K = shape
@@ -54,6 +54,24 @@ def test_spgemm_matches_dense_oracle(cuda, op, shape, with_c):
         assert np.all(np.diff(row) > 0)  # sorted, no duplicates
         got_pattern[i, row] = True
     assert np.array_equal(got_pattern, pattern)
+
+
+@pytest.mark.parametrize("op", OPS)
+@pytest.mark.parametrize("n_cols", [300, 17000])
+def test_spgemm_dense_ties(cuda, op, n_cols):
+    """Dense-ish operands with values in {1, 2}: many products meet on every
+    output column from different k (the min/max fill folds them from
+    different warps without ordering), with accumulators in shared memory
+    (300 columns) and in the global scratch (17000 columns)."""
+    rng = np.random.default_rng(n_cols)
+    ident = np.float32(s2.SPARSE_IDENTITY[op])
+    a = np.where(rng.random((48, 200)) < 0.6, rng.integers(1, 3, (48, 200)), ident).astype(np.float32)
+    b = np.where(rng.random((200, n_cols)) < 0.6, rng.integers(1, 3, (200, n_cols)), ident).astype(np.float32)
+    c = np.where(rng.random((48, n_cols)) < 0.3, rng.integers(1, 3, (48, n_cols)), ident).astype(np.float32)
+    D = s2.spgemm(op, to_csr(a, op, cuda), to_csr(b, op, cuda), n_cols, C=to_csr(c, op, cuda))
+    got = s2.csr_to_dense(D, n_cols, op).cpu().numpy()
+    want = oracle.srgemm(op, a, b, c, do_epilogue=True)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
 def test_spgemm_empty_rows_and_matrices(cuda):
