@@ -344,7 +344,8 @@ def extra_measurements(args, dev):
     it4 = s2.closure("or_and", X)
     ms4 = (time.perf_counter() - t0) * 1e3
     cfg4["or_and_closure_16384"] = {"ms": ms4, "iters": it4, "gops": 2.0 * n4 ** 3 * it4 / ms4 / 1e6,
-                                    "how": "simd2_closure_orand_u8 wall clock, INT8 tcgen05 per squaring"}
+                                    "how": "simd2_closure_orand_u8 wall clock: CSR SpGEMM steps while X is sparse, then INT8 "
+                                           "tcgen05 per squaring"}
     del X
     q, r = datagen.point_cloud(16384, 65536, 128, seed=4, dup_frac=0.05)
     Q, R = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)

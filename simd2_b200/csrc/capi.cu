@@ -804,9 +804,13 @@ int dense_split(int n, int sms) {
   return s;
 }
 
+constexpr int kOrAndSparseMinN = 8192;
+
 // Defined with the SpGEMM host code below.
 int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, int* steps, bool* changed,
                            int* step_cfg, float* step_ms, cudaStream_t stream);
+int closure_sparse_opening_u8(int n, uint8_t* X, long long ldx, int max_iter, int* steps, bool* changed,
+                              cudaStream_t stream);
 
 // Closure steps enqueued in chunks without a host round trip per step.
 // changed[t] is written by step t; every kernel of step t+1 reads changed[t]
@@ -1220,6 +1224,19 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
   if (n == 0 || max_iter == 0) return SIMD2_OK;
   int rc = check_device();
   if (rc) return rc;
+  // From n = 8192 a dense INT8 step takes ~0.4 ms or more, so a sparse X is
+  // first squared as CSR SpGEMM steps (see closure_sparse_opening_t); smaller
+  // closures would spend more on the opening's host round trips than it saves.
+  int it0 = 0;
+  if (n >= kOrAndSparseMinN) {
+    bool ch = true;
+    if ((rc = closure_sparse_opening_u8(n, X, ldx, max_iter, &it0, &ch, stream))) return rc;
+    if (!ch || it0 == max_iter) {
+      if (iters_out) *iters_out = it0;
+      return ch ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
+    }
+    max_iter -= it0;
+  }
   // Workspace: [tensor-core operands][Xnew n x n bytes][change flag]
   const TcPlan plan = tc_plan_u8(n, n, n);
   const size_t x_off = align_up(plan.total, kAlign);
@@ -1248,11 +1265,9 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
   }
   if (cur != X) {
     SIMD2_CUDA_TRY(cudaMemcpy2DAsync(X, ldx, cur, ldcur, (size_t)n, n, cudaMemcpyDeviceToDevice, stream));
-  } else if (it == 0) {
-    // nothing ran
   }
   SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
-  if (iters_out) *iters_out = it;
+  if (iters_out) *iters_out = it0 + it;
   return changed ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
 }
 
@@ -1522,30 +1537,37 @@ int spgemm_fill(int op, int M, int N, int K, const int* ap, const int* aj, const
 }
 
 // FILL pass into a dense M x N matrix D (pitch ldd) that holds the identity.
+// (A 0/1 byte matrix D gets 1 at every touched column.)
+template <typename T>
 int spgemm_fill_dense(int op, int M, int N, int K, const int* ap, const int* aj, const float* av, int a_nnz,
                       const int* bp, const int* bj, const float* bv, int b_nnz, const int* cp, const int* cj,
-                      const float* cv, int c_nnz, float* D, long long ldd, uint8_t* ws, const SpPlan& plan,
+                      const float* cv, int c_nnz, T* D, long long ldd, uint8_t* ws, const SpPlan& plan,
                       cudaStream_t stream) {
   SpArgs a{};
   a.M = M, a.N = N, a.K = K, a.a_nnz = a_nnz, a.b_nnz = b_nnz, a.c_nnz = c_nnz;
   a.ap = ap, a.aj = aj, a.av = av, a.bp = bp, a.bj = bj, a.bv = bv, a.cp = cp, a.cj = cj, a.cv = cv;
-  a.dense = D, a.ldd = ldd;
+  if constexpr (std::is_same<T, uint8_t>::value) a.dense_u8 = D;
+  else a.dense = D;
+  a.ldd = ldd;
   a.acc = reinterpret_cast<float*>(ws + plan.acc_off);
   a.next_row = reinterpret_cast<int*>(ws + plan.ctr_off);
   SIMD2_CUDA_TRY(cudaMemsetAsync(a.next_row, 0, 4, stream));
   return spgemm_launch<false, true>(op, a, plan, stream);
 }
 
-// Sparse opening of a learned closure: while X is sparse, square it in CSR.
-// A step runs as a semiring SpGEMM when X holds at most n^2/32 entries, the
-// step forms at most n^3/256 products (sum over k of row count x column
-// count; at B200's rates of about 100 G products/s sparse and 17 T MAC/s
-// dense, that is under two thirds of a dense step's time).  A result with
-// more than n^2/32 entries goes straight into X and ends the opening.  X
-// (dense, pitch ldx) is rewritten when any step ran.  *steps: steps run; *changed: false when the last one changed
-// nothing.  Every step gives the dense step's bits (same contract, same order).
-int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, int* steps, bool* changed,
-                           int* step_cfg, float* step_ms, cudaStream_t stream) {
+// Sparse opening of a closure: while X is sparse, square it in CSR.
+// A step runs as a semiring SpGEMM when X holds at most n^2/32 entries and
+// the step forms at most max_products products (sum over k of row count x
+// column count).  A result with more than n^2/32 entries goes straight into
+// X and ends the opening.  X (pitch ldx) is rewritten when any step ran.
+// T = float: X holds values, absent = the add identity of op.  T = uint8_t:
+// X is a 0/1 matrix (or_and), squared as max_min over stored 1.0 values.
+// *steps: steps run; *changed: false when the last one changed nothing.
+// Every step gives the dense step's bits (same contract, same result).
+template <typename T>
+int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, unsigned long long max_products,
+                             int* steps, bool* changed, int* step_cfg, float* step_ms, cudaStream_t stream) {
+  constexpr bool kBool = std::is_same<T, uint8_t>::value;
   *steps = 0;
   *changed = true;
   if (!spgemm_op(op) || op == SIMD2_PLUS_MUL || max_iter <= 0 || n < 2) return SIMD2_OK;
@@ -1577,19 +1599,36 @@ int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter,
   int* counts = reinterpret_cast<int*>(ws + plan.cnt_off);
   int* flag = reinterpret_cast<int*>(ws + plan.flag_off);
   long long* tot = reinterpret_cast<long long*>(ws + plan.tot_off);
+  const int rows_grid = grid_for((long long)n * 32);
+  // X as a dense matrix again (ident / 0 everywhere first)
+  auto clear_x = [&]() -> int {
+    if constexpr (kBool) {
+      SIMD2_CUDA_TRY(cudaMemset2DAsync(X, (size_t)ldx, 0, (size_t)n, (size_t)n, stream));
+    } else {
+      fill_kernel<float><<<grid_for(nn2), 256, 0, stream>>>(X, ldx, n, n, ident);
+      count_launch();
+    }
+    return SIMD2_OK;
+  };
 
   // X -> CSR, when sparse enough
-  SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, 8, stream));
-  dense_row_count_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, n, X, ldx, ident, counts);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, 12, stream));
+  // flag[2]: a byte other than 0 / 1 -- the dense step rewrites it to 1 and
+  // counts that as a change, which a structure-only step would not see
+  if constexpr (kBool) dense_row_count_u8_kernel<<<rows_grid, 256, 0, stream>>>(n, n, X, ldx, counts, flag + 2);
+  else dense_row_count_kernel<<<rows_grid, 256, 0, stream>>>(n, n, X, ldx, ident, counts);
   offsets_scan_kernel<<<1, 1024, 0, stream>>>(counts, n, rp[0], flag + 1, tot);
   count_launch();
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   long long nnz = 0;
+  int non01 = 0;
   SIMD2_CUDA_TRY(cudaMemcpyAsync(&nnz, tot, 8, cudaMemcpyDeviceToHost, stream));
+  SIMD2_CUDA_TRY(cudaMemcpyAsync(&non01, flag + 2, 4, cudaMemcpyDeviceToHost, stream));
   SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
-  if (nnz > cap) return SIMD2_OK;
-  dense_to_csr_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, n, X, ldx, ident, rp[0], cj[0], cv[0]);
+  if (nnz > cap || non01) return SIMD2_OK;
+  if constexpr (kBool) dense_to_csr_u8_kernel<<<rows_grid, 256, 0, stream>>>(n, n, X, ldx, rp[0], cj[0], cv[0]);
+  else dense_to_csr_kernel<<<rows_grid, 256, 0, stream>>>(n, n, X, ldx, ident, rp[0], cj[0], cv[0]);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
 
@@ -1598,7 +1637,6 @@ int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter,
     for (auto& e : ev) SIMD2_CUDA_TRY(cudaEventCreate(&e));
   int cur = 0, it = 0;
   bool ch = true, in_x = false;  // in_x: the last step wrote X itself
-  const unsigned long long max_products = (unsigned long long)nn2 * (unsigned long long)n / 256ull;
   while (ch && it < max_iter) {
     SIMD2_CUDA_TRY(cudaMemsetAsync(colcnt, 0, (size_t)n * 4, stream));
     SIMD2_CUDA_TRY(cudaMemsetAsync(prod, 0, 8, stream));
@@ -1617,41 +1655,34 @@ int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter,
     rc = spgemm_count(op, n, n, n, rp[cur], cj[cur], (int)nnz, rp[cur], cj[cur], (int)nnz, rp[cur], cj[cur], (int)nnz,
                       rp[nx], &nn, ws, plan, stream);
     if (rc && rc != kSpOverflow) return rc;
-    if (rc == kSpOverflow || nn > cap) {
+    const bool to_x = rc == kSpOverflow || nn > cap;
+    if (to_x) {
       // the result is too dense for CSR: this step writes it straight into X
       // (more entries than X had, so it changed) and the dense loop goes on
-      fill_kernel<float><<<grid_for(nn2), 256, 0, stream>>>(X, ldx, n, n, ident);
-      count_launch();
+      if ((rc = clear_x())) return rc;
       SIMD2_CUDA_TRY(cudaGetLastError());
-      rc = spgemm_fill_dense(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz,
-                             rp[cur], cj[cur], cv[cur], (int)nnz, X, ldx, ws, plan, stream);
+      rc = spgemm_fill_dense<T>(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur],
+                                (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz, X, ldx, ws, plan, stream);
       if (rc) return rc;
-      if (step_ms) {
-        cudaEventRecord(ev[1], stream);
-        cudaEventSynchronize(ev[1]);
-        cudaEventElapsedTime(&step_ms[it], ev[0], ev[1]);
-      }
-      if (step_cfg) step_cfg[it] = kNumConfigs;
-      it++;
       in_x = true;
       ch = true;
-      break;
-    }
-    rc = spgemm_fill(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur],
-                     cj[cur], cv[cur], (int)nnz, rp[nx], cj[nx], cv[nx], nn, ws, plan, stream);
-    if (rc) return rc;
-    // X' holds X's structure (C = X) plus new entries: equal counts mean equal structure
-    if (nn != nnz) {
-      ch = true;
     } else {
-      SIMD2_CUDA_TRY(cudaMemsetAsync(flag + 2, 0, 4, stream));
-      values_differ_kernel<<<grid_for(std::max(nn, 1LL)), 256, 0, stream>>>(cv[cur], cv[nx], nn, flag + 2);
-      count_launch();
-      SIMD2_CUDA_TRY(cudaGetLastError());
-      int h = 0;
-      SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag + 2, 4, cudaMemcpyDeviceToHost, stream));
-      SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
-      ch = h != 0;
+      rc = spgemm_fill(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur],
+                       cj[cur], cv[cur], (int)nnz, rp[nx], cj[nx], cv[nx], nn, ws, plan, stream);
+      if (rc) return rc;
+      // X' holds X's structure (C = X) plus new entries: equal counts mean equal structure
+      if (nn != nnz) {
+        ch = true;
+      } else {
+        SIMD2_CUDA_TRY(cudaMemsetAsync(flag + 2, 0, 4, stream));
+        values_differ_kernel<<<grid_for(std::max(nn, 1LL)), 256, 0, stream>>>(cv[cur], cv[nx], nn, flag + 2);
+        count_launch();
+        SIMD2_CUDA_TRY(cudaGetLastError());
+        int h = 0;
+        SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag + 2, 4, cudaMemcpyDeviceToHost, stream));
+        SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
+        ch = h != 0;
+      }
     }
     if (step_ms) {
       cudaEventRecord(ev[1], stream);
@@ -1660,15 +1691,16 @@ int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter,
     }
     if (step_cfg) step_cfg[it] = kNumConfigs;  // the sparse step
     it++;
+    if (to_x) break;
     cur = nx;
     nnz = nn;
   }
   if (step_ms)
     for (auto& e : ev) cudaEventDestroy(e);
   if (it > 0 && !in_x) {
-    fill_kernel<float><<<grid_for(nn2), 256, 0, stream>>>(X, ldx, n, n, ident);
-    csr_scatter_kernel<<<grid_for((long long)n * 32), 256, 0, stream>>>(n, rp[cur], cj[cur], cv[cur], X, ldx);
-    count_launch();
+    if ((rc = clear_x())) return rc;
+    if constexpr (kBool) csr_scatter_u8_kernel<<<rows_grid, 256, 0, stream>>>(n, rp[cur], cj[cur], X, ldx);
+    else csr_scatter_kernel<<<rows_grid, 256, 0, stream>>>(n, rp[cur], cj[cur], cv[cur], X, ldx);
     count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
   }
@@ -1676,6 +1708,25 @@ int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter,
   *steps = it;
   *changed = ch;
   return SIMD2_OK;
+}
+
+// The learned float closure's opening: a step under n^3/256 products (at
+// B200's rates of about 100 G products/s sparse and 17 T MAC/s on the
+// CUDA-core dense kernel, under two thirds of a dense step's time).
+int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, int* steps, bool* changed,
+                           int* step_cfg, float* step_ms, cudaStream_t stream) {
+  const unsigned long long nn2 = (unsigned long long)n * (unsigned long long)n;
+  return closure_sparse_opening_t<float>(op, n, X, ldx, max_iter, nn2 * (unsigned long long)n / 256ull, steps, changed,
+                                         step_cfg, step_ms, stream);
+}
+
+// The or_and closure's opening: the dense step runs on the INT8 tensor cores
+// (about 1.3 P MAC/s), so a sparse step must stay under n^3/16384 products.
+int closure_sparse_opening_u8(int n, uint8_t* X, long long ldx, int max_iter, int* steps, bool* changed,
+                              cudaStream_t stream) {
+  const unsigned long long nn2 = (unsigned long long)n * (unsigned long long)n;
+  return closure_sparse_opening_t<uint8_t>(SIMD2_MAX_MIN, n, X, ldx, max_iter, nn2 * (unsigned long long)n / 16384ull,
+                                           steps, changed, nullptr, nullptr, stream);
 }
 
 }  // namespace

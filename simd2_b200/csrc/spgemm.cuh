@@ -84,6 +84,7 @@ struct SpArgs {
   int* dj;        // FILL: output columns
   float* dv;      // FILL: output values
   float* dense;   // FILL into a dense matrix (DENSE): D rows of pitch ldd, prefilled with the identity
+  uint8_t* dense_u8;  // or, for a Boolean closure, a 0/1 byte matrix prefilled with 0 (touched -> 1)
   long long ldd;
   int* row_nnz;   // COUNT: per-row nonzero count
   float* acc;     // gridDim.x * N floats of scratch (FILL)
@@ -239,13 +240,16 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
       if (threadIdx.x == 0) a.row_nnz[r] = total;
     } else if constexpr (DENSE) {
       // the touched columns straight into the dense row (the rest holds the identity)
-      float* drow = a.dense + (long long)r * a.ldd;
+      float* drow = a.dense_u8 ? nullptr : a.dense + (long long)r * a.ldd;
+      uint8_t* brow = a.dense_u8 ? a.dense_u8 + (long long)r * a.ldd : nullptr;
       for (int w = threadIdx.x; w < words; w += kSpThreads) {
         uint32_t bits = bitmap[w];
         while (bits) {
           const int j = (w << 5) + __ffs(bits) - 1;
           bits &= bits - 1;
-          drow[j] = result(j);
+          const float v = result(j);
+          if (brow) brow[j] = 1;
+          else drow[j] = v;
         }
       }
     } else {
@@ -389,6 +393,73 @@ __global__ void dense_row_count_kernel(int rows, int cols, const float* __restri
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     if (lane == 0) counts[r] = c;
   }
+}
+
+// Nonzero bytes of each row of a byte matrix; one warp per row, 4 bytes per
+// lane.  *non01 |= 1 when a byte is neither 0 nor 1.
+__global__ void dense_row_count_u8_kernel(int rows, int cols, const uint8_t* __restrict__ X, long long ld,
+                                          int* __restrict__ counts, int* __restrict__ non01) {
+  const int lane = threadIdx.x & 31;
+  int bad = 0;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
+    const uint8_t* xr = X + (long long)r * ld;
+    int c = 0;
+    for (int j = 4 * lane; j < cols; j += 128)
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int v = j + e < cols ? xr[j + e] : 0;
+        c += v != 0;
+        bad |= v > 1;
+      }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) counts[r] = c;
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(non01, 1);
+}
+
+// CSR (values 1.0f) <- the nonzero bytes of a 0/1 byte matrix at the offsets
+// rp, increasing column; one warp per row, 4 bytes per lane.
+__global__ void dense_to_csr_u8_kernel(int rows, int cols, const uint8_t* __restrict__ X, long long ld,
+                                       const int* __restrict__ rp, int* __restrict__ cj, float* __restrict__ cv) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
+    const uint8_t* xr = X + (long long)r * ld;
+    int pos = rp[r];
+    for (int j0 = 0; j0 < cols; j0 += 128) {
+      const int j = j0 + 4 * lane;
+      bool f[4];
+      int c = 0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        f[e] = j + e < cols && xr[j + e] != 0;
+        c += f[e];
+      }
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      int at = pos + incl - c;
+#pragma unroll
+      for (int e = 0; e < 4; e++)
+        if (f[e]) {
+          cj[at] = j + e;
+          cv[at] = 1.0f;
+          at++;
+        }
+      pos += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+}
+
+// Byte matrix entries <- 1 at the CSR's stored columns (the rest was zeroed before).
+__global__ void csr_scatter_u8_kernel(int rows, const int* __restrict__ rp, const int* __restrict__ cj,
+                                      uint8_t* __restrict__ X, long long ld) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5)
+    for (int e = rp[r] + lane; e < rp[r + 1]; e += 32) X[(long long)r * ld + cj[e]] = 1;
 }
 
 // CSR <- dense rows (entries that are not the identity, increasing column),

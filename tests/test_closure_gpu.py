@@ -104,3 +104,44 @@ def test_or_and_closure(cuda):
     it = s2.closure("or_and", X)
     assert it == it_want
     np.testing.assert_array_equal(X.cpu().numpy(), want)
+
+
+def _orand_dense_closure(X, max_iter=64):
+    """The dense INT8 squaring step repeated to the fixed point (the panel
+    step over all rows), as the reference's closure loop runs it."""
+    changed = torch.zeros(1, dtype=torch.int32, device=X.device)
+    out = torch.empty_like(X)
+    it = 0
+    while it < max_iter:
+        it += 1
+        changed.zero_()
+        s2.closure_panel_step("or_and", X, X, out, changed)
+        X, out = out, X
+        if int(changed.item()) == 0:
+            break
+    return X, it
+
+
+@pytest.mark.parametrize("case", ["er_deg2", "cycles", "non01"])
+def test_or_and_closure_sparse_opening(cuda, case):
+    """From n = 8192 the or_and closure squares a sparse X as CSR SpGEMM
+    steps before the INT8 tensor-core steps: same bits and step count as the
+    dense loop ('cycles' converges while still sparse; 'non01' holds bytes
+    other than 0 / 1, which the dense step rewrites, so the opening stands
+    aside)."""
+    n = 8192
+    rng = np.random.default_rng(8192)
+    X = torch.zeros((n, n), dtype=torch.uint8, device=cuda)
+    if case == "cycles":
+        i = torch.arange(n, device=cuda)
+        X[i, (i // 8) * 8 + (i + 1) % 8] = 1
+    else:
+        m = 2 * n
+        X[torch.from_numpy(rng.integers(0, n, m)).to(cuda), torch.from_numpy(rng.integers(0, n, m)).to(cuda)] = 1
+    X.fill_diagonal_(1)
+    if case == "non01":
+        X[5, 7] = 2
+    want, it_want = _orand_dense_closure(X.clone())
+    it = s2.closure("or_and", X)
+    assert it == it_want
+    assert torch.equal(X, want)
