@@ -530,7 +530,8 @@ inline bool use_tc2(int M, int N) {
 // SM-pair launch: clusters of 2 CTAs, one pair per pair of SMs at most.
 template <int KIND>
 int launch_tc2(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
-               const CUtensorMap& b1, const TcEpilogue& ep, cudaStream_t stream) {
+               const CUtensorMap& b1, const CUtensorMap& bh0, const CUtensorMap& bh1, const TcEpilogue& ep,
+               cudaStream_t stream) {
   auto kern = tc_gemm2_kernel<KIND>;
   const size_t smem = tc2_smem_bytes<KIND>();
   static int max_pairs[64] = {};
@@ -561,7 +562,7 @@ int launch_tc2(int M, int N, int K, const CUtensorMap& a0, const CUtensorMap& a1
   lc.gridDim = dim3(2 * pairs);
   auto* ev = prof_slot(2LL * M * N * K, kProfTensor);
   if (ev) cudaEventRecord(ev->first, stream);
-  SIMD2_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, a0, a1, b0, b1, M, N, K, ep, tiles_m, tiles_n));
+  SIMD2_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, a0, a1, b0, b1, bh0, bh1, M, N, K, ep, tiles_m, tiles_n));
   count_launch();
   if (ev) cudaEventRecord(ev->second, stream);
   SIMD2_CUDA_TRY(cudaGetLastError());
@@ -642,6 +643,12 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   if ((rc = make_map_2d(&ma1, BF, 2, alo, M, Kp, Kp, BX, kTcBM, SW))) return rc;
   if ((rc = make_map_2d(&mb0, BF, 2, ws + plan.b0, N, Kp, Kp, BX, brows, SW))) return rc;
   if ((rc = make_map_2d(&mb1, BF, 2, ws + plan.b1, N, Kp, Kp, BX, brows, SW))) return rc;
+  // the pair kernel's half tiles stage 64 rows of B^T per CTA
+  CUtensorMap mbh0 = mb0, mbh1 = mb1;
+  if (pair) {
+    if ((rc = make_map_2d(&mbh0, BF, 2, ws + plan.b0, N, Kp, Kp, BX, 64, SW))) return rc;
+    if ((rc = make_map_2d(&mbh1, BF, 2, ws + plan.b1, N, Kp, Kp, BX, 64, SW))) return rc;
+  }
   TcEpilogue ep{};
   ep.op = op;
   ep.do_epilogue = do_epilogue;
@@ -657,7 +664,7 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   ep.ldb32 = ldb;
   ep.K = K;
   ep.band = kMinusSquareBand;
-  if (pair) return launch_tc2<0>(M, N, K, ma0, ma1, mb0, mb1, ep, stream);
+  if (pair) return launch_tc2<0>(M, N, K, ma0, ma1, mb0, mb1, mbh0, mbh1, ep, stream);
   return launch_tc<0>(M, N, K, ma0, ma1, mb0, mb1, ep, stream);
 }
 
@@ -681,6 +688,8 @@ int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, 
   const bool pair = use_tc2(M, N);
   if ((rc = make_map_2d(&ma, U8, 1, a8, M, Kp, Kp, 128, kTcBM, SW))) return rc;
   if ((rc = make_map_2d(&mb, U8, 1, b8, N, Kp, Kp, 128, pair ? 128 : kTcBN, SW))) return rc;
+  CUtensorMap mbh = mb;  // the pair kernel's half tiles stage 64 rows of B^T per CTA
+  if (pair && (rc = make_map_2d(&mbh, U8, 1, b8, N, Kp, Kp, 128, 64, SW))) return rc;
   TcEpilogue ep{};
   ep.op = SIMD2_OR_AND;
   ep.do_epilogue = do_epilogue;
@@ -690,7 +699,7 @@ int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, 
   ep.ldd = ldd;
   ep.out_u8 = sizeof(T) == 1;
   ep.changed = changed;
-  if (pair) return launch_tc2<1>(M, N, K, ma, ma, mb, mb, ep, stream);
+  if (pair) return launch_tc2<1>(M, N, K, ma, ma, mb, mb, mbh, mbh, ep, stream);
   return launch_tc<1>(M, N, K, ma, ma, mb, mb, ep, stream);
 }
 

@@ -196,12 +196,13 @@ __device__ __forceinline__ float exact_minus_square(const float* a, const float*
   return s;
 }
 
-// Epilogue of one 128 x 256 tile for the 32 rows of one warp: lane l holds
-// row row0 + l of the accumulator in TMEM at trow (lane quadrant and column
-// base included).  Sets changed when an or_and output differs from C.
+// Epilogue of one 128 x ncols tile (ncols = 256, or 128 for a split tail
+// tile) for the 32 rows of one warp: lane l holds row row0 + l of the
+// accumulator in TMEM at trow (lane quadrant and column base included).  Sets
+// changed when an or_and output differs from C.
 template <int KIND>
 __device__ __forceinline__ void tc_tile_epilogue(const TcEpilogue& ep, int M, int N, int n0, int row0, uint32_t trow,
-                                                 uint32_t* epi_tile, int lane, int& changed) {
+                                                 uint32_t* epi_tile, int lane, int& changed, int ncols = kTcBN) {
   if constexpr (KIND == 1) {
     // or_and: 32 flags of one row are 32 contiguous bytes (u8) or 128 bytes
     // (i32), so each lane writes its own row with 16-byte vector stores.
@@ -212,7 +213,7 @@ __device__ __forceinline__ void tc_tile_epilogue(const TcEpilogue& ep, int M, in
                         (!ep.do_epilogue ||
                          (((ep.ldc * esz) % 16 == 0) && ((reinterpret_cast<uintptr_t>(ep.C) & 15) == 0)));
 #pragma unroll 1
-    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+    for (int c0 = 0; c0 < ncols; c0 += 32) {
       uint32_t r[32];
       tmem_ld32(trow + c0, r);  // all lanes take part (sync.aligned)
       if (row >= M) continue;
@@ -299,7 +300,7 @@ __device__ __forceinline__ void tc_tile_epilogue(const TcEpilogue& ep, int M, in
     const float na_lane = (msq && row0 + lane < M) ? ep.norm_a[row0 + lane] : 0.f;
     const int rows_here = min(32, M - row0);
 #pragma unroll 1
-    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+    for (int c0 = 0; c0 < ncols; c0 += 32) {
       const int col = n0 + c0 + lane;
       const bool col_ok = col < N;
       float cv[32];

@@ -21,6 +21,12 @@
 //                    barrier (remote arrive from the odd CTA).
 // Every wait is bounded; every path ends at one cluster barrier, so neither
 // CTA leaves while its peer may still signal it.
+//
+// Tail split: with T tiles on P pairs the last round holds r = T mod P tiles.
+// When 2r <= P those r tiles run as 2r half tiles of 256 x 128 (MMA N = 128;
+// each CTA loads a 64-row B box through the tmBh maps), so the last round
+// takes about half a tile's time: 4096^2 on 74 pairs is 3.5 rounds of work
+// instead of 4.
 #pragma once
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -40,10 +46,11 @@ template <int KIND>
 constexpr size_t tc2_smem_bytes() {
   return (size_t)kTc2Stages * tc2_stage_bytes<KIND>() + (size_t)kTcEpiWarps * 32 * 33 * 4 + 1024 + 256;
 }
-// instruction descriptor: TcCfg's with M = 256
+// instruction descriptor: TcCfg's with M = 256 and N = n
 template <int KIND>
-__host__ __device__ constexpr uint32_t tc2_idesc() {
-  return (TcCfg<KIND>::kIdesc & ~(0x1Fu << 24)) | ((uint32_t)(kTc2BM >> 4) << 24);
+__host__ __device__ constexpr uint32_t tc2_idesc(int n = kTcBN) {
+  return (TcCfg<KIND>::kIdesc & ~(0x1Fu << 24) & ~(0x3Fu << 17)) | ((uint32_t)(kTc2BM >> 4) << 24) |
+         ((uint32_t)(n >> 3) << 17);
 }
 
 __device__ __forceinline__ uint32_t cluster_rank2() {
@@ -74,8 +81,8 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* m
       : "memory");
 }
 template <int KIND>
-__device__ __forceinline__ void tc2_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-  constexpr uint32_t idesc = tc2_idesc<KIND>();
+__device__ __forceinline__ void tc2_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate,
+                                        uint32_t idesc) {
   if constexpr (KIND == 0) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -104,7 +111,8 @@ __device__ __forceinline__ void tc2_commit_both(uint64_t* bar) {
 template <int KIND>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_gemm2_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1,
-                    const __grid_constant__ CUtensorMap tmB0, const __grid_constant__ CUtensorMap tmB1, int M, int N,
+                    const __grid_constant__ CUtensorMap tmB0, const __grid_constant__ CUtensorMap tmB1,
+                    const __grid_constant__ CUtensorMap tmBh0, const __grid_constant__ CUtensorMap tmBh1, int M, int N,
                     int K, TcEpilogue ep, int tiles_m, int tiles_n) {
   using Cfg = TcCfg<KIND>;
   constexpr int S = kTc2Stages;
@@ -136,6 +144,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     m0 = (first_m + local % gsize) * kTc2BM;
     n0 = (local / gsize) * kTcBN;
   };
+  // work items: the first `whole` tiles, then the tail's tiles as half tiles
+  const int rem = tiles % pairs;
+  const bool split_tail = rem > 0 && 2 * rem <= pairs;
+  const int whole = split_tail ? tiles - rem : tiles;
+  const int items = split_tail ? whole + 2 * rem : tiles;
+  auto item_origin = [&](int w, int& m0, int& n0, int& ncols) {
+    if (w < whole) {
+      tile_origin(w, m0, n0);
+      ncols = kTcBN;
+    } else {
+      const int h = w - whole;
+      tile_origin(whole + (h >> 1), m0, n0);
+      n0 += (h & 1) * (kTcBN / 2);
+      ncols = kTcBN / 2;
+    }
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; s++) {
@@ -165,12 +189,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // ---------------- TMA producer of this CTA's halves ----------------
       prefetch_tensormap(&tmA0);
       prefetch_tensormap(&tmB0);
+      prefetch_tensormap(&tmBh0);
       int j = 0;
       bool ok = true;
-      for (int t = pair; t < tiles && ok; t += pairs) {
-        int m0, n0;
-        tile_origin(t, m0, n0);
-        const int ma = m0 + (int)rank * 128, nb = n0 + (int)rank * 128;
+      for (int t = pair; t < items && ok; t += pairs) {
+        int m0, n0, ncols;
+        item_origin(t, m0, n0, ncols);
+        // this CTA's ncols/2 rows of B^T: a 128-row box, or 64 rows for a half tile
+        const bool half = ncols != kTcBN;
+        const CUtensorMap* mb0 = half ? &tmBh0 : &tmB0;
+        const CUtensorMap* mb1 = half ? &tmBh1 : &tmB1;
+        const uint32_t bytes = 2 * (Cfg::kNumA * kHalf + Cfg::kNumB * (half ? kHalf / 2 : kHalf));
+        const int ma = m0 + (int)rank * 128, nb = n0 + (int)rank * (ncols / 2);
         for (int kt = 0; kt < ktiles; kt++, j++) {
           const int s = j % S;
           if (!mbar_wait(&empty[s], ((j / S) & 1) ^ 1)) {
@@ -178,15 +208,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             ok = false;
             break;
           }
-          if (rank == 0) mbar_arrive_expect_tx(&full[s], 2 * kStage);
+          if (rank == 0) mbar_arrive_expect_tx(&full[s], bytes);
           const uint32_t bar0 = map_to_rank(&full[s], 0);
           uint8_t* st = smem + s * kStage;
           const int kx = kt * Cfg::kBK;
           tma_load_2d_pair(st, &tmA0, bar0, kx, ma);
           if constexpr (Cfg::kNumA == 2) tma_load_2d_pair(st + kHalf, &tmA1, bar0, kx, ma);
           uint8_t* sb = st + Cfg::kNumA * kHalf;
-          tma_load_2d_pair(sb, &tmB0, bar0, kx, nb);
-          if constexpr (Cfg::kNumB == 2) tma_load_2d_pair(sb + kHalf, &tmB1, bar0, kx, nb);
+          tma_load_2d_pair(sb, mb0, bar0, kx, nb);
+          if constexpr (Cfg::kNumB == 2) tma_load_2d_pair(sb + kHalf, mb1, bar0, kx, nb);
         }
       }
     }
@@ -197,8 +227,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int j = 0;
       bool ok = true;
       int lt = 0;
-      for (int t = pair; t < tiles && ok; t += pairs, lt++) {
+      for (int t = pair; t < items && ok; t += pairs, lt++) {
         const int acc = lt & 1;
+        const uint32_t idesc = t < whole ? tc2_idesc<KIND>() : tc2_idesc<KIND>(kTcBN / 2);
         if (!mbar_wait(&acc_empty[acc], ((lt >> 1) & 1) ^ 1)) {
           report_timeout(124);
           break;
@@ -222,11 +253,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const uint32_t koff = ks * Cfg::kKStep * (KIND == 0 ? 2 : 1);
             const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
             if constexpr (KIND == 0) {
-              tc2_mma<0>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
-              tc2_mma<0>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b1 + koff, RB), 1u);
-              tc2_mma<0>(d, umma_desc_swizzled(a1 + koff, RB), umma_desc_swizzled(b0 + koff, RB), 1u);
+              tc2_mma<0>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0, idesc);
+              tc2_mma<0>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b1 + koff, RB), 1u, idesc);
+              tc2_mma<0>(d, umma_desc_swizzled(a1 + koff, RB), umma_desc_swizzled(b0 + koff, RB), 1u, idesc);
             } else {
-              tc2_mma<1>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0);
+              tc2_mma<1>(d, umma_desc_swizzled(a0 + koff, RB), umma_desc_swizzled(b0 + koff, RB), acc0, idesc);
             }
           }
           tc2_commit_both(&empty[s]);  // stage s free in both CTAs once these MMAs have read it
@@ -242,7 +273,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint32_t* epi_tile = epi_smem + (warp - 2) * (32 * 33);
     bool ok = true;
     int lt = 0;
-    for (int t = pair; t < tiles; t += pairs, lt++) {
+    for (int t = pair; t < items; t += pairs, lt++) {
       const int acc = lt & 1;
       if (ok && !mbar_wait(&acc_full[acc], (lt >> 1) & 1)) {
         report_timeout(123);
@@ -251,12 +282,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) break;
       tc_fence_after();
-      int m0, n0;
-      tile_origin(t, m0, n0);
+      int m0, n0, ncols;
+      item_origin(t, m0, n0, ncols);
       const uint32_t trow = tmem + acc * kTcBN + ((uint32_t)(quad * 32) << 16);
       const int row0 = m0 + (int)rank * 128 + quad * 32;
       int changed = 0;
-      tc_tile_epilogue<KIND>(ep, M, N, n0, row0, trow, epi_tile, lane, changed);
+      tc_tile_epilogue<KIND>(ep, M, N, n0, row0, trow, epi_tile, lane, changed, ncols);
       if (ep.changed && KIND == 1) {
         if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
       }

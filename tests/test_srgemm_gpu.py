@@ -214,11 +214,14 @@ def test_selection_fp16_and_fp32_paths(cuda, op):
 
 
 @pytest.mark.parametrize("op", ["plus_mul", "minus_square", "or_and"])
-@pytest.mark.parametrize("shape", [(1024, 1024, 2048), (4096, 4096, 256), (130, 300, 700)])
+@pytest.mark.parametrize("shape", [(1024, 1024, 2048), (4096, 4096, 256), (130, 300, 700), (4096, 1200, 512),
+                                   (2560, 2560, 384)])
 def test_tensor_core_partial_rounds(cuda, op, shape):
     """Shapes that leave the persistent tensor-core grid partly idle (fewer
-    tiles than SMs; a 68-tile last round of 4096 x 4096; ragged edges): the
-    oracle's result (or_and exactly) on rows sampled across the output."""
+    tiles than SMs; the last round of 4096 x 4096, 4096 x 1200 and 2560 x 2560
+    on the SM-pair kernel, run as 256 x 128 half tiles, one of them past a
+    ragged column edge; ragged edges): the oracle's result (or_and exactly) on
+    rows sampled across the output."""
     M, N, K = shape
     a, b, c = datagen.semiring_operands(op, M, N, K, seed=M + K)
     A, B, C = (torch.from_numpy(x).to(cuda) for x in (a, b, c))
