@@ -1362,6 +1362,9 @@ int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ld
       a_pitch = Kp;
     }
     SIMD2_CUDA_TRY(cudaGetLastError());
+    // 16-byte loads in the witness re-scan: X's rows and X^T's rows aligned
+    const int vec4 = (reinterpret_cast<uintptr_t>(Xc) % 16 == 0) && (ldc % 4 == 0) &&
+                     (reinterpret_cast<uintptr_t>(XT) % 16 == 0) && (n % 4 == 0);
     CUtensorMap mA, mB;
     if ((rc = make_map_f32(&mA, a_base, n, pack_a ? Kp : n, a_pitch, kBK, kBM, CU_TENSOR_MAP_SWIZZLE_128B, true)))
       return rc;
@@ -1379,7 +1382,8 @@ int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ld
       configured[dev] = true;                                                                                         \
     }                                                                                                                 \
     pred_fast_kernel<OPV><<<tiles * tiles, kSimtThreads, smem, stream>>>(                                             \
-        mA, mB, n, Xc, ldc, XT, n, bufp[cur], ldp_[cur], bufx[nx], ldx_[nx], bufp[nx], ldp_[nx], flag, tiles, tiles); \
+        mA, mB, n, Xc, ldc, XT, n, bufp[cur], ldp_[cur], bufx[nx], ldx_[nx], bufp[nx], ldp_[nx], flag, tiles, tiles,   \
+        vec4);                                                                                                         \
     break;                                                                                                            \
   }
       SIMD2_PRED_CASE(SIMD2_MIN_PLUS)

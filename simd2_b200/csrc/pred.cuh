@@ -25,6 +25,8 @@
 // k-tile for each output whose value improves (X[i][k] from the row, X[k][j]
 // from a transposed copy, both contiguous) and takes the first one equal to
 // best -- the same IEEE operation on the same operands, so the same bits.
+// The re-scan loads all 32 operand pairs before comparing (one memory round
+// trip per output instead of up to 32 dependent ones).
 #pragma once
 #include "common.cuh"
 #include "srgemm_simt.cuh"
@@ -82,6 +84,32 @@ constexpr size_t pred_smem_bytes() {
   return simt_smem_bytes(kPredStages) + (size_t)kBM * kPredRecStride * sizeof(uint16_t);
 }
 
+// The lowest k in [k0, k0 + 32) with X[i][k] (x) X[k][j] == b, or -1; xr and
+// tr point at X[i][k0] and X^T[j][k0].  All 32 operand pairs are loaded before
+// the compares (16-byte loads when vec4 and the k-tile is whole), so an output
+// costs one memory round trip.  One copy of the code for all call sites.
+template <int OP>
+__device__ __noinline__ int pred_witness(const float* __restrict__ xr, const float* __restrict__ tr, int k0, int n,
+                                         float b, int vec4) {
+  using O = PredOps<OP>;
+  uint32_t hit = 0;
+  if (vec4 && k0 + kBK <= n) {
+#pragma unroll
+    for (int q = 0; q < kBK / 4; q++) {
+      const float4 x4 = __ldg(reinterpret_cast<const float4*>(xr) + q);
+      const float4 t4 = __ldg(reinterpret_cast<const float4*>(tr) + q);
+      hit |= ((uint32_t)(O::mul(x4.x, t4.x) == b) << (4 * q)) | ((uint32_t)(O::mul(x4.y, t4.y) == b) << (4 * q + 1)) |
+             ((uint32_t)(O::mul(x4.z, t4.z) == b) << (4 * q + 2)) |
+             ((uint32_t)(O::mul(x4.w, t4.w) == b) << (4 * q + 3));
+    }
+  } else {
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk++)
+      if (k0 + kk < n && O::mul(__ldg(xr + kk), __ldg(tr + kk)) == b) hit |= 1u << kk;
+  }
+  return hit ? k0 + __ffs(hit) - 1 : -1;
+}
+
 // One predecessor-tracking squaring step on a 128 x 128 output tile per CTA:
 // X, P (pitch ldx, ldp) -> Xn, Pn (pitch ldxn, ldpn).  tmA reads X in k-tiles
 // (NaN beyond n), tmB the k-pair interleaved copy of X, XT is X transposed
@@ -92,7 +120,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
                      const float* __restrict__ X, long long ldx, const float* __restrict__ XT, long long ldt,
                      const int32_t* __restrict__ P, long long ldp, float* __restrict__ Xn, long long ldxn,
                      int32_t* __restrict__ Pn, long long ldpn, int* __restrict__ changed, int tiles_m,
-                     int tiles_n) {
+                     int tiles_n, int vec4) {
   using O = PredOps<OP>;
   constexpr int STAGES = kPredStages;
   extern __shared__ uint8_t smem_raw[];
@@ -230,15 +258,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
       int32_t pv;
       if (O::better(b, cv)) {
         const int k0 = (int)rec[(ty + 16 * ii) * kPredRecStride + cl] * kBK;
-        const int k1 = min(k0 + kBK, n);
-        const float* xr = X + (long long)i * ldx;
-        const float* tr = XT + (long long)col * ldt;
-        int ks = -1;
-        for (int k = k0; k < k1; k++)
-          if (O::mul(xr[k], tr[k]) == b) {
-            ks = k;
-            break;
-          }
+        int ks = pred_witness<OP>(X + (long long)i * ldx + k0, XT + (long long)col * ldt + k0, k0, n, b, vec4);
         if (ks < 0) {
           // cannot happen with the precondition (no NaN, no -0.0): the
           // product that set best is re-formed with the same operation
