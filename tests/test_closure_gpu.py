@@ -145,3 +145,18 @@ def test_or_and_closure_sparse_opening(cuda, case):
     it = s2.closure("or_and", X)
     assert it == it_want
     assert torch.equal(X, want)
+
+
+def test_or_and_closure_opening_step_cap(cuda):
+    """max_iter = 2 inside the or_and closure's sparse opening: NotConverged and
+    the dense loop's X after two squarings."""
+    n = 8192
+    rng = np.random.default_rng(3)
+    X = torch.zeros((n, n), dtype=torch.uint8, device=cuda)
+    m = 2 * n
+    X[torch.from_numpy(rng.integers(0, n, m)).to(cuda), torch.from_numpy(rng.integers(0, n, m)).to(cuda)] = 1
+    X.fill_diagonal_(1)
+    want, _ = _orand_dense_closure(X.clone(), max_iter=2)
+    with pytest.raises(s2.NotConverged):
+        s2.closure("or_and", X, max_iter=2)
+    assert torch.equal(X, want)

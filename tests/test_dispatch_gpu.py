@@ -165,3 +165,18 @@ def test_learned_sparse_opening_identical(cuda, case):
     Xc = torch.from_numpy(x.copy()).to(cuda)
     assert s2.closure_ex("min_plus", Xc, dispatch="learned", mlp_params=params) == ra["iters"]
     assert torch.equal(Xa.view(torch.int32), Xc.view(torch.int32))
+
+
+@pytest.mark.parametrize("steps", [1, 2])
+def test_learned_opening_step_cap(cuda, steps):
+    """max_iter reached inside the sparse opening: NotConverged, and X holds
+    exactly the dense path's X after the same number of squarings."""
+    x = datagen.rmat_graph(4096, 4.0, seed=31)
+    params = torch.randn(costmodel.param_count(), generator=torch.Generator().manual_seed(2)).to(cuda)
+    Xa = torch.from_numpy(x.copy()).to(cuda)
+    Xb = torch.from_numpy(x.copy()).to(cuda)
+    with pytest.raises(s2.NotConverged):
+        s2.closure_ex("min_plus", Xa, dispatch="dense", max_iter=steps)
+    with pytest.raises(s2.NotConverged):
+        s2.closure_ex("min_plus", Xb, dispatch="learned", mlp_params=params, max_iter=steps)
+    assert torch.equal(Xa.view(torch.int32), Xb.view(torch.int32))
