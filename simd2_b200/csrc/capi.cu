@@ -48,17 +48,17 @@ int check_device() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return SIMD2_ERR_NO_DEVICE;
   static std::mutex mu;
-  static std::map<int, int> verdict;
+  static std::map<int, int> checked;
   std::lock_guard<std::mutex> lk(mu);
-  auto it = verdict.find(dev);
-  if (it != verdict.end()) return it->second;
+  auto it = checked.find(dev);
+  if (it != checked.end()) return it->second;
   int major = 0, minor = 0;
   int rc = SIMD2_OK;
   if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess || major != 10 ||
       minor != 0)
     rc = SIMD2_ERR_NO_DEVICE;
-  verdict[dev] = rc;
+  checked[dev] = rc;
   return rc;
 }
 
