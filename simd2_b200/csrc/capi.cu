@@ -1139,7 +1139,7 @@ struct BatchedPlan {
 template <int OP>
 int launch_batched(BatchedPlan* p, cudaStream_t stream) {
   auto kern = closure_batched_kernel<OP>;
-  const size_t smem = simt_smem_bytes(4);
+  const size_t smem = simt_smem_bytes(kSimtStages);
   static bool configured[64] = {};
   if (!configured[p->dev]) {
     SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -39,7 +39,7 @@ constexpr int kSimtThreads = kSimtWarps * 32;
 constexpr int kATileBytes = kBM * kBK * 4;  // 16 KiB
 constexpr int kBTileBytes = kBK * kBN * 4;  // 16 KiB
 constexpr int kStageBytes = kATileBytes + kBTileBytes;
-constexpr int kSimtStages = 4;
+constexpr int kSimtStages = 6;
 
 constexpr size_t simt_smem_bytes(int stages) {
   return (size_t)stages * kStageBytes + 1024 /* alignment slack */ + 2 * stages * sizeof(uint64_t);
