@@ -343,7 +343,7 @@ def extra_measurements(args, dev):
     t0 = time.perf_counter()
     it4 = s2.closure("or_and", X)
     ms4 = (time.perf_counter() - t0) * 1e3
-    cfg4["or_and_closure_16384"] = {"ms": ms4, "iters": it4, "gops": 2.0 * n4 ** 3 * it4 / ms4 / 1e6,
+    cfg4["or_and_closure_16384"] = {"ms": ms4, "iters": it4, "gops_dense_equivalent": 2.0 * n4 ** 3 * it4 / ms4 / 1e6,
                                     "how": "simd2_closure_orand_u8 wall clock: CSR SpGEMM steps while X is sparse, then INT8 "
                                            "tcgen05 per squaring"}
     del X
