@@ -118,70 +118,57 @@ __global__ void compare_update_kernel(T* __restrict__ prev, T* __restrict__ cur,
 }
 
 // ---------------------------------------------------------------------------
-// FP16 selection path (max_min, min_max): gates and operand packing.
-// Both gates must be non-zero (or absent) for a gated kernel to run.
+// FP16 selection path (max_min, min_max): path flags and operand packing.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool gates_open(const int* g1, const int* g2) {
-  return (!g1 || *g1 != 0) && (!g2 || *g2 != 0);
-}
-
-// flags[0] = 1 (FP16 path), flags[1] = 0 (FP32 path) before the check.
+// flags[0] = 1 (FP16 path), flags[1] = 0 (FP32 path) before the packing.
 __global__ void fp16_flags_init_kernel(int* flags) {
   flags[0] = 1;
   flags[1] = 0;
 }
 
-// Clears flags[0] when some entry of A or B is not exactly an FP16 value
-// (round trip float -> half -> float changes its bits, NaN included).
-__global__ void fp16_exact_kernel(const float* __restrict__ A, long long lda, int M, int K,
-                                  const float* __restrict__ B, long long ldb, int N, int* flags, const int* gate) {
-  if (gate && *gate == 0) return;
-  bool bad = false;
-  const long long na = (long long)M * K, nb = (long long)K * N;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < na + nb;
-       t += (long long)gridDim.x * blockDim.x) {
-    float x;
-    if (t < na) {
-      const long long i = t / K, k = t - i * K;
-      x = A[i * lda + k];
-    } else {
-      const long long u = t - na, k = u / N, j = u - k * N;
-      x = B[k * ldb + j];
-    }
-    bad |= __float_as_uint(__half2float(__float2half_rn(x))) != __float_as_uint(x);
-  }
-  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicAnd(flags, 0);
-}
-
 __global__ void fp16_flags_finish_kernel(int* flags) { flags[1] = flags[0] ? 0 : 1; }
 
-// A [M][K] -> half [M][Kp], NaN padding (k >= K).
+// The FP16 form of x; *bad is set when the round trip float -> half -> float
+// changes x's bits (x is not exactly an FP16 value, NaN included).
+__device__ __forceinline__ __half to_half_exact(float x, bool& bad) {
+  const __half h = __float2half_rn(x);
+  bad |= __float_as_uint(__half2float(h)) != __float_as_uint(x);
+  return h;
+}
+
+// A [M][K] -> half [M][Kp], NaN padding (k >= K).  Clears flags[0] when an
+// entry of A is not exactly an FP16 value.
 __global__ void pack_half_rows_kernel(const float* __restrict__ A, long long lda, int M, int K,
-                                      __half* __restrict__ out, int Kp, const int* g1, const int* g2) {
-  if (!gates_open(g1, g2)) return;
+                                      __half* __restrict__ out, int Kp, const int* gate, int* flags) {
+  if (gate && *gate == 0) return;
+  bool bad = false;
   const long long total = (long long)M * Kp;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / Kp), k = (int)(t - (long long)i * Kp);
-    out[t] = k < K ? __float2half_rn(A[(long long)i * lda + k]) : __ushort_as_half(0x7e00);
+    out[t] = k < K ? to_half_exact(A[(long long)i * lda + k], bad) : __ushort_as_half(0x7e00);
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicAnd(flags, 0);
 }
 
 // B [K][N] -> k-pair words [Kp/2][Np]: word (p, j) = (half B[2p][j], half B[2p+1][j]),
-// NaN padding for k >= K and j >= N.
+// NaN padding for k >= K and j >= N.  Clears flags[0] when an entry of B is
+// not exactly an FP16 value.
 __global__ void interleave_half_kernel(const float* __restrict__ B, long long ldb, int K, int N,
-                                       __half2* __restrict__ out, int Kp, int Np, const int* g1, const int* g2) {
-  if (!gates_open(g1, g2)) return;
+                                       __half2* __restrict__ out, int Kp, int Np, const int* gate, int* flags) {
+  if (gate && *gate == 0) return;
+  bool bad = false;
   const long long total = (long long)(Kp / 2) * Np;
   const __half nanh = __ushort_as_half(0x7e00);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int p = (int)(t / Np), j = (int)(t - (long long)p * Np);
     const int k0 = 2 * p, k1 = 2 * p + 1;
-    const __half lo = (k0 < K && j < N) ? __float2half_rn(B[(long long)k0 * ldb + j]) : nanh;
-    const __half hi = (k1 < K && j < N) ? __float2half_rn(B[(long long)k1 * ldb + j]) : nanh;
+    const __half lo = (k0 < K && j < N) ? to_half_exact(B[(long long)k0 * ldb + j], bad) : nanh;
+    const __half hi = (k1 < K && j < N) ? to_half_exact(B[(long long)k1 * ldb + j], bad) : nanh;
     out[t] = __halves2half2(lo, hi);
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicAnd(flags, 0);
 }
 
 // D = (C != 0) as 0/1 of type T.
