@@ -615,7 +615,7 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   const int Kp = plan.Kp;
   auto* ahi = reinterpret_cast<__nv_bfloat16*>(ws + plan.a0);
   auto* alo = reinterpret_cast<__nv_bfloat16*>(ws + plan.a1);
-  split_rows_bf16_kernel<<<grid_for((long long)M * Kp), 256, 0, stream>>>(A, lda, M, K, ahi, alo, Kp);
+  split_rows_bf16_kernel<<<grid_for((long long)M * Kp / 8), 256, 0, stream>>>(A, lda, M, K, ahi, alo, Kp);
   count_launch();
   float* na = reinterpret_cast<float*>(ws + plan.na);
   float* nb = reinterpret_cast<float*>(ws + plan.nb);
@@ -2435,8 +2435,8 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   float* n_q = reinterpret_cast<float*>(ws + nq);
   float* n_r = reinterpret_cast<float*>(ws + nr);
   float* t_max = reinterpret_cast<float*>(ws + tm);
-  split_rows_bf16_kernel<<<grid_for((long long)Q * Dp), 256, 0, stream>>>(query, ldq, Q, D, q_hi, q_lo, Dp);
-  split_rows_bf16_kernel<<<grid_for((long long)R * Dp), 256, 0, stream>>>(ref, ldr, R, D, r_hi, r_lo, Dp);
+  split_rows_bf16_kernel<<<grid_for((long long)Q * Dp / 8), 256, 0, stream>>>(query, ldq, Q, D, q_hi, q_lo, Dp);
+  split_rows_bf16_kernel<<<grid_for((long long)R * Dp / 8), 256, 0, stream>>>(ref, ldr, R, D, r_hi, r_lo, Dp);
   row_norms_kernel<<<grid_for((long long)Q * 32), 256, 0, stream>>>(query, ldq, Q, D, n_q);
   row_norms_kernel<<<grid_for((long long)R * 32), 256, 0, stream>>>(ref, ldr, R, D, n_r);
   for (int i = 0; i < 4; i++) count_launch();
@@ -2533,8 +2533,8 @@ extern "C" int simd2_knn_ex(const float* query, int Q, int ldq, const float* ref
   float* n_q = reinterpret_cast<float*>(ws + nq);
   float* n_r = reinterpret_cast<float*>(ws + nr);
   float* dist = reinterpret_cast<float*>(ws + dch);
-  split_rows_bf16_kernel<<<grid_for((long long)Q * Dp), 256, 0, stream>>>(query, ldq, Q, D, q_hi, q_lo, Dp);
-  split_rows_bf16_kernel<<<grid_for((long long)R * Dp), 256, 0, stream>>>(ref, ldr, R, D, r_hi, r_lo, Dp);
+  split_rows_bf16_kernel<<<grid_for((long long)Q * Dp / 8), 256, 0, stream>>>(query, ldq, Q, D, q_hi, q_lo, Dp);
+  split_rows_bf16_kernel<<<grid_for((long long)R * Dp / 8), 256, 0, stream>>>(ref, ldr, R, D, r_hi, r_lo, Dp);
   row_norms_kernel<<<grid_for((long long)Q * 32), 256, 0, stream>>>(query, ldq, Q, D, n_q);
   row_norms_kernel<<<grid_for((long long)R * 32), 256, 0, stream>>>(ref, ldr, R, D, n_r);
   for (int i = 0; i < 4; i++) count_launch();

@@ -213,18 +213,44 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
   lo = __float2bfloat16_rn(__fsub_rn(x, __bfloat162float(hi)));
 }
 
-// A [M][K] (pitch lda) -> A_hi, A_lo [M][Kp].
+__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// A [M][K] (pitch lda) -> A_hi, A_lo [M][Kp], zeros for k >= K.  Kp is a
+// multiple of 8 and hi / lo are 16-byte aligned: a thread converts 8
+// consecutive elements of a row (two 16-byte loads when A's rows allow) and
+// writes 16 bytes to each output.
 __global__ void split_rows_bf16_kernel(const float* __restrict__ A, long long lda, int M, int K,
                                        __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int Kp) {
-  const long long total = (long long)M * Kp;
+  const int groups = Kp >> 3;
+  const long long total = (long long)M * groups;
+  const bool vec = (lda % 4 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / Kp);
-    const int k = (int)(t - (long long)i * Kp);
-    __nv_bfloat16 h = __float2bfloat16_rn(0.f), l = h;
-    if (k < K) split_bf16(A[(long long)i * lda + k], h, l);
-    hi[t] = h;
-    lo[t] = l;
+    const int i = (int)(t / groups);
+    const int k0 = (int)(t - (long long)i * groups) * 8;
+    const float* row = A + (long long)i * lda;
+    float x[8];
+    if (vec && k0 + 8 <= K) {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(row + k0));
+      const float4 w = __ldg(reinterpret_cast<const float4*>(row + k0 + 4));
+      x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w, x[4] = w.x, x[5] = w.y, x[6] = w.z, x[7] = w.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; e++) x[e] = k0 + e < K ? row[k0 + e] : 0.f;
+    }
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      __nv_bfloat16 h0, l0, h1, l1;
+      split_bf16(x[2 * q], h0, l0);
+      split_bf16(x[2 * q + 1], h1, l1);
+      hw[q] = pack_bf16x2(h0, h1);
+      lw[q] = pack_bf16x2(l0, l1);
+    }
+    reinterpret_cast<uint4*>(hi)[t] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    reinterpret_cast<uint4*>(lo)[t] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
   }
 }
 
