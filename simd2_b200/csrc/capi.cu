@@ -397,9 +397,9 @@ int enqueue_half_path(int op, int M, int N, int K, const float* A, long long lda
   // the FP16 copies are made unconditionally and clear flags[0] when an entry
   // is not exactly an FP16 value; then flags[1] = !flags[0] gates the FP32 path
   fp16_flags_init_kernel<<<1, 1, 0, stream>>>(flags);
-  pack_half_rows_kernel<<<grid_for((long long)M * plan.Kh), 256, 0, stream>>>(A, lda, M, K, Ah, plan.Kh, ep.gate,
+  pack_half_rows_kernel<<<grid_for((long long)M * plan.Kh / 8), 256, 0, stream>>>(A, lda, M, K, Ah, plan.Kh, ep.gate,
                                                                               flags);
-  interleave_half_kernel<<<grid_for((long long)(plan.Kh / 2) * plan.Np), 256, 0, stream>>>(B, ldb, K, N, Bh, plan.Kh,
+  interleave_half_kernel<<<grid_for((long long)(plan.Kh / 2) * plan.Np / 4), 256, 0, stream>>>(B, ldb, K, N, Bh, plan.Kh,
                                                                                             plan.Np, ep.gate, flags);
   fp16_flags_finish_kernel<<<1, 1, 0, stream>>>(flags);
   for (int i = 0; i < 4; i++) count_launch();

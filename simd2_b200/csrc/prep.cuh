@@ -137,36 +137,77 @@ __device__ __forceinline__ __half to_half_exact(float x, bool& bad) {
 }
 
 // A [M][K] -> half [M][Kp], NaN padding (k >= K).  Clears flags[0] when an
-// entry of A is not exactly an FP16 value.
+// entry of A is not exactly an FP16 value.  Kp is a multiple of 8: a thread
+// converts 8 consecutive elements of a row and writes them as one 16-byte store.
 __global__ void pack_half_rows_kernel(const float* __restrict__ A, long long lda, int M, int K,
                                       __half* __restrict__ out, int Kp, const int* gate, int* flags) {
   if (gate && *gate == 0) return;
   bool bad = false;
-  const long long total = (long long)M * Kp;
+  const int groups = Kp >> 3;
+  const long long total = (long long)M * groups;
+  const bool vec = (lda % 4 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0);
+  const __half nanh = __ushort_as_half(0x7e00);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / Kp), k = (int)(t - (long long)i * Kp);
-    out[t] = k < K ? to_half_exact(A[(long long)i * lda + k], bad) : __ushort_as_half(0x7e00);
+    const int i = (int)(t / groups);
+    const int k0 = (int)(t - (long long)i * groups) * 8;
+    const float* row = A + (long long)i * lda;
+    __half h[8];
+    if (vec && k0 + 8 <= K) {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(row + k0));
+      const float4 w = __ldg(reinterpret_cast<const float4*>(row + k0 + 4));
+      const float x[8] = {u.x, u.y, u.z, u.w, w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int e = 0; e < 8; e++) h[e] = to_half_exact(x[e], bad);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; e++) h[e] = k0 + e < K ? to_half_exact(row[k0 + e], bad) : nanh;
+    }
+    uint32_t wv[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      wv[q] = (uint32_t)__half_as_ushort(h[2 * q]) | ((uint32_t)__half_as_ushort(h[2 * q + 1]) << 16);
+    reinterpret_cast<uint4*>(out)[t] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicAnd(flags, 0);
 }
 
 // B [K][N] -> k-pair words [Kp/2][Np]: word (p, j) = (half B[2p][j], half B[2p+1][j]),
 // NaN padding for k >= K and j >= N.  Clears flags[0] when an entry of B is
-// not exactly an FP16 value.
+// not exactly an FP16 value.  Np is a multiple of 4: a thread forms the words
+// of 4 consecutive columns and writes them as one 16-byte store.
 __global__ void interleave_half_kernel(const float* __restrict__ B, long long ldb, int K, int N,
                                        __half2* __restrict__ out, int Kp, int Np, const int* gate, int* flags) {
   if (gate && *gate == 0) return;
   bool bad = false;
-  const long long total = (long long)(Kp / 2) * Np;
+  const int quads = Np >> 2;
+  const long long total = (long long)(Kp / 2) * quads;
+  const bool vec = (ldb % 4 == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0);
   const __half nanh = __ushort_as_half(0x7e00);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int p = (int)(t / Np), j = (int)(t - (long long)p * Np);
-    const int k0 = 2 * p, k1 = 2 * p + 1;
-    const __half lo = (k0 < K && j < N) ? to_half_exact(B[(long long)k0 * ldb + j], bad) : nanh;
-    const __half hi = (k1 < K && j < N) ? to_half_exact(B[(long long)k1 * ldb + j], bad) : nanh;
-    out[t] = __halves2half2(lo, hi);
+    const int p = (int)(t / quads);
+    const int j0 = (int)(t - (long long)p * quads) * 4;
+    __half lo[4], hi[4];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      const int k = 2 * p + r;
+      __half* dst = r == 0 ? lo : hi;
+      const float* row = B + (long long)k * ldb;
+      if (k < K && vec && j0 + 4 <= N) {
+        const float4 u = __ldg(reinterpret_cast<const float4*>(row + j0));
+        dst[0] = to_half_exact(u.x, bad), dst[1] = to_half_exact(u.y, bad);
+        dst[2] = to_half_exact(u.z, bad), dst[3] = to_half_exact(u.w, bad);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; e++) dst[e] = (k < K && j0 + e < N) ? to_half_exact(row[j0 + e], bad) : nanh;
+      }
+    }
+    uint32_t wv[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      wv[e] = (uint32_t)__half_as_ushort(lo[e]) | ((uint32_t)__half_as_ushort(hi[e]) << 16);
+    reinterpret_cast<uint4*>(out)[t] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicAnd(flags, 0);
 }
