@@ -455,7 +455,7 @@ int srgemm_core(int op, int M, int N, int K, const T* A, long long lda, const T*
   ep32.gate2 = path_gate;
   SimtConfig cfg32 = cfg;
   if (path_gate) cfg32.count_ops = false;  // the FP16 kernel's slot carries the operation count
-  interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 2), 256, 0, stream>>>(
+  interleave_pairs_kernel<T, MODE><<<grid_for((long long)plan.Kp / 2 * plan.Np / 4), 256, 0, stream>>>(
       B, ldb, K, N, Bp, plan.Kp, plan.Np, pad, ep.gate, path_gate);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
@@ -675,7 +675,7 @@ int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, 
   const int Kp = plan.Kp;
   uint8_t* a8 = ws + plan.a0;
   uint8_t* b8 = ws + plan.b0;
-  bool_rows_u8_kernel<T><<<grid_for((long long)M * Kp), 256, 0, stream>>>(A, lda, M, K, a8, Kp);
+  bool_rows_u8_kernel<T><<<grid_for((long long)M * Kp / 16), 256, 0, stream>>>(A, lda, M, K, a8, Kp);
   count_launch();
   dim3 tgrid((N + 31) / 32, (Kp + 31) / 32), tblock(32, 8);
   transpose_prep_kernel<T, 1><<<tgrid, tblock, 0, stream>>>(B, ldb, K, N, b8, nullptr, Kp);
@@ -1349,7 +1349,7 @@ int simd2_closure_pred(simd2_op op, int n, float* X, int ldx, int32_t* P, int ld
     // interleaved, and A = X itself when its rows suit TMA (else a packed copy)
     transpose_f32_kernel<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, stream>>>(n, Xc, ldc, XT, n);
     count_launch();
-    interleave_pairs_kernel<float, 0><<<grid_for((long long)Kp / 2 * Np / 2), 256, 0, stream>>>(Xc, ldc, n, n, Bp, Kp,
+    interleave_pairs_kernel<float, 0><<<grid_for((long long)Kp / 2 * Np / 4), 256, 0, stream>>>(Xc, ldc, n, n, Bp, Kp,
                                                                                                Np, pad);
     count_launch();
     const bool pack_a = !a_tma_ok(Xc, ldc) || (n % 4 != 0);

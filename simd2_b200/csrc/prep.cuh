@@ -10,32 +10,47 @@
 namespace simd2 {
 
 // B'[p][2j+e] = B[2p+e][j] for 2p+e < K and j < N, else `pad`.
-// B' has Kp/2 rows of 2*Np floats (Kp, Np are the padded sizes).  Each thread
-// writes one float4 = (B[2p][j], B[2p+1][j], B[2p][j+1], B[2p+1][j+1]).
+// B' has Kp/2 rows of 2*Np floats (Kp, Np are the padded sizes); a float4 of
+// B' is (B[2p][j], B[2p+1][j], B[2p][j+1], B[2p+1][j+1]).
 template <typename T, int MODE>
 __device__ __forceinline__ float load_operand(const T* p) {
   if constexpr (MODE == 1) return (*p != T(0)) ? 1.0f : 0.0f;  // boolean (or_and as max_min on {0,1})
   else return static_cast<float>(*p);
 }
 
+// A thread fills 4 columns (two float4 stores); float B with 16-byte aligned
+// rows is read with one float4 load per k row where the 4 columns are in range.
 template <typename T, int MODE>
 __global__ void interleave_pairs_kernel(const T* __restrict__ B, long long ldb, int K, int N,
                                         float* __restrict__ Bp, int Kp, int Np, float pad,
                                         const int* gate = nullptr, const int* gate2 = nullptr) {
   if ((gate && *gate == 0) || (gate2 && *gate2 == 0)) return;
-  const long long pairs_j = Np / 2;
-  const long long total = (long long)(Kp / 2) * pairs_j;
+  const long long quads = Np / 4;
+  const long long total = (long long)(Kp / 2) * quads;
+  constexpr bool kFloat = std::is_same<T, float>::value && MODE == 0;
+  const bool vec = kFloat && (ldb % 4 == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int p = (int)(t / pairs_j);
-    const int j = (int)(t - (long long)p * pairs_j) * 2;
-    const int k0 = 2 * p, k1 = 2 * p + 1;
-    float4 v;
-    v.x = (k0 < K && j < N) ? load_operand<T, MODE>(B + (long long)k0 * ldb + j) : pad;
-    v.y = (k1 < K && j < N) ? load_operand<T, MODE>(B + (long long)k1 * ldb + j) : pad;
-    v.z = (k0 < K && j + 1 < N) ? load_operand<T, MODE>(B + (long long)k0 * ldb + j + 1) : pad;
-    v.w = (k1 < K && j + 1 < N) ? load_operand<T, MODE>(B + (long long)k1 * ldb + j + 1) : pad;
-    reinterpret_cast<float4*>(Bp)[t] = v;
+    const int p = (int)(t / quads);
+    const int j = (int)(t - (long long)p * quads) * 4;
+    float x[2][4];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      const int k = 2 * p + r;
+      if constexpr (kFloat) {
+        if (vec && k < K && j + 4 <= N) {
+          const float4 u = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const float*>(B) + (long long)k * ldb + j));
+          x[r][0] = u.x, x[r][1] = u.y, x[r][2] = u.z, x[r][3] = u.w;
+          continue;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++)
+        x[r][e] = (k < K && j + e < N) ? load_operand<T, MODE>(B + (long long)k * ldb + j + e) : pad;
+    }
+    float4* o = reinterpret_cast<float4*>(Bp) + 2 * t;
+    o[0] = make_float4(x[0][0], x[1][0], x[0][1], x[1][1]);
+    o[1] = make_float4(x[0][2], x[1][2], x[0][3], x[1][3]);
   }
 }
 
@@ -295,16 +310,44 @@ __global__ void split_rows_bf16_kernel(const float* __restrict__ A, long long ld
   }
 }
 
-// A [M][K] of T -> bytes {0,1} [M][Kp].
+// A [M][K] of T -> bytes {0,1} [M][Kp].  Kp is a multiple of 16: a thread
+// writes 16 bytes of a row; byte inputs with 16-byte aligned rows are read
+// with one 16-byte load and normalised four bytes at a time.
 template <typename T>
 __global__ void bool_rows_u8_kernel(const T* __restrict__ A, long long lda, int M, int K, uint8_t* __restrict__ out,
                                     int Kp) {
-  const long long total = (long long)M * Kp;
+  const int groups = Kp >> 4;
+  const long long total = (long long)M * groups;
+  constexpr bool kBytes = sizeof(T) == 1;
+  const bool vec = kBytes && (lda % 16 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / Kp);
-    const int k = (int)(t - (long long)i * Kp);
-    out[t] = (k < K && A[(long long)i * lda + k] != T(0)) ? 1 : 0;
+    const int i = (int)(t / groups);
+    const int k0 = (int)(t - (long long)i * groups) * 16;
+    const T* row = A + (long long)i * lda;
+    uint32_t w[4];
+    if (kBytes && vec && k0 + 16 <= K) {
+      const uint4 u = __ldg(reinterpret_cast<const uint4*>(row + k0));
+      const uint32_t in[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        // 0x01 in every byte that is nonzero, carry-free
+        const uint32_t b = in[q];
+        w[q] = (((b & 0x7f7f7f7fu) + 0x7f7f7f7fu | b) & 0x80808080u) >> 7;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int k = k0 + 4 * q + e;
+          v |= (uint32_t)(k < K && row[k] != T(0)) << (8 * e);
+        }
+        w[q] = v;
+      }
+    }
+    reinterpret_cast<uint4*>(out)[t] = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
