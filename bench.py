@@ -417,6 +417,9 @@ def extra_measurements(args, dev):
         identical = True
         for i, (n, d) in enumerate([(4096, 4), (4096, 64), (4096, 1024), (8192, 4), (8192, 64), (8192, 1024)]):
             g = torch.from_numpy(datagen.rmat_graph(n, d, seed=500 + i)).to(dev)
+            # warm-up of both policies: workspaces are allocated outside the timing
+            s2.closure_ex("min_plus", g.clone(), dispatch="dense")
+            s2.closure_ex("min_plus", g.clone(), dispatch="learned", mlp_params=params)
             Xa, Xb = g.clone(), g.clone()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
