@@ -112,7 +112,10 @@ int simd2_closure(simd2_op op, int n, float* X, int ldx, int max_iter,
 int simd2_closure_bf(simd2_op op, int n, const float* A0, int lda0, float* X, int ldx, int max_iter,
                      simd2_conv conv, int* iters_out, cudaStream_t stream);
 
-/* or_and transitive closure on uint8 0/1 (apps/gtc/cuASR), synchronous. */
+/* or_and transitive closure on uint8 0/1 (apps/gtc/cuASR), synchronous.
+ * From n = 8192 a sparse X is first squared as CSR SpGEMM steps (while X
+ * holds at most n^2/32 entries and a step forms at most n^3/16384 products),
+ * then on the INT8 tensor cores; same result and step count either way. */
 int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter,
                            int* iters_out, cudaStream_t stream);
 
