@@ -207,6 +207,13 @@ def closure_ex(op: str, X: torch.Tensor, dispatch: str = "dense", config: int = 
                max_iter: int = 500, conv: str = "exact", record: bool = False, stream=None):
     """Closure with a per-step dispatch policy.
 
+    ``dispatch``: "dense" (the plain path), "fixed" (``config`` every step) or
+    "learned": above n = 1024 (bitwise change test, a semiring the SpGEMM
+    supports) sparse steps run as CSR SpGEMM while X is sparse (recorded as
+    config ``NUM_CONFIGS``), then the MLP in ``mlp_params`` picks each dense
+    step's configuration (n > 2048; the plain path for smaller n).  Every
+    policy gives the same bits and step count.
+
     Returns the step count, or with ``record`` a dict with the per-step
     configurations, device times (ms) and cost-model features.
     """
