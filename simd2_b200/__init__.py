@@ -236,7 +236,10 @@ def closure_ex(op: str, X: torch.Tensor, dispatch: str = "dense", config: int = 
 
 def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", stream=None,
             raise_not_converged: bool = True) -> int:
-    """Repeated squaring X <- X (+) X(x)X in place until unchanged; returns the step count."""
+    """Repeated squaring X <- X (+) X(x)X in place until unchanged; returns the step count.
+
+    or_and takes a uint8 0/1 matrix; from n = 8192 its sparse first steps run
+    as CSR SpGEMM steps (same result and step count as the dense loop)."""
     n = X.shape[0]
     if X.shape != (n, n):
         raise ValueError("closure needs a square matrix")
