@@ -23,7 +23,6 @@ absent) on every host core, on a bounded row sample of the same workload.
 from __future__ import annotations
 
 import argparse
-import ctypes
 import json
 import os
 import re
