@@ -14,7 +14,13 @@
  * D may alias C (in-place accumulation); D must not overlap A or B.
  *
  * Exactness: the six min/max semirings and or_and are bit-exact against
- * host_srgemm.  Preconditions for that: operands hold no NaN and no -0.0.
+ * host_srgemm.  Preconditions for that: operands hold no NaN and no -0.0,
+ * and for max_mul / min_mul no product is -0.0, i.e. no zero operand meets a
+ * negative one (operands >= 0, as in the reference's maxrp / minrp apps,
+ * always qualify).  host_srgemm keeps the first of several products that tie
+ * at zero with its sign; the device folds products in another order, so
+ * outside this precondition results still equal host_srgemm's in value and
+ * can differ only in the sign of a zero result.
  * plus_mul and minus_square are dense contractions computed on the tensor
  * cores (BF16 hi/lo split, FP32 accumulate); their error bound is stated in
  * the library documentation and checked against an FP64 oracle.
@@ -372,9 +378,13 @@ int simd2_device_status(void);
  * larger problems return SIMD2_ERR_SCRATCH_LIMIT.  The other five semirings
  * return SIMD2_ERR_UNSUPPORTED.
  *
- * The first call on each device looks up that array's device address
- * (cudaGetSymbolAddress) with the device current; make that first call before
- * any stream capture.  Every call, on every stream, shares the one array and
+ * Each call looks up that array's device address (cudaGetSymbolAddress)
+ * with the device current.  With CUDA's lazy module loading the array is
+ * only placed in device memory by the first call on a device, so a caller
+ * that is going to hand out all device memory makes one small call first
+ * (and makes that first call before any stream capture); if the device has
+ * no room left for the array, the call returns SIMD2_ERR_ALLOC.  Every
+ * call, on every stream, shares the one array and
  * each call overwrites the part it uses completely before reading it (nothing
  * has to start at zero), so calls whose kernels can overlap on the GPU race
  * with each other: order them on one stream or synchronize between them. */

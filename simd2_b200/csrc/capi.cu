@@ -2725,26 +2725,22 @@ namespace {
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[SIMD2_NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch per device.  In host code the symbol
-// name is only a host-side stand-in; the address a kernel may use comes from
-// cudaGetSymbolAddress, looked up once per device with that device current.
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {};
-
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the symbol name is only a host-side stand-in; the address a kernel may use
+// comes from cudaGetSymbolAddress with the device current.  It is looked up
+// on every call (cheap once the module is loaded) rather than cached, so a
+// context recreated after cudaDeviceReset never sees a stale address.  Under
+// lazy module loading the first lookup on a device is what places the array
+// in device memory; if the device has no room left for it that shows up here
+// as cudaErrorMemoryAllocation and is reported as SIMD2_ERR_ALLOC.
 int noalloc_scratch(uint8_t** out) {
-  int dev = 0;
-  SIMD2_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
-      cudaGetLastError();
-      return SIMD2_ERR_CUDA;
-    }
-    g_noalloc_addr[dev] = p;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? SIMD2_ERR_ALLOC : SIMD2_ERR_CUDA;
   }
-  *out = static_cast<uint8_t*>(g_noalloc_addr[dev]);
+  *out = static_cast<uint8_t*>(p);
   return SIMD2_OK;
 }
 
