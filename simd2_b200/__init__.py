@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
         L.simd2_batched_plan_iters.argtypes = [P, PI, PI]
         L.simd2_batched_plan_destroy.argtypes = [P]
         L.simd2_closure_batched.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, PI, P]
+        L.simd2_srgemm_f16.argtypes = [I, I, I, I, P, I, P, I, P, I, P, I, I, P]
         L.simd2_knn.argtypes = [P, I, I, P, I, I, I, I, P, P, I, P]
         L.simd2_knn.restype = I
         L.simd2_knn_ex.argtypes = [P, I, I, P, I, I, I, I, P, P, I, I, P]
@@ -106,7 +107,7 @@ def lib() -> ctypes.CDLL:
                      "simd2_batched_plan_create", "simd2_batched_plan_run", "simd2_batched_plan_iters",
                      "simd2_batched_plan_destroy", "simd2_closure_batched", "simd2_srgemm_tuned",
                      "simd2_closure_ex", "simd2_mlp_param_count", "simd2_mlp_forward", "simd2_mlp_gradient",
-                     "simd2_mlp_adam"):
+                     "simd2_mlp_adam", "simd2_srgemm_f16"):
             getattr(L, name).restype = I
         _lib = L
     return _lib
@@ -170,6 +171,28 @@ def srgemm(op: str, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = N
         rc = lib().simd2_srgemm(OP_ID[op], M, N, K, A.data_ptr(), lda, B.data_ptr(), ldb, cptr, ldc, D.data_ptr(),
                                 ldd, int(do_epilogue), s)
     _check(rc, f"srgemm({op})")
+    return D
+
+
+def srgemm_f16(op: str, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, do_epilogue: bool = False,
+               D: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """srgemm with float16 A and B and float32 C / D: the entry behind the
+    reference's ``tensor_srgemm`` (kernel/tensor_srgemm.cuh:197-218).  The
+    halves are widened exactly; or_and reads any nonzero as true and writes 0/1."""
+    M, K = A.shape
+    K2, N = B.shape
+    if K != K2:
+        raise ValueError("inner dimensions differ")
+    if A.dtype != torch.float16 or B.dtype != torch.float16:
+        raise TypeError("srgemm_f16 takes float16 A and B")
+    if D is None:
+        D = torch.empty((M, N), dtype=torch.float32, device=A.device)
+    if D.dtype != torch.float32 or (do_epilogue and (C is None or C.dtype != torch.float32)):
+        raise TypeError("srgemm_f16 takes float32 C and D")
+    cptr, ldc = (C.data_ptr(), _mat(C, "C")) if do_epilogue else (None, N)
+    rc = lib().simd2_srgemm_f16(OP_ID[op], M, N, K, A.data_ptr(), _mat(A, "A"), B.data_ptr(), _mat(B, "B"), cptr, ldc,
+                                D.data_ptr(), _mat(D, "D"), int(do_epilogue), _stream(stream))
+    _check(rc, f"srgemm_f16({op})")
     return D
 
 

@@ -189,6 +189,22 @@ def test_full_size_row_sample(cuda, op):
     assert s2.device_status() == 0
 
 
+def test_min_plus_8192_row_sample(cuda):
+    """min_plus at 8192^3 (the size of the reference's srgemm micro-benchmark,
+    micro_bench/srgemm_bench.cu:252) on the sweep's value distribution:
+    bit-exact against host_srgemm on 32 sampled rows -- the reference's own
+    compiled header where it was built, else the restatement pinned to it."""
+    n = 8192
+    a, b, c = datagen.semiring_operands("min_plus", n, n, n, seed=8192)
+    got = run_gpu("min_plus", a, b, c, True, cuda)
+    rows = np.random.default_rng(8192).choice(n, size=32, replace=False)
+    use_ref = oracle.ref_lib() is not None
+    want = oracle.srgemm("min_plus", a[rows], b, c[rows], do_epilogue=True, use_ref=use_ref)
+    np.testing.assert_array_equal(bits(got[rows]), bits(want))
+    assert np.isfinite(got[rows]).mean() > 0.99  # 20 % identities in A and B still leave finite minima
+    assert s2.device_status() == 0
+
+
 @pytest.mark.parametrize("op", ["max_min", "min_max"])
 def test_selection_fp16_and_fp32_paths(cuda, op):
     """max_min / min_max take the packed-FP16 kernel when every A and B entry
