@@ -25,7 +25,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -202,45 +201,52 @@ def run_reference_arm(args):
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
-def traffic_from_profile(name="srgemm_simt_kernel_min_plus_4096.md"):
-    """DRAM bytes per launch of a kernel from its committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", name)
+def traffic_from_profile(key="srgemm_simt_kernel min_plus 4096^3"):
+    """DRAM bytes per launch of a kernel, from the byte counts kept beside the
+    ncu summaries (profiles/dram_traffic.json)."""
     try:
-        with open(path) as f:
-            m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
-            return float(m.group(1)) if m else None
-    except OSError:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            return float(json.load(f)[key]["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError):
         return None
 
 
-def batched_sharded(args, dev, rank, world):
-    """Batched APSP over `world` ranks: every rank builds the same seeded graph
-    list, closes its size-balanced shard in one persistent launch, and the
-    slowest rank's device time is the job's time (no collective in the data
-    path; only the timing is reduced)."""
+def batched_sharded(args, dev, rank, world, op="min_plus", reps=3):
+    """Batched closure over `world` ranks: every rank builds the same seeded
+    graph list, closes its size-balanced shard in one persistent launch
+    captured in a CUDA graph, and the slowest rank's device time of a graph
+    replay is the job's time (no collective in the data path; only the
+    timing is reduced).  The inputs are restored before each replay, outside
+    the timed region."""
     import torch
 
     import simd2_b200 as s2
     from simd2_b200 import datagen
     from simd2_b200.shard import assign_graphs, max_over_ranks
 
-    graphs = datagen.batched_graphs(args.batched_count, 32, 1024, seed=3)
+    graphs = datagen.batched_graphs(args.batched_count, 32, 1024, seed=3, op=op)
     mine = assign_graphs([g.shape[0] for g in graphs], world)[rank]
     mats = [torch.from_numpy(graphs[g]).to(dev) for g in mine]
     origs = [m.clone() for m in mats]
-    plan = s2.BatchedClosure("min_plus", mats)
+    plan = s2.BatchedClosure(op, mats)
+    plan.run()  # warm-up outside the capture (sets the kernel's shared-memory attribute)
+    torch.cuda.synchronize()
+    torch._foreach_copy_(mats, origs)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        plan.run()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     times = []
-    for _ in range(3):
-        for m, o in zip(mats, origs):
-            m.copy_(o)
+    for _ in range(reps):
+        torch._foreach_copy_(mats, origs)
         torch.cuda.synchronize()
         ev0.record()
-        plan.run()
+        graph.replay()
         ev1.record()
         torch.cuda.synchronize()
         times.append(ev0.elapsed_time(ev1))
     its, nc = plan.iters()
+    del graph
     plan.close()
     local_ms = min(times)
     ms = max_over_ranks(local_ms, device=dev) if world > 1 else local_ms
@@ -249,9 +255,120 @@ def batched_sharded(args, dev, rank, world):
         ops_t = torch.tensor([ops], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(ops_t)
         ops = float(ops_t.item())
-    return {"graphs": len(graphs), "n_gpus": world, "batched_ms": ms, "graphs_per_s": len(graphs) / ms * 1e3,
-            "gops_dense_equivalent": ops / ms / 1e6, "not_converged": nc,
-            "how": "one persistent launch per rank on an n^3-balanced shard; max-over-ranks CUDA-event time"}, graphs
+    res = {"semiring": op, "graphs": len(graphs), "n_gpus": world, "batched_ms": ms,
+           "graphs_per_s": len(graphs) / ms * 1e3, "gops_dense_equivalent": ops / ms / 1e6, "not_converged": nc,
+           "how": "one persistent launch per rank on an n^3-balanced shard, captured in a CUDA graph; CUDA-event time "
+                  f"of a graph replay (best of {reps}), max over ranks"}
+    return res, graphs, mats, mine
+
+
+def fp64_errors(got, want, scale=None):
+    """Error of a float32 result against its FP64 value: max abs, max rel over
+    the entries at least as large as the result's rms (near-zero sums make the
+    elementwise ratio meaningless), normwise (max abs / max |FP64|) and, with
+    ``scale`` = the sum of the absolute terms, max |err| / scale."""
+    import torch
+    d = (got.double() - want).abs()
+    mag = want.abs()
+    rms = float(torch.sqrt((want * want).mean()))
+    big = mag >= rms
+    out = {"max_abs_err": float(d.max()), "max_rel_err": float((d[big] / mag[big]).max()) if bool(big.any()) else None,
+           "normwise_rel_err": float(d.max() / mag.max())}
+    if scale is not None:
+        out["max_err_over_abs_sum"] = float((d / scale).max())
+    return out
+
+
+def sum_op_errors(op, A, B, C, D):
+    """FP64 (torch, on the GPU) errors of a plus_mul / minus_square result
+    D = A (x) B (+) C."""
+    import torch
+    A64, B64, C64 = A.double(), B.double(), C.double()
+    if op == "plus_mul":
+        want = A64 @ B64 + C64
+        scale = A64.abs() @ B64.abs() + C64.abs()
+    else:  # sum_k (a_ik - b_kj)^2 = |a_i|^2 + |b_j|^2 - 2 a_i . b_j
+        an = (A64 * A64).sum(1, keepdim=True)
+        bn = (B64 * B64).sum(0, keepdim=True)
+        want = an + bn - 2.0 * (A64 @ B64) + C64
+        scale = 2.0 * (an + bn) + C64.abs()
+    e = fp64_errors(D, want, scale)
+    del A64, B64, C64, want, scale
+    return e
+
+
+def knn_errors(query, ref, dist, idx, sample=2048, k=16):
+    """The k-NN result against FP64 on the first ``sample`` queries: distance
+    errors (all returned pairs, and the near-duplicate queries whose nearest
+    distance is below 0.1), and index agreement position by position as the
+    reference's PLD test counts it, plus as sets."""
+    import torch
+    q = query[:sample].double()
+    r = ref.double()
+    d2 = (q * q).sum(1, keepdim=True) + (r * r).sum(1)[None, :] - 2.0 * (q @ r.T)
+    cand = torch.topk(d2, k + 8, dim=1, largest=False).indices
+    del d2
+    exact = ((q[:, None, :] - r[cand]) ** 2).sum(2)  # FP64 sum of squares of the candidates
+    # order by (distance, index): ties keep the lower reference index
+    key_order = torch.argsort(cand, dim=1)
+    cand = torch.gather(cand, 1, key_order)
+    exact = torch.gather(exact, 1, key_order)
+    order = torch.argsort(exact, dim=1, stable=True)[:, :k]
+    want_idx = torch.gather(cand, 1, order)
+    want_d = torch.sqrt(torch.gather(exact, 1, order))
+    got_d = dist[:sample].double()
+    got_i = idx[:sample].long()
+    rel = (got_d - want_d).abs() / want_d.clamp_min(1e-300)
+    near = want_d[:, 0] < 0.1
+    pos = (got_i == want_idx).double().mean()
+    sets = sum(len(set(a.tolist()) & set(b.tolist())) for a, b in zip(got_i.cpu(), want_idx.cpu())) / (sample * k)
+    return {"queries_checked": sample, "max_abs_err": float((got_d - want_d).abs().max()),
+            "max_rel_err": float(rel.max()), "near_duplicate_queries": int(near.sum()),
+            "near_duplicate_max_rel_err": float(rel[near].max()) if bool(near.any()) else None,
+            "index_agreement": float(pos), "index_set_agreement": float(sets),
+            "how": "FP64 distances of the first queries to every reference (torch on the GPU), exact FP64 sums of "
+                   "squares for the 24 nearest, ordered by (distance, index)"}
+
+
+def min_plus_8192(dev, reps=3):
+    """min_plus srgemm at M = N = K = 8192 with C (integer-valued FP32 in
+    [1,1000], 20 % +inf): CUDA-event kernel time from the library's own
+    events on the launching stream, and the call's time with its operand
+    preparation."""
+    import torch
+
+    import simd2_b200 as s2
+
+    n = 8192
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(8192)
+
+    def ints():
+        x = torch.randint(1, 1001, (n, n), device=dev, generator=gen).float()
+        x[torch.rand((n, n), device=dev, generator=gen) < 0.2] = float("inf")
+        return x
+
+    A, B, C = ints(), ints(), ints()
+    D = torch.empty_like(A)
+    s2.srgemm("min_plus", A, B, C, do_epilogue=True, D=D)  # warm-up
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with s2.KernelTimer() as kt:
+        ev0.record()
+        for _ in range(reps):
+            s2.srgemm("min_plus", A, B, C, do_epilogue=True, D=D)
+        ev1.record()
+        torch.cuda.synchronize()
+    kms, launches, _ = kt.by_kind["simt"]
+    kms /= max(launches, 1)
+    peaks, kind = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    peak = SMS * LANES * sm_max * 1e6 / 1e9
+    gops = 2.0 * n ** 3 / kms / 1e6
+    del A, B, C, D
+    return {"kernel_ms": kms, "call_ms": ev0.elapsed_time(ev1) / reps, "gops": gops, "peak_gops": peak,
+            "frac": gops / peak, "peak_source": f"{SMS} SMs x {LANES} lanes x {sm_max:.0f} MHz ({kind} sm_max_mhz)",
+            "how": f"srgemm_simt_kernel, {reps} launches with C; kernel time from CUDA events on the launching stream"}
 
 
 def extra_measurements(args, dev):
@@ -284,20 +401,25 @@ def extra_measurements(args, dev):
                      "gops": 2.0 * 512 ** 3 * it / best / 1e6}
     out["apsp_er512"] = res
 
-    # --- batched closure: graphs with N log-uniform in [32,1024], p in U[0.01,0.3]
-    res_b, graphs = batched_sharded(args, dev, 0, 1)
-    mats = [torch.from_numpy(g).to(dev) for g in graphs]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for m in mats:
-        s2.closure("min_plus", m)
-    torch.cuda.synchronize()
-    pms = (time.perf_counter() - t0) * 1e3
-    res_b.update({"plain_ms": pms, "plain_graphs_per_s": len(graphs) / pms * 1e3,
-                  "speedup_vs_plain": pms / res_b["batched_ms"],
-                  "how": "one persistent launch (CUDA events) vs simd2_closure per graph (wall clock, host loop)"})
-    out["batched_apsp"] = res_b
-    del mats
+    # --- batched closure: graphs with N log-uniform in [32,1024], p in U[0.01,0.3],
+    # min_plus APSP and max_min maximum capacity, each against simd2_closure per graph
+    out["batched_apsp"] = {}
+    for op in ("min_plus", "max_min"):
+        res_b, graphs, closed, _ = batched_sharded(args, dev, 0, 1, op=op)
+        mats = [torch.from_numpy(g).to(dev) for g in graphs]
+        s2.closure(op, mats[0].clone())  # warm-up: the per-graph path's workspace
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        its = [s2.closure(op, m) for m in mats]
+        torch.cuda.synchronize()
+        pms = (time.perf_counter() - t0) * 1e3
+        same = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(mats, closed))
+        res_b.update({"plain_ms": pms, "plain_graphs_per_s": len(graphs) / pms * 1e3,
+                      "speedup_vs_plain": pms / res_b["batched_ms"], "outputs_identical_to_plain": same,
+                      "plain_how": "simd2_closure per graph in a host loop (wall clock around synchronize)",
+                      "plain_iters_total": int(sum(its))})
+        out["batched_apsp"][op] = res_b
+        del mats, closed
 
     # --- paths: closure with a predecessor matrix, and the MST from the min_max closure
     paths = {}
@@ -329,6 +451,9 @@ def extra_measurements(args, dev):
     out["paths"] = paths
     del xp
 
+    # --- the headline size: min_plus srgemm at 8192^3 on the sweep's value distribution
+    out["min_plus_8192"] = min_plus_8192(dev)
+
     # --- dense-contraction workloads at full size (tensor cores)
     cfg4 = {}
     n4 = 16384
@@ -352,7 +477,7 @@ def extra_measurements(args, dev):
     for mode in ("fused", "materialised"):
         s2.knn(Q, R, 16, mode=mode)  # warm-up at full size (workspace growth stays outside the timing)
         ev0.record()
-        s2.knn(Q, R, 16, mode=mode)
+        kd, ki = s2.knn(Q, R, 16, mode=mode)
         ev1.record()
         torch.cuda.synchronize()
         kms = ev0.elapsed_time(ev1)
@@ -361,6 +486,9 @@ def extra_measurements(args, dev):
             "how": "simd2_knn_ex, CUDA events: " + (
                 "selection inside the BF16 hi/lo distance MMA's epilogue, then a per-query merge" if mode == "fused"
                 else "BF16 hi/lo minus_square blocks of 1 GiB written, then top-k + sqrt")}
+        if mode == "fused":
+            cfg4[f"knn_16384x65536x128_k16_{mode}"]["fp64_error"] = knn_errors(Q, R, kd, ki)
+        del kd, ki
     del Q, R
     # --- very sparse inputs: semiring SpGEMM and the hybrid sparse/dense closure
     sp = {}
@@ -395,18 +523,21 @@ def extra_measurements(args, dev):
                  "closure throughout (wall clock)")
     del Xs, As, Ds
     cfg4["sparse_er16384_deg4"] = sp
-    A = torch.randn((8192, 8192), device=dev)
-    B = torch.randn((8192, 8192), device=dev)
-    s2.srgemm("plus_mul", A, B)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(8192)
+    A = torch.randn((8192, 8192), device=dev, generator=gen)
+    B = torch.randn((8192, 8192), device=dev, generator=gen)
+    Dp = s2.srgemm("plus_mul", A, B)
     ev0.record()
     for _ in range(3):
-        s2.srgemm("plus_mul", A, B)
+        s2.srgemm("plus_mul", A, B, D=Dp)
     ev1.record()
     torch.cuda.synchronize()
     pms = ev0.elapsed_time(ev1) / 3
     cfg4["plus_mul_8192"] = {"ms": pms, "gops": 2.0 * 8192 ** 3 / pms / 1e6,
-                             "bf16_equiv_tflops": 3 * 2.0 * 8192 ** 3 / pms / 1e9}
-    del A, B
+                             "bf16_equiv_tflops": 3 * 2.0 * 8192 ** 3 / pms / 1e9,
+                             "fp64_error": sum_op_errors("plus_mul", A, B, torch.zeros_like(A), Dp)}
+    del A, B, Dp
     out["dense_contraction"] = cfg4
 
     # --- learned dispatch on mixed-density R-MAT (a=.57 b=.19 c=.19), vs the plain dense path
@@ -529,7 +660,7 @@ def main():
         return 0
 
     if args.workload == "batched":
-        res, _ = batched_sharded(args, dev, rank, world)
+        res = {op: batched_sharded(args, dev, rank, world, op=op)[0] for op in ("min_plus", "max_min")}
         if rank == 0:
             print(json.dumps({"workload": "batched closure", **res}), flush=True)
         if world > 1:
@@ -588,6 +719,13 @@ def main():
             for _ in range(3):
                 s2.srgemm(op, A, B, C, do_epilogue=True, D=outs[op])
         per_op[op] = t1.ops / (t1.kernel_ms / 1e3) / 1e9
+    # FP64 error of the two summing semirings' sweep results (the last launch's D)
+    sweep_err = {}
+    for op in ("plus_mul", "minus_square"):
+        if op in SWEEP_OPS:
+            A, B, C = devb[op]
+            sweep_err[op] = sum_op_errors(op, A, B, C, outs[op])
+            torch.cuda.synchronize()
 
     # e2e through the public API with host buffers: H2D inputs, srgemm, D2H result,
     # pipelined over two buffer sets and three streams.
@@ -676,7 +814,8 @@ def main():
         if world == 1:
             extras = extra_measurements(args, dev)
         else:
-            extras = {"batched_apsp": batched_sharded(args, dev, rank, world)[0]}
+            extras = {"batched_apsp": {op: batched_sharded(args, dev, rank, world, op=op)[0]
+                                       for op in ("min_plus", "max_min")}}
     if world > 1:
         lt = torch.tensor([launches], dtype=torch.float64, device=dev)
         dist.all_reduce(lt)
@@ -691,6 +830,9 @@ def main():
                        "l2": "inputs larger than L2: 9 semirings x (A,B,C) x 64 MiB rotated every step",
                        "parallelism": f"independent sweep per rank x{world}"},
             "per_semiring_kernel_gops": per_op,
+            "fp64_error": dict(sweep_err, how="full 4096 x 4096 results against FP64 (torch on the GPU): max abs, max "
+                                              "rel over entries >= the rms, normwise, and max |err| / sum of |terms|; "
+                                              "min/max semirings and or_and are bit-exact (tests)"),
             "roofline": {"bound": "cuda_core_issue",
                          "kernel": "srgemm_simt_kernel (min_plus, max_plus, max_min, max_mul, min_mul, min_max)",
                          "achieved": achieved, "peak": issue_peak_gops, "unit": "Gop/s",
@@ -704,7 +846,7 @@ def main():
                                 "peak": bf16_peak, "unit": "TFLOP/s (BF16-equivalent)",
                                 "frac": (tc_equiv / (tc_ms / 1e3) / 1e12) / bf16_peak if tc_ms > 0 else None,
                                 "peak_source": f"{peak_kind} bf16_tflops (cuBLAS burst)", "timed_launches": tc_n,
-                                "traffic": traffic_from_profile("tc_gemm2_kernel_plus_mul_4096.md"),
+                                "traffic": traffic_from_profile("tc_gemm2_kernel plus_mul 4096^3"),
                                 "traffic_of": "one plus_mul 4096^3 launch with C (ncu dram read + write)"},
             "cpu_baseline": cpu,
             "e2e": e2e,

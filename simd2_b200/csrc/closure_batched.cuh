@@ -14,7 +14,8 @@
 // overwritten, so every tile load is in bounds and a padded k contributes a
 // NaN product, which min/max drop.  Tiles are staged by TMA through
 // per-graph tensor maps kept in device memory (encoded once per plan) into
-// the same 4-stage mbarrier ring as the single srgemm, with the barrier
+// the same kSimtStages-deep mbarrier ring as the single srgemm (the launch
+// sizes shared memory from that same constant), with the barrier
 // phases running on across tiles and graphs; the epilogue of iteration t
 // writes both layouts of X_{t+1} and a per-graph change flag, then a
 // generic-to-async proxy fence orders those writes before the next step's
