@@ -371,6 +371,65 @@ def min_plus_8192(dev, reps=3):
             "how": f"srgemm_simt_kernel, {reps} launches with C; kernel time from CUDA events on the launching stream"}
 
 
+def learned_dispatch_mixed(dev, params, weights_path, count=64):
+    """min_plus APSP closures of the 64 mixed-density R-MAT graphs (n in
+    {4096, 8192, 16384}, average degree 4..4096) under three policies of
+    simd2_closure_ex: the plain dense path, the hand-written rules (sparse
+    steps under fixed thresholds, then the autotuner's best fixed dense
+    configuration) and the learned dispatch (the MLP chooses every step,
+    sparse or dense).  Wall clock per call (each call synchronizes); outputs
+    are compared bit for bit with the dense path's."""
+    import torch
+
+    import simd2_b200 as s2
+    from simd2_b200 import datagen
+
+    with open(weights_path) as f:
+        rules_cfg = int(json.load(f).get("training", {}).get("best_fixed_config", s2.config_id(2, True)))
+    arms = (("dense", {"dispatch": "dense"}), ("rules", {"dispatch": "rules", "config": rules_cfg}),
+            ("learned", {"dispatch": "learned", "mlp_params": params}))
+    # warm-up per size: workspaces and kernels outside the timing
+    for n in (4096, 8192, 16384):
+        g = datagen.rmat_graph_device(n, 8.0, seed=1, device=dev)
+        for _, kw in arms:
+            s2.closure_ex("min_plus", g.clone(), **kw)
+        del g
+    rows, tot = [], {a: 0.0 for a, _ in arms}
+    identical = True
+    for n, deg, seed in datagen.rmat_mixed_set(count):
+        g = datagen.rmat_graph_device(n, deg, seed=seed, device=dev)
+        res, ref, ref_it = {}, None, None
+        for name, kw in arms:
+            X = g.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            it = s2.closure_ex("min_plus", X, **kw)
+            res[name] = (time.perf_counter() - t0) * 1e3
+            if ref is None:
+                ref, ref_it = X, it
+            else:
+                identical &= it == ref_it and bool(torch.equal(X.view(torch.int32), ref.view(torch.int32)))
+                del X
+        # the learned steps' choices, from a recorded (untimed) call
+        r = s2.closure_ex("min_plus", g.clone(), record=True, **dict(arms)["learned"])
+        cfgs = "".join("s" if c == s2.SPARSE_CONFIG else str(c) for c in r["configs"])
+        for a in res:
+            tot[a] += res[a]
+        rows.append({"n": n, "degree": deg, "iters": ref_it, **{f"{a}_ms": round(v, 3) for a, v in res.items()},
+                     "learned_steps": cfgs})
+        del g, ref
+    return {"graphs": len(rows), "dense_ms": tot["dense"], "rules_ms": tot["rules"], "learned_ms": tot["learned"],
+            "speedup_learned_vs_dense": tot["dense"] / tot["learned"],
+            "speedup_rules_vs_dense": tot["dense"] / tot["rules"],
+            "mlp_gain_learned_vs_rules": tot["rules"] / tot["learned"], "outputs_identical": identical,
+            "rules_dense_config": s2.config_desc(rules_cfg),
+            "learned_steps_legend": "per step: s = CSR SpGEMM step, else the dense config id (split = 1 << (id & 3), "
+                                    "skip = id >> 2)",
+            "per_graph": rows,
+            "how": "simd2_closure_ex wall clock per graph (synchronous calls, no recording); R-MAT a=.57 b=.19 c=.19 "
+                   "drawn on the GPU (datagen.rmat_mixed_set / rmat_graph_device), weights 1..100"}
+
+
 def extra_measurements(args, dev):
     """The metric's other two parts, on one GPU: batched APSP graphs/s against
     per-graph launches, and the learned dispatch against the plain dense path
@@ -540,34 +599,10 @@ def extra_measurements(args, dev):
     del A, B, Dp
     out["dense_contraction"] = cfg4
 
-    # --- learned dispatch on mixed-density R-MAT (a=.57 b=.19 c=.19), vs the plain dense path
+    # --- learned dispatch on mixed-density R-MAT (a=.57 b=.19 c=.19): plain dense path,
+    # the hand-written rules, and the MLP's choices
     if params is not None:
-        rows = []
-        td = tl = 0.0
-        identical = True
-        for i, (n, d) in enumerate([(4096, 4), (4096, 64), (4096, 1024), (8192, 4), (8192, 64), (8192, 1024)]):
-            g = torch.from_numpy(datagen.rmat_graph(n, d, seed=500 + i)).to(dev)
-            # warm-up of both policies: workspaces are allocated outside the timing
-            s2.closure_ex("min_plus", g.clone(), dispatch="dense")
-            s2.closure_ex("min_plus", g.clone(), dispatch="learned", mlp_params=params)
-            Xa, Xb = g.clone(), g.clone()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            ita = s2.closure_ex("min_plus", Xa, dispatch="dense")
-            t1 = time.perf_counter()
-            itb = s2.closure_ex("min_plus", Xb, dispatch="learned", mlp_params=params)
-            t2 = time.perf_counter()
-            rb = s2.closure_ex("min_plus", g.clone(), dispatch="learned", mlp_params=params, record=True)
-            same = bool(torch.equal(Xa.view(torch.int32), Xb.view(torch.int32))) and ita == itb
-            identical &= same
-            td += (t1 - t0) * 1e3
-            tl += (t2 - t1) * 1e3
-            rows.append({"n": n, "degree": d, "iters": ita, "dense_ms": (t1 - t0) * 1e3,
-                         "learned_ms": (t2 - t1) * 1e3, "learned_configs": [s2.config_desc(c) for c in rb["configs"]]})
-            del g, Xa, Xb
-        out["learned_dispatch"] = {"graphs": rows, "dense_ms": td, "learned_ms": tl, "speedup": td / tl,
-                                   "outputs_identical": identical,
-                                   "how": "wall clock of simd2_closure_ex per graph, dense vs learned"}
+        out["learned_dispatch"] = learned_dispatch_mixed(dev, params, weights)
     return out
 
 

@@ -163,30 +163,42 @@ int simd2_srgemm_tuned(simd2_op op, int M, int N, int K,
 typedef enum simd2_dispatch {
   SIMD2_DISPATCH_DENSE = 0,   /* no block skipping; split-K chosen from the tile count
                                  (the plain autotuned dense path) */
-  SIMD2_DISPATCH_FIXED = 1,   /* `fixed_config` every step */
-  SIMD2_DISPATCH_LEARNED = 2  /* the MLP cost model picks each step's config */
+  SIMD2_DISPATCH_FIXED = 1,   /* `fixed_config` every step (8: sparse steps, see below) */
+  SIMD2_DISPATCH_LEARNED = 2, /* the MLP cost model picks each step's config, sparse or dense */
+  SIMD2_DISPATCH_RULES = 3    /* the hand-written policy: sparse steps under fixed
+                                 thresholds, then `fixed_config` (no MLP) */
 } simd2_dispatch;
 
 /* simd2_closure with a dispatch policy.  mlp_params: device array of
  * simd2_mlp_param_count() floats (LEARNED only).  Optional host outputs of
- * max_iter entries: step_configs (config run per step), step_ms (device time
- * of each step), step_features (7 floats per step: the cost-model features).
- * Results are bit-identical for every policy.  LEARNED decides per step only
- * for n > 1024: a decision (occupancy pass, MLP launch, host round trip) costs
- * about as much as a whole dense step below that, so smaller closures run the
- * DENSE path (step_features then stay zero).  Above that, with SIMD2_CONV_EXACT
- * and a semiring simd2_spgemm_compute supports, LEARNED first squares X as a
- * CSR SpGEMM while X holds at most n^2/32 entries and the step forms at most
- * n^3/256 products (a result past n^2/32 entries is written densely and ends
- * the opening; sparse steps are recorded as config 8, features zero).  The
- * dense steps then follow the MLP's per-step choice for n > 2048, and the
- * DENSE path for 1024 < n <= 2048. */
+ * max_iter entries: step_configs (config run per step; 8 = a CSR SpGEMM
+ * step), step_ms (device time of each step), step_features (9 floats per
+ * step: the cost-model features).  Results are bit-identical for every
+ * policy.
+ *
+ * LEARNED and RULES decide per step only for n > 1024: a decision (statistics
+ * pass, MLP launch, host round trip) costs about as much as a whole dense
+ * step below that, so smaller closures run the DENSE path (step_features then
+ * stay zero).  Above that, with SIMD2_CONV_EXACT and a semiring
+ * simd2_spgemm_compute supports, both open with CSR SpGEMM steps while X
+ * holds at most n^2/32 entries (a result past that is written densely and
+ * ends the opening):
+ *   LEARNED runs a sparse step when the MLP predicts it faster than every
+ *   dense configuration (steps past n^3/16 products are never sparse);
+ *   RULES runs it when the step forms at most n^3/256 products.
+ * The dense steps then follow the MLP's per-step choice (LEARNED) or
+ * fixed_config (RULES) for n > 2048, and the DENSE path for
+ * 1024 < n <= 2048.  Once every block of X is occupied no step can skip, and
+ * both keep the last split factor without the statistics pass.
+ * FIXED with fixed_config 8 runs sparse steps while X holds at most n^2/32
+ * entries and a step forms at most n^3/16 products, then the DENSE path: the
+ * autotuner records sparse-step times with it. */
 int simd2_closure_ex(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_conv conv,
                      simd2_dispatch dispatch, int fixed_config, const float* mlp_params,
                      int* iters_out, int* step_configs, float* step_ms, float* step_features,
                      cudaStream_t stream);
 
-/* Cost-model MLP (12-32-32-1, ReLU) kernels.  X: [batch][12] features+config,
+/* Cost-model MLP (15-32-32-1, ReLU) kernels.  X: [batch][15] features+config,
  * y: [batch] targets (log2 ms).  simd2_mlp_gradient writes d/dparams of
  * mean((f(X)-y)^2) to grad (param_count floats) using sample_grads
  * ([batch][param_count] floats) as scratch; the batch sum is deterministic.

@@ -1,12 +1,12 @@
 """FP64 CPU oracle of the cost-model MLP -- TEST INFRASTRUCTURE ONLY.
 
-Restates the 12-32-32-1 ReLU network of simd2_b200/csrc/mlp.cuh (flat
+Restates the 15-32-32-1 ReLU network of simd2_b200/csrc/mlp.cuh (flat
 parameter layout W1|b1|W2|b2|W3|b3) with its forward pass and the gradient of
 mean((f(X) - y)^2), in float64, to check the GPU training kernels.
 """
 import numpy as np
 
-N_IN, H = 12, 32
+N_IN, H = 15, 32
 
 
 def unpack(p):

@@ -197,7 +197,8 @@ def srgemm_f16(op: str, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None
 
 
 NUM_CONFIGS = 8
-DISPATCH = {"dense": 0, "fixed": 1, "learned": 2}
+DISPATCH = {"dense": 0, "fixed": 1, "learned": 2, "rules": 3}
+SPARSE_CONFIG = NUM_CONFIGS  # a CSR SpGEMM closure step
 
 
 def config_id(split: int, skip: bool) -> int:
@@ -230,21 +231,25 @@ def closure_ex(op: str, X: torch.Tensor, dispatch: str = "dense", config: int = 
                max_iter: int = 500, conv: str = "exact", record: bool = False, stream=None):
     """Closure with a per-step dispatch policy.
 
-    ``dispatch``: "dense" (the plain path), "fixed" (``config`` every step) or
-    "learned": above n = 1024 (bitwise change test, a semiring the SpGEMM
-    supports) sparse steps run as CSR SpGEMM while X is sparse (recorded as
-    config ``NUM_CONFIGS``), then the MLP in ``mlp_params`` picks each dense
-    step's configuration (n > 2048; the plain path for smaller n).  Every
-    policy gives the same bits and step count.
+    ``dispatch``: "dense" (the plain path), "fixed" (``config`` every step;
+    ``SPARSE_CONFIG`` runs CSR SpGEMM steps while X fits the sparse store,
+    then the plain path), "learned" (above n = 1024, bitwise change test: the
+    MLP in ``mlp_params`` chooses each step between the dense configurations
+    and, while X is sparse, a CSR SpGEMM step) or "rules" (the hand-written
+    policy: sparse steps under fixed entry and product thresholds, then
+    ``config`` for the dense steps).  Every policy gives the same bits and
+    step count.
 
     Returns the step count, or with ``record`` a dict with the per-step
-    configurations, device times (ms) and cost-model features.
+    configurations (``SPARSE_CONFIG`` for a sparse step), device times (ms)
+    and cost-model features (9 per step).
     """
     n = X.shape[0]
     it = ctypes.c_int(0)
     cfgs = (ctypes.c_int * max(max_iter, 1))()
     ms = (ctypes.c_float * max(max_iter, 1))()
-    feats = (ctypes.c_float * (max(max_iter, 1) * 7))()
+    nf = 9
+    feats = (ctypes.c_float * (max(max_iter, 1) * nf))()
     pp = None if mlp_params is None else ctypes.c_void_p(mlp_params.data_ptr())
     rc = lib().simd2_closure_ex(OP_ID[op], n, X.data_ptr(), _mat(X, "X"), max_iter, CONV[conv], DISPATCH[dispatch],
                                 int(config), pp, ctypes.byref(it), cfgs if record else None,
@@ -254,7 +259,7 @@ def closure_ex(op: str, X: torch.Tensor, dispatch: str = "dense", config: int = 
         return it.value
     k = it.value
     return {"iters": k, "configs": list(cfgs)[:k], "ms": list(ms)[:k],
-            "features": [list(feats)[7 * i:7 * i + 7] for i in range(k)]}
+            "features": [list(feats)[nf * i:nf * i + nf] for i in range(k)]}
 
 
 def closure(op: str, X: torch.Tensor, max_iter: int = 500, conv: str = "exact", stream=None,

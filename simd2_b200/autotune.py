@@ -1,6 +1,7 @@
 """Autotuner of the closure-step kernel configuration.
 
-Runs a closure once per configuration (split-K 1/2/4/8 x block skip) with
+Runs a closure once per configuration (split-K 1/2/4/8 x block skip, and
+the sparse configuration: CSR SpGEMM steps while X is sparse) with
 ``simd2_closure_ex(dispatch="fixed")`` and records, for every step, the
 cost-model features and each configuration's device time.  Every
 configuration computes the same bits, so step t of all runs sees the same
@@ -14,7 +15,7 @@ import math
 
 import torch
 
-from . import NUM_CONFIGS, closure_ex, config_desc
+from . import NUM_CONFIGS, SPARSE_CONFIG, closure_ex, config_desc
 
 
 _warm = set()
@@ -26,15 +27,18 @@ def warm_up(op: str, device) -> None:
         return
     from .datagen import rmat_graph
     g = torch.from_numpy(rmat_graph(256, 4.0, seed=0)).to(device)
-    for cfg in range(NUM_CONFIGS):
+    for cfg in range(NUM_CONFIGS + 1):
         closure_ex(op, g.clone(), dispatch="fixed", config=cfg)
     _warm.add((op, str(device)))
 
 
-def profile_closure(op: str, X0: torch.Tensor, configs=range(NUM_CONFIGS), repeats: int = 1, max_iter: int = 500):
+def profile_closure(op: str, X0: torch.Tensor, configs=range(NUM_CONFIGS + 1), repeats: int = 1,
+                    max_iter: int = 500):
     """Per-step timings of every configuration on one input matrix.
 
-    Returns {"n", "iters", "features": [step][7], "ms": {config: [step]}}.
+    Returns {"n", "iters", "features": [step][9], "ms": {config: [step]}};
+    the sparse configuration's list holds None for the steps it did not run
+    sparse (X too dense for the sparse store, or past n^3/16 products).
     """
     warm_up(op, X0.device)
     rec = {"n": int(X0.shape[0]), "ms": {}}
@@ -43,31 +47,38 @@ def profile_closure(op: str, X0: torch.Tensor, configs=range(NUM_CONFIGS), repea
         for _ in range(repeats):
             X = X0.clone()
             r = closure_ex(op, X, dispatch="fixed", config=cfg, max_iter=max_iter, record=True)
-            best = r["ms"] if best is None else [min(a, b) for a, b in zip(best, r["ms"])]
+            ms = r["ms"]
+            if cfg == SPARSE_CONFIG:
+                ms = [m if c == SPARSE_CONFIG else None for m, c in zip(r["ms"], r["configs"])]
+            best = ms if best is None else [None if a is None else min(a, b) for a, b in zip(best, ms)]
             rec["iters"] = r["iters"]
-            rec["features"] = r["features"]
+            if cfg != SPARSE_CONFIG:
+                rec["features"] = r["features"]
         rec["ms"][int(cfg)] = best
     return rec
 
 
 def dataset(records):
-    """(inputs [rows][12], targets log2(ms) [rows]) from profile records."""
+    """(inputs [rows][15], targets log2(ms) [rows]) from profile records."""
     from .costmodel import encode
     xs, ys = [], []
     for rec in records:
         for cfg, times in rec["ms"].items():
             for t, ms in enumerate(times):
+                if ms is None:
+                    continue
                 xs.append(encode(rec["features"][t], int(cfg)))
                 ys.append(math.log2(max(ms, 1e-4)))
     return torch.tensor(xs, dtype=torch.float32), torch.tensor(ys, dtype=torch.float32)
 
 
 def best_fixed(records):
-    """Configuration with the smallest total time over all records."""
+    """Dense configuration with the smallest total time over all records."""
     tot = {}
     for rec in records:
         for cfg, times in rec["ms"].items():
-            tot[int(cfg)] = tot.get(int(cfg), 0.0) + sum(times)
+            if int(cfg) < NUM_CONFIGS:
+                tot[int(cfg)] = tot.get(int(cfg), 0.0) + sum(times)
     return min(tot, key=tot.get), tot
 
 

@@ -1,9 +1,10 @@
 """Learned cost model of the closure-step dispatch.
 
-A 12-32-32-1 ReLU MLP predicts log2(device time in ms) of one closure step
-for each of the eight kernel configurations (split-K 1/2/4/8 x block skip)
-from seven features of the step's block occupancy (``simd2_closure_ex``
-computes them on the device).  Training and inference run on the GPU through
+A 15-32-32-1 ReLU MLP predicts log2(device time in ms) of one closure step
+for each of the eight dense kernel configurations (split-K 1/2/4/8 x block
+skip) and for a CSR SpGEMM step (configuration 8), from nine features of the
+step's matrix: its block occupancy, stored entries and the products a sparse
+step would form (``simd2_closure_ex`` computes them on the device).  Training and inference run on the GPU through
 libsimd2's own kernels (``simd2_mlp_forward``, ``simd2_mlp_gradient`` with a
 deterministic batch sum, ``simd2_mlp_adam``); the dispatcher evaluates the
 network inside ``simd2_closure_ex`` (dispatch="learned").
@@ -19,8 +20,9 @@ import torch
 
 from . import _check, _stream, lib
 
-N_IN = 12
-N_FEAT = 7
+N_IN = 15
+N_FEAT = 9
+SPARSE = 8
 HIDDEN = 32
 
 
@@ -40,9 +42,11 @@ def init_params(seed: int = 0, device="cuda") -> torch.Tensor:
 
 
 def encode(features, config: int) -> list:
-    """Cost-model input: step features + one-hot split + skip flag."""
+    """Cost-model input: step features + one-hot split + skip flag + sparse flag."""
+    if config == SPARSE:
+        return list(features) + [0.0] * 5 + [1.0]
     s = config & 3
-    return list(features) + [1.0 if j == s else 0.0 for j in range(4)] + [float(config >> 2)]
+    return list(features) + [1.0 if j == s else 0.0 for j in range(4)] + [float(config >> 2), 0.0]
 
 
 def forward(params: torch.Tensor, X: torch.Tensor, stream=None) -> torch.Tensor:
@@ -93,6 +97,11 @@ def save(params: torch.Tensor, path: str):
 
 
 def load(path: str, device="cuda") -> torch.Tensor:
+    """Weights saved by ``save``; raises unless they fit this network (the
+    dispatcher reads simd2_mlp_param_count() floats from the array)."""
     with open(path) as f:
         d = json.load(f)
+    if d.get("inputs") != N_IN or d.get("hidden") != HIDDEN or len(d["params"]) != param_count():
+        raise ValueError(f"{path}: weights of a {d.get('inputs')}-input network with {len(d['params'])} parameters, "
+                         f"not the {N_IN}-input network with {param_count()}")
     return torch.tensor(d["params"], dtype=torch.float32, device=device)

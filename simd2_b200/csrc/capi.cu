@@ -339,8 +339,13 @@ int dispatch_simt(int op, int M, int N, int K, const CUtensorMap& mA, const CUte
 struct OccPlan {
   int brA, bcA, brB, bcB;  // 32 x 32 block grid of A (M x K) and B (K x N)
   int tiles_m, tiles_n, ktiles;
-  size_t occ32A, occ32B, occA, occB, stats, total;
+  size_t occ32A, occ32B, occA, occB, stats, rowcnt, colcnt, total;
 };
+
+// Grid of occupancy_strip_kernel over a rows x cols matrix.
+inline dim3 strip_grid(int rows, int cols) {
+  return dim3((unsigned)((cols + kOccCols - 1) / kOccCols), (unsigned)((rows + kOccRows - 1) / kOccRows));
+}
 
 OccPlan make_occ_plan(int M, int N, int K, bool same) {
   OccPlan o{};
@@ -357,7 +362,9 @@ OccPlan make_occ_plan(int M, int N, int K, bool same) {
   o.occ32B = same ? o.occ32A : take((size_t)o.brB * o.bcB);
   o.occA = take((size_t)o.tiles_m * o.ktiles);
   o.occB = take((size_t)o.ktiles * o.tiles_n);
-  o.stats = take(4 * sizeof(unsigned long long));
+  o.stats = take(8 * sizeof(unsigned long long));
+  o.rowcnt = take((size_t)std::max(M, K) * sizeof(int));
+  o.colcnt = take((size_t)std::max(N, K) * sizeof(int));
   o.total = off;
   return o;
 }
@@ -370,17 +377,41 @@ int compute_occupancy(int op, int M, int N, int K, const float* A, long long lda
   const float ann = annihilator(op);
   auto* occ32A = base + o.occ32A;
   auto* occ32B = base + o.occ32B;
-  occupancy32_kernel<<<dim3(o.bcA, o.brA), dim3(32, 8), 0, stream>>>(A, lda, M, K, ann, occ32A, o.bcA);
+  occupancy_strip_kernel<false><<<strip_grid(M, K), 256, 0, stream>>>(A, lda, M, K, ann, ann, occ32A, o.bcA, nullptr,
+                                                                      nullptr);
   count_launch();
   if (!same) {
-    occupancy32_kernel<<<dim3(o.bcB, o.brB), dim3(32, 8), 0, stream>>>(B, ldb, K, N, ann, occ32B, o.bcB);
+    occupancy_strip_kernel<false><<<strip_grid(K, N), 256, 0, stream>>>(B, ldb, K, N, ann, ann, occ32B, o.bcB,
+                                                                        nullptr, nullptr);
     count_launch();
   }
   auto* stats = reinterpret_cast<unsigned long long*>(base + o.stats);
-  SIMD2_CUDA_TRY(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), stream));
+  SIMD2_CUDA_TRY(cudaMemsetAsync(stats, 0, 8 * sizeof(unsigned long long), stream));
   occupancy_panels_kernel<<<std::min(o.ktiles, 148 * 4), 256, 0, stream>>>(
       occ32A, o.bcA, o.brA, occ32B, o.bcB, o.brB, o.tiles_m, o.tiles_n, o.ktiles, base + o.occA, base + o.occB, stats);
   count_launch();
+  SIMD2_CUDA_TRY(cudaGetLastError());
+  return SIMD2_OK;
+}
+
+// The statistics of a closure step's X (n x n, A = B = X) that the cost
+// model reads: the block occupancy (skip lists and stats[0..2]) and the
+// stored entries / Gustavson products (stats[3], stats[4]), in one pass over X.
+int compute_step_stats(int op, int n, const float* X, long long ldx, uint8_t* base, const OccPlan& o,
+                       cudaStream_t stream) {
+  auto* stats = reinterpret_cast<unsigned long long*>(base + o.stats);
+  int* rowcnt = reinterpret_cast<int*>(base + o.rowcnt);
+  int* colcnt = reinterpret_cast<int*>(base + o.colcnt);
+  SIMD2_CUDA_TRY(cudaMemsetAsync(stats, 0, 8 * sizeof(unsigned long long), stream));
+  SIMD2_CUDA_TRY(cudaMemsetAsync(rowcnt, 0, (size_t)n * sizeof(int), stream));
+  SIMD2_CUDA_TRY(cudaMemsetAsync(colcnt, 0, (size_t)n * sizeof(int), stream));
+  occupancy_strip_kernel<true><<<strip_grid(n, n), 256, 0, stream>>>(X, ldx, n, n, annihilator(op), add_identity(op),
+                                                                     base + o.occ32A, o.bcA, rowcnt, colcnt);
+  occupancy_panels_kernel<<<std::min(o.ktiles, 148 * 4), 256, 0, stream>>>(
+      base + o.occ32A, o.bcA, o.brA, base + o.occ32A, o.bcA, o.brA, o.tiles_m, o.tiles_n, o.ktiles, base + o.occA,
+      base + o.occB, stats);
+  count_products_kernel<<<grid_for(n), 256, 0, stream>>>(n, rowcnt, colcnt, stats);
+  for (int i = 0; i < 3; i++) count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
 }
@@ -815,9 +846,26 @@ int dense_split(int n, int sms) {
 
 constexpr int kOrAndSparseMinN = 8192;
 
+// How a closure's sparse opening decides, step by step, whether the next
+// squaring runs as a CSR SpGEMM step.  Every policy gives the same bits.
+struct OpeningPolicy {
+  // a step forming more products than this is never run sparse
+  unsigned long long max_products = 0;
+  // learned: the MLP in `mlp` compares the sparse step with the dense
+  // configurations from the step's statistics (computed into the occupancy
+  // workspace `obase` / `occ`); null: every step under max_products runs sparse
+  const float* mlp = nullptr;
+  uint8_t* obase = nullptr;
+  const OccPlan* occ = nullptr;
+  int* decision = nullptr;  // device int[1 + kSparseConfig + 1]
+  int sms = 148;
+  int can_skip = 0;
+  float* step_feat = nullptr;  // optional: features of each opening step (kMlpFeat each)
+};
+
 // Defined with the SpGEMM host code below.
-int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, int* steps, bool* changed,
-                           int* step_cfg, float* step_ms, cudaStream_t stream);
+int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, const OpeningPolicy& pol,
+                           int* steps, bool* changed, int* step_cfg, float* step_ms, cudaStream_t stream);
 int closure_sparse_opening_u8(int n, uint8_t* X, long long ldx, int max_iter, int* steps, bool* changed,
                               cudaStream_t stream);
 
@@ -916,21 +964,33 @@ int closure_gated(int op, int n, float* X, long long ldx, int max_iter, int conv
 
 // Closure by repeated squaring with a per-step kernel configuration:
 //   dispatch 0 (dense)  : no skip, split-K from the tile count (the plain path);
-//   dispatch 1 (fixed)  : `fixed_cfg` (split = 1 << (cfg & 3), skip = cfg >> 2) every step;
-//   dispatch 2 (learned): block occupancy of X_t -> features -> the MLP
-//                         `mlp_params` predicts each configuration's time and
-//                         the cheapest one runs.
+//   dispatch 1 (fixed)  : `fixed_cfg` every step: a dense configuration
+//                         (split = 1 << (cfg & 3), skip = cfg >> 2), or
+//                         kSparseConfig: CSR SpGEMM steps for as long as X fits
+//                         the sparse store (under n^3/16 products), then the
+//                         plain dense steps (used to record sparse-step times);
+//   dispatch 2 (learned): per step, the statistics of X_t -> features -> the
+//                         MLP `mlp_params` predicts the time of every dense
+//                         configuration and, while X_t is sparse, of a CSR
+//                         SpGEMM step; the cheapest one runs;
+//   dispatch 3 (rules)  : the hand-written policy without the MLP: sparse
+//                         steps while X_t holds at most n^2/32 entries and the
+//                         step forms at most n^3/256 products, then `fixed_cfg`
+//                         for every dense step.
 // Every configuration computes the same bits, so the dispatch only moves time.
 // step_cfg / step_ms / step_feat (host arrays of max_iter, max_iter,
 // max_iter * kMlpFeat entries, each optional) record what each step ran, its
-// device time (occupancy + operand prep + srgemm) and its features.
+// device time (operand prep + srgemm, plus the occupancy pass of a skipping
+// step; a sparse step's count and fill passes, the first one with X's
+// conversion to CSR) and its features.
 int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int conv, int dispatch, int fixed_cfg,
                    const float* mlp_params, int* iters_out, int* step_cfg, float* step_ms, float* step_feat,
                    cudaStream_t stream) {
   if (iters_out) *iters_out = 0;
   if (n < 0 || max_iter < 0 || !is_float_op(op) || is_sum_op(op) || (n > 0 && (!X || ldx < n)))
     return SIMD2_ERR_INVALID_ARG;
-  if (dispatch < 0 || dispatch > 2 || (dispatch == 2 && !mlp_params) || fixed_cfg < 0 || fixed_cfg >= kNumConfigs)
+  if (dispatch < 0 || dispatch > 3 || (dispatch == 2 && !mlp_params) || fixed_cfg < 0 ||
+      fixed_cfg > (dispatch == 1 ? kSparseConfig : kNumConfigs - 1))
     return SIMD2_ERR_INVALID_ARG;
   if (n == 0 || max_iter == 0) return SIMD2_OK;
   int rc = check_device();
@@ -941,40 +1001,21 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     SIMD2_CUDA_TRY(cudaGetDevice(&dev));
     SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   }
-  // A learned step costs an occupancy pass, the MLP launch and a host round
+  const bool fixed_sparse = dispatch == 1 && fixed_cfg == kSparseConfig;
+  // A learned step costs a statistics pass, the MLP launch and a host round
   // trip (about 25 us together on B200).  Up to n = kLearnedMinN a whole dense
   // step costs about as much (2n^3 <= 2.1 Gop, under 70 us on 148 SMs), so no
-  // choice can win back its decision and the plain gated path runs instead.
-  if (dispatch == 2 && n <= kLearnedMinN) {
+  // choice can win back its decision and the plain gated path runs instead;
+  // the rules policy does the same.
+  if ((dispatch == 2 || dispatch == 3) && n <= kLearnedMinN) {
     dispatch = 0;
     if (step_feat) std::fill(step_feat, step_feat + (size_t)max_iter * kMlpFeat, 0.f);
     step_feat = nullptr;
   }
-  // The learned policy opens with sparse steps while X is sparse (see
-  // closure_sparse_opening; bitwise change test only).
-  int it0 = 0;
-  if (dispatch == 2 && conv == SIMD2_CONV_EXACT) {
-    bool ch = true;
-    if ((rc = closure_sparse_opening(op, n, X, ldx, max_iter, &it0, &ch, step_cfg, step_ms, stream))) return rc;
-    if (step_feat) std::fill(step_feat, step_feat + (size_t)it0 * kMlpFeat, 0.f);
-    if (!ch || it0 == max_iter) {
-      if (iters_out) *iters_out = it0;
-      return ch ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
-    }
-    max_iter -= it0;
-    if (step_cfg) step_cfg += it0;
-    if (step_ms) step_ms += it0;
-    if (step_feat) step_feat += (size_t)it0 * kMlpFeat;
-    // Up to n = kLearnedLoopMinN the MLP's per-step choice (measured on R-MAT
-    // graphs) gains less than its decisions cost: the gated dense path goes on.
-    if (n <= kLearnedLoopMinN) {
-      dispatch = 0;
-      if (step_feat) std::fill(step_feat, step_feat + (size_t)max_iter * kMlpFeat, 0.f);
-      step_feat = nullptr;
-    }
-  }
   const bool can_skip = skip_supported(op) && (n + kBK - 1) / kBK <= kMaxSkipKtiles;
-  const bool need_occ = dispatch == 2 || step_feat != nullptr || (dispatch == 1 && config_skip(fixed_cfg) && can_skip);
+  const bool opening = (dispatch == 2 || dispatch == 3 || fixed_sparse) && conv == SIMD2_CONV_EXACT;
+  const bool fixed_skip = (dispatch == 1 || dispatch == 3) && fixed_cfg < kNumConfigs && config_skip(fixed_cfg);
+  const bool need_occ = dispatch == 2 || step_feat != nullptr || (fixed_skip && can_skip);
   // Workspace: [srgemm plan][Xnew n x n][flag + decision][occupancy]
   const bool pack_a = !a_tma_ok(X, ldx) || (n % 4 != 0);
   const Plan plan = make_plan(n, n, n, pack_a, selection_op(op));
@@ -989,46 +1030,90 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   uint8_t* ws = static_cast<uint8_t*>(p);
   float* Xn = reinterpret_cast<float*>(ws + x_off);
   int* flag = reinterpret_cast<int*>(ws + f_off);
-  int* decision = flag + 8;  // [0] config, [1..8] predictions
+  int* decision = flag + 8;  // [0] config, [1 + c] prediction of config c
   uint8_t* obase = ws + o_off;
 
-  if (dispatch != 2 && step_feat == nullptr) {
+  // The opening: sparse steps while X is sparse, under the dispatch's policy
+  // (bitwise change test only).
+  int it0 = 0;
+  if (opening) {
+    const unsigned long long n3 = (unsigned long long)n * (unsigned long long)n * (unsigned long long)n;
+    OpeningPolicy pol;
+    // A sparse step past n^3/16 products would cost at least 9x a dense step
+    // at the measured rates (about 120 G products/s against 17 T MAC/s), so
+    // neither the learned nor the recording policy considers it; the rules
+    // policy keeps a step sparse only under n^3/256 (two thirds of a dense step).
+    pol.max_products = dispatch == 3 ? n3 / 256ull : n3 / 16ull;
+    if (dispatch == 2) {
+      pol.mlp = mlp_params;
+      pol.obase = obase;
+      pol.occ = &occ;
+      pol.decision = decision;
+      pol.sms = sms;
+      pol.can_skip = can_skip ? 1 : 0;
+      pol.step_feat = step_feat;
+    }
+    bool ch = true;
+    if (step_feat) std::fill(step_feat, step_feat + (size_t)max_iter * kMlpFeat, 0.f);
+    if ((rc = closure_sparse_opening(op, n, X, ldx, max_iter, pol, &it0, &ch, step_cfg, step_ms, stream))) return rc;
+    if (!ch || it0 == max_iter) {
+      if (iters_out) *iters_out = it0;
+      return ch ? SIMD2_ERR_NOT_CONVERGED : SIMD2_OK;
+    }
+    max_iter -= it0;
+    if (step_cfg) step_cfg += it0;
+    if (step_ms) step_ms += it0;
+    if (step_feat) step_feat += (size_t)it0 * kMlpFeat;
+    // Up to n = kLearnedLoopMinN a per-step choice (measured on R-MAT graphs)
+    // gains less than its decisions cost: the gated dense path goes on.
+    if ((dispatch == 2 || dispatch == 3) && n <= kLearnedLoopMinN) {
+      dispatch = 0;
+      if (step_feat) std::fill(step_feat, step_feat + (size_t)max_iter * kMlpFeat, 0.f);
+      step_feat = nullptr;
+    }
+  }
+  if (fixed_sparse) dispatch = 0;  // the dense steps after a recorded opening run the plain path
+
+  const bool per_step = dispatch == 2 || dispatch == 3 || step_feat != nullptr;
+  if (!per_step) {
     int it2 = 0;
     rc = closure_gated(op, n, X, ldx, max_iter, conv, fixed_cfg, dispatch == 1, can_skip, need_occ, occ, ws, x_off,
                        reinterpret_cast<int*>(ws + f_off + 256), obase, &it2, step_cfg, step_ms, sms, stream);
     if (iters_out) *iters_out = it0 + it2;
     return rc;
   }
-  // Per-step loop (learned dispatch, or feature recording): the occupancy and
-  // the cost-model choice for step t+1 are enqueued right after step t's
-  // srgemm, so one host synchronisation per step reads step t's change flag
-  // together with step t+1's decision (and features).
+  // Per-step loop (learned or rules dispatch, or feature recording): the
+  // statistics and the cost-model choice for step t+1 are enqueued right after
+  // step t's srgemm, so one host synchronisation per step reads step t's
+  // change flag together with step t+1's decision (and features).
+  const bool want_feat = dispatch == 2 || step_feat != nullptr;
   cudaEvent_t ev[4] = {};  // srgemm start/end, occupancy start/end
   if (step_ms)
     for (auto& e : ev) SIMD2_CUDA_TRY(cudaEventCreate(&e));
   float occ_ms = 0.f;
   auto enqueue_occ = [&](const float* m, long long ld) -> int {
     if (step_ms) cudaEventRecord(ev[2], stream);
-    int r = compute_occupancy(op, n, n, n, m, ld, m, ld, true, obase, occ, stream);
+    int r = want_feat ? compute_step_stats(op, n, m, ld, obase, occ, stream)
+                      : compute_occupancy(op, n, n, n, m, ld, m, ld, true, obase, occ, stream);
     if (r) return r;
     if (dispatch == 2) {
       mlp_choose_kernel<<<1, 32, 0, stream>>>(mlp_params, reinterpret_cast<unsigned long long*>(obase + occ.stats), n,
-                                              occ.tiles_m, occ.tiles_n, occ.ktiles, sms, can_skip ? 1 : 0, 8,
+                                              occ.tiles_m, occ.tiles_n, occ.ktiles, sms, can_skip ? 1 : 0, 8, 0,
                                               decision);
       count_launch();
     }
     if (step_ms) cudaEventRecord(ev[3], stream);
     return SIMD2_OK;
   };
-  // host copies of {flag, decision[0..8]} and the occupancy statistics
+  // host copies of {flag, decision[0..8]} and the step statistics
   int hbuf[9] = {};
-  unsigned long long hst[3] = {};
+  unsigned long long hst[5] = {};
   auto read_back = [&](bool want_flag, bool want_dec) -> int {
     if (want_flag || want_dec) {
       if (cudaMemcpyAsync(hbuf, flag, sizeof(hbuf), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
         return SIMD2_ERR_CUDA;
     }
-    if (want_dec && (step_feat || dispatch == 2)) {
+    if (want_dec) {
       if (cudaMemcpyAsync(hst, obase + occ.stats, sizeof(hst), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
         return SIMD2_ERR_CUDA;
     }
@@ -1037,7 +1122,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     return SIMD2_OK;
   };
   const int ds = dense_split(n, sms);
-  const int default_cfg = dispatch == 1 ? fixed_cfg : (ds == 1 ? 0 : ds == 2 ? 1 : 2);
+  const int default_cfg = dispatch == 1 || dispatch == 3 ? fixed_cfg : (ds == 1 ? 0 : ds == 2 ? 1 : 2);
   float* cur = X;
   long long ldcur = ldx;
   float* nxt = Xn;
@@ -1046,20 +1131,21 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   int changed = 1;
   int cfg_id = default_cfg;
   // Closure steps only fill X in: once every (tile, k-tile) block triple is
-  // occupied, no later step can skip anything, so the learned loop stops the
-  // occupancy pass and runs the dense configuration (feature recording keeps it).
+  // occupied, no later step can skip anything, so the learned and rules loops
+  // stop the statistics pass and keep the split factor of the last choice
+  // without skipping (feature recording keeps the pass).
   const unsigned long long all_triples = (unsigned long long)occ.tiles_m * occ.tiles_n * occ.ktiles;
   bool occ_on = need_occ;
   auto settle = [&]() {
-    if (dispatch == 2 && !step_feat && hst[0] >= all_triples) {
+    if ((dispatch == 2 || dispatch == 3) && !step_feat && hst[0] >= all_triples) {
       occ_on = false;
-      cfg_id = default_cfg;
+      cfg_id &= 3;
     }
   };
   if (need_occ) {
     if ((rc = enqueue_occ(cur, ldcur)) || (rc = read_back(false, true))) return rc;
     if (dispatch == 2) cfg_id = hbuf[8];  // decision[0]
-    if (step_feat) mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst[0], hst[1], hst[2], sms, step_feat);
+    if (step_feat) mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst, sms, step_feat);
     settle();
   }
   while (changed && it < max_iter) {
@@ -1084,7 +1170,8 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     if (rc) break;
     if (step_ms) cudaEventRecord(ev[1], stream);
     it++;
-    const bool next = occ_on && it < max_iter;
+    // the rules policy needs no statistics for a configuration that does not skip
+    const bool next = occ_on && it < max_iter && (dispatch != 3 || config_skip(cfg_id) || step_feat);
     if (next && (rc = enqueue_occ(nxt, ldnxt))) break;
     float srg_ms = 0.f;
     if ((rc = read_back(true, next))) break;
@@ -1096,8 +1183,7 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     if (next) {
       if (dispatch == 2) cfg_id = hbuf[8];
       if (step_feat && changed)
-        mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst[0], hst[1], hst[2], sms,
-                     step_feat + (size_t)it * kMlpFeat);
+        mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst, sms, step_feat + (size_t)it * kMlpFeat);
       settle();
     }
     std::swap(cur, nxt);
@@ -1133,12 +1219,15 @@ struct BatchedPlan {
   BatchMaps* d_maps;
   int* d_order;
   int* d_queue;
+  bool fp16;            // FP16 copies exist (max_min / min_max, change test other than APLP)
+  int* d_fp16_bad;      // set by the FP16 prep when an entry is not an FP16 value
   std::vector<BatchGraph> host;
 };
 
-template <int OP>
+template <int OP, bool H2>
 int launch_batched(BatchedPlan* p, cudaStream_t stream) {
-  auto kern = closure_batched_kernel<OP>;
+  auto kern = H2 ? closure_batched_h2_kernel<(OP == SIMD2_MIN_MAX ? SIMD2_MIN_MAX : SIMD2_MAX_MIN)>
+                 : closure_batched_kernel<OP>;
   const size_t smem = simt_smem_bytes(kSimtStages);
   static bool configured[64] = {};
   if (!configured[p->dev]) {
@@ -1149,7 +1238,7 @@ int launch_batched(BatchedPlan* p, cudaStream_t stream) {
   SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->dev));
   const int grid = std::max(1, std::min(sms, p->count));
   kern<<<grid, kSimtThreads, smem, stream>>>(p->d_graphs, p->d_maps, p->d_order, p->count, p->d_queue, p->max_iter,
-                                             p->conv);
+                                             p->conv, p->fp16 ? p->d_fp16_bad : nullptr);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
@@ -1158,21 +1247,34 @@ int launch_batched(BatchedPlan* p, cudaStream_t stream) {
 int batched_run(BatchedPlan* p, cudaStream_t stream) {
   SIMD2_CUDA_TRY(cudaMemsetAsync(p->d_queue, 0, sizeof(int), stream));
   dim3 pg(64, std::min(p->count, 65535));
-  batched_prep_kernel<<<pg, 256, 0, stream>>>(p->d_graphs, p->count);
+  const int* bad = p->fp16 ? p->d_fp16_bad : nullptr;
+  if (p->fp16) {
+    // FP16 copies first; they flag an entry that is not an FP16 value, and the
+    // FP32 prep and kernel below run only then (the FP16 kernel otherwise)
+    SIMD2_CUDA_TRY(cudaMemsetAsync(p->d_fp16_bad, 0, sizeof(int), stream));
+    batched_prep_h_kernel<<<pg, 256, 0, stream>>>(p->d_graphs, p->count, p->d_fp16_bad);
+    count_launch();
+  }
+  batched_prep_kernel<<<pg, 256, 0, stream>>>(p->d_graphs, p->count, bad);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   int rc;
   switch (p->op) {
-    case SIMD2_MIN_PLUS: rc = launch_batched<SIMD2_MIN_PLUS>(p, stream); break;
-    case SIMD2_MAX_PLUS: rc = launch_batched<SIMD2_MAX_PLUS>(p, stream); break;
-    case SIMD2_MAX_MIN: rc = launch_batched<SIMD2_MAX_MIN>(p, stream); break;
-    case SIMD2_MAX_MUL: rc = launch_batched<SIMD2_MAX_MUL>(p, stream); break;
-    case SIMD2_MIN_MUL: rc = launch_batched<SIMD2_MIN_MUL>(p, stream); break;
-    case SIMD2_MIN_MAX: rc = launch_batched<SIMD2_MIN_MAX>(p, stream); break;
+    case SIMD2_MIN_PLUS: rc = launch_batched<SIMD2_MIN_PLUS, false>(p, stream); break;
+    case SIMD2_MAX_PLUS: rc = launch_batched<SIMD2_MAX_PLUS, false>(p, stream); break;
+    case SIMD2_MAX_MIN: rc = launch_batched<SIMD2_MAX_MIN, false>(p, stream); break;
+    case SIMD2_MAX_MUL: rc = launch_batched<SIMD2_MAX_MUL, false>(p, stream); break;
+    case SIMD2_MIN_MUL: rc = launch_batched<SIMD2_MIN_MUL, false>(p, stream); break;
+    case SIMD2_MIN_MAX: rc = launch_batched<SIMD2_MIN_MAX, false>(p, stream); break;
     default: return SIMD2_ERR_UNSUPPORTED;
   }
   if (rc) return rc;
-  batched_finish_kernel<<<pg, 256, 0, stream>>>(p->d_graphs, p->count);
+  if (p->fp16) {
+    rc = p->op == SIMD2_MAX_MIN ? launch_batched<SIMD2_MAX_MIN, true>(p, stream)
+                                : launch_batched<SIMD2_MIN_MAX, true>(p, stream);
+    if (rc) return rc;
+  }
+  batched_finish_kernel<<<pg, 256, 0, stream>>>(p->d_graphs, p->count, bad);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
@@ -1577,9 +1679,17 @@ int spgemm_fill_dense(int op, int M, int N, int K, const int* ap, const int* aj,
 // X is a 0/1 matrix (or_and), squared as max_min over stored 1.0 values.
 // *steps: steps run; *changed: false when the last one changed nothing.
 // Every step gives the dense step's bits (same contract, same result).
+// stats[3] = nnz, stats[4] = *products (device), for the cost model's features.
+__global__ void stats_from_csr_kernel(unsigned long long* stats, long long nnz, const unsigned long long* products) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    stats[3] = (unsigned long long)nnz;
+    stats[4] = *products;
+  }
+}
+
 template <typename T>
-int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, unsigned long long max_products,
-                             int* steps, bool* changed, int* step_cfg, float* step_ms, cudaStream_t stream) {
+int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, const OpeningPolicy& pol, int* steps,
+                             bool* changed, int* step_cfg, float* step_ms, cudaStream_t stream) {
   constexpr bool kBool = std::is_same<T, uint8_t>::value;
   *steps = 0;
   *changed = true;
@@ -1613,6 +1723,7 @@ int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, u
   int* flag = reinterpret_cast<int*>(ws + plan.flag_off);
   long long* tot = reinterpret_cast<long long*>(ws + plan.tot_off);
   const int rows_grid = grid_for((long long)n * 32);
+  const bool learned = pol.mlp != nullptr;
   // X as a dense matrix again (ident / 0 everywhere first)
   auto clear_x = [&]() -> int {
     if constexpr (kBool) {
@@ -1623,6 +1734,15 @@ int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, u
     }
     return SIMD2_OK;
   };
+  cudaEvent_t ev[2] = {};
+  if (step_ms)
+    for (auto& e : ev) SIMD2_CUDA_TRY(cudaEventCreate(&e));
+  auto destroy_events = [&]() {
+    if (step_ms)
+      for (auto& e : ev) cudaEventDestroy(e);
+  };
+  // the first step's time includes the conversion of X to CSR
+  if (step_ms) cudaEventRecord(ev[0], stream);
 
   // X -> CSR, when sparse enough
   SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, 12, stream));
@@ -1639,17 +1759,18 @@ int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, u
   SIMD2_CUDA_TRY(cudaMemcpyAsync(&nnz, tot, 8, cudaMemcpyDeviceToHost, stream));
   SIMD2_CUDA_TRY(cudaMemcpyAsync(&non01, flag + 2, 4, cudaMemcpyDeviceToHost, stream));
   SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
-  if (nnz > cap || non01) return SIMD2_OK;
+  if (nnz > cap || non01) {
+    destroy_events();
+    return SIMD2_OK;
+  }
   if constexpr (kBool) dense_to_csr_u8_kernel<<<rows_grid, 256, 0, stream>>>(n, n, X, ldx, rp[0], cj[0], cv[0]);
   else dense_to_csr_kernel<<<rows_grid, 256, 0, stream>>>(n, n, X, ldx, ident, rp[0], cj[0], cv[0]);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
 
-  cudaEvent_t ev[2] = {};
-  if (step_ms)
-    for (auto& e : ev) SIMD2_CUDA_TRY(cudaEventCreate(&e));
   int cur = 0, it = 0;
   bool ch = true, in_x = false;  // in_x: the last step wrote X itself
+  bool converted = false;        // the conversion's time went into a recorded step
   while (ch && it < max_iter) {
     SIMD2_CUDA_TRY(cudaMemsetAsync(colcnt, 0, (size_t)n * 4, stream));
     SIMD2_CUDA_TRY(cudaMemsetAsync(prod, 0, 8, stream));
@@ -1658,31 +1779,68 @@ int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, u
     count_launch();
     count_launch();
     SIMD2_CUDA_TRY(cudaGetLastError());
+    unsigned long long hst[5] = {};
+    if (learned) {
+      // the step's statistics from the CSR copy, then the MLP's choice between
+      // the sparse step and the dense configurations
+      const OccPlan& o = *pol.occ;
+      auto* stats = reinterpret_cast<unsigned long long*>(pol.obase + o.stats);
+      SIMD2_CUDA_TRY(cudaMemsetAsync(stats, 0, 8 * sizeof(unsigned long long), stream));
+      SIMD2_CUDA_TRY(cudaMemsetAsync(pol.obase + o.occ32A, 0, (size_t)o.brA * o.bcA, stream));
+      csr_occupancy32_kernel<<<rows_grid, 256, 0, stream>>>(n, rp[cur], cj[cur], pol.obase + o.occ32A, o.bcA);
+      occupancy_panels_kernel<<<std::min(o.ktiles, 148 * 4), 256, 0, stream>>>(
+          pol.obase + o.occ32A, o.bcA, o.brA, pol.obase + o.occ32A, o.bcA, o.brA, o.tiles_m, o.tiles_n, o.ktiles,
+          pol.obase + o.occA, pol.obase + o.occB, stats);
+      stats_from_csr_kernel<<<1, 32, 0, stream>>>(stats, nnz, prod);
+      mlp_choose_kernel<<<1, 32, 0, stream>>>(pol.mlp, stats, n, o.tiles_m, o.tiles_n, o.ktiles, pol.sms,
+                                              pol.can_skip, 8, 1, pol.decision);
+      for (int i = 0; i < 4; i++) count_launch();
+      SIMD2_CUDA_TRY(cudaGetLastError());
+      SIMD2_CUDA_TRY(cudaMemcpyAsync(hst, stats, sizeof(hst), cudaMemcpyDeviceToHost, stream));
+    }
     unsigned long long hp = 0;
+    int choice = kSparseConfig;
     SIMD2_CUDA_TRY(cudaMemcpyAsync(&hp, prod, 8, cudaMemcpyDeviceToHost, stream));
+    if (learned) SIMD2_CUDA_TRY(cudaMemcpyAsync(&choice, pol.decision, 4, cudaMemcpyDeviceToHost, stream));
     SIMD2_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (hp > max_products) break;
+    if (hp > pol.max_products || choice != kSparseConfig) break;
+    if (learned && pol.step_feat)
+      mlp_features(n, pol.occ->tiles_m, pol.occ->tiles_n, pol.occ->ktiles, hst, pol.sms,
+                   pol.step_feat + (size_t)it * kMlpFeat);
     const int nx = cur ^ 1;
-    if (step_ms) cudaEventRecord(ev[0], stream);
+    if (step_ms && converted) cudaEventRecord(ev[0], stream);
+    converted = true;
     long long nn = 0;
     rc = spgemm_count(op, n, n, n, rp[cur], cj[cur], (int)nnz, rp[cur], cj[cur], (int)nnz, rp[cur], cj[cur], (int)nnz,
                       rp[nx], &nn, ws, plan, stream);
-    if (rc && rc != kSpOverflow) return rc;
+    if (rc && rc != kSpOverflow) {
+      destroy_events();
+      return rc;
+    }
     const bool to_x = rc == kSpOverflow || nn > cap;
     if (to_x) {
       // the result is too dense for CSR: this step writes it straight into X
       // (more entries than X had, so it changed) and the dense loop goes on
-      if ((rc = clear_x())) return rc;
+      if ((rc = clear_x())) {
+        destroy_events();
+        return rc;
+      }
       SIMD2_CUDA_TRY(cudaGetLastError());
       rc = spgemm_fill_dense<T>(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur],
                                 (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz, X, ldx, ws, plan, stream);
-      if (rc) return rc;
+      if (rc) {
+        destroy_events();
+        return rc;
+      }
       in_x = true;
       ch = true;
     } else {
       rc = spgemm_fill(op, n, n, n, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur], cj[cur], cv[cur], (int)nnz, rp[cur],
                        cj[cur], cv[cur], (int)nnz, rp[nx], cj[nx], cv[nx], nn, ws, plan, stream);
-      if (rc) return rc;
+      if (rc) {
+        destroy_events();
+        return rc;
+      }
       // X' holds X's structure (C = X) plus new entries: equal counts mean equal structure
       if (nn != nnz) {
         ch = true;
@@ -1702,14 +1860,13 @@ int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, u
       cudaEventSynchronize(ev[1]);
       cudaEventElapsedTime(&step_ms[it], ev[0], ev[1]);
     }
-    if (step_cfg) step_cfg[it] = kNumConfigs;  // the sparse step
+    if (step_cfg) step_cfg[it] = kSparseConfig;
     it++;
     if (to_x) break;
     cur = nx;
     nnz = nn;
   }
-  if (step_ms)
-    for (auto& e : ev) cudaEventDestroy(e);
+  destroy_events();
   if (it > 0 && !in_x) {
     if ((rc = clear_x())) return rc;
     if constexpr (kBool) csr_scatter_u8_kernel<<<rows_grid, 256, 0, stream>>>(n, rp[cur], cj[cur], X, ldx);
@@ -1723,14 +1880,10 @@ int closure_sparse_opening_t(int op, int n, T* X, long long ldx, int max_iter, u
   return SIMD2_OK;
 }
 
-// The learned float closure's opening: a step under n^3/256 products (at
-// B200's rates of about 100 G products/s sparse and 17 T MAC/s on the
-// CUDA-core dense kernel, under two thirds of a dense step's time).
-int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, int* steps, bool* changed,
-                           int* step_cfg, float* step_ms, cudaStream_t stream) {
-  const unsigned long long nn2 = (unsigned long long)n * (unsigned long long)n;
-  return closure_sparse_opening_t<float>(op, n, X, ldx, max_iter, nn2 * (unsigned long long)n / 256ull, steps, changed,
-                                         step_cfg, step_ms, stream);
+// The float closure's sparse opening under a policy (see OpeningPolicy).
+int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter, const OpeningPolicy& pol,
+                           int* steps, bool* changed, int* step_cfg, float* step_ms, cudaStream_t stream) {
+  return closure_sparse_opening_t<float>(op, n, X, ldx, max_iter, pol, steps, changed, step_cfg, step_ms, stream);
 }
 
 // The or_and closure's opening: the dense step runs on the INT8 tensor cores
@@ -1738,8 +1891,10 @@ int closure_sparse_opening(int op, int n, float* X, long long ldx, int max_iter,
 int closure_sparse_opening_u8(int n, uint8_t* X, long long ldx, int max_iter, int* steps, bool* changed,
                               cudaStream_t stream) {
   const unsigned long long nn2 = (unsigned long long)n * (unsigned long long)n;
-  return closure_sparse_opening_t<uint8_t>(SIMD2_MAX_MIN, n, X, ldx, max_iter, nn2 * (unsigned long long)n / 16384ull,
-                                           steps, changed, nullptr, nullptr, stream);
+  OpeningPolicy pol;
+  pol.max_products = nn2 * (unsigned long long)n / 16384ull;
+  return closure_sparse_opening_t<uint8_t>(SIMD2_MAX_MIN, n, X, ldx, max_iter, pol, steps, changed, nullptr, nullptr,
+                                           stream);
 }
 
 }  // namespace
@@ -2120,24 +2275,36 @@ int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int
   p->max_iter = max_iter;
   p->conv = conv;
   p->host.resize(count);
-  // layout: [graphs][order][queue] then per-graph buffers
+  // the FP16 path of the selection semirings (the APLP change test writes
+  // -FLT_MAX, which is no FP16 value)
+  p->fp16 = selection_op(op) && conv != SIMD2_CONV_APLP;
+  // layout: [graphs][order][queue][FP16 flag] then per-graph buffers
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
   const size_t g_off = take(sizeof(BatchGraph) * std::max(count, 1));
   const size_t m_off = take(sizeof(BatchMaps) * std::max(count, 1));
   const size_t o_off = take(sizeof(int) * std::max(count, 1));
   const size_t q_off = take(sizeof(int));
+  const size_t f_off = take(sizeof(int));
   std::vector<size_t> buf_off(count);
+  auto half_bytes = [&](const BatchGraph& G, size_t* xh, size_t* ph) {
+    *xh = p->fp16 ? (size_t)G.Mp * G.Kh * 2 : 0;
+    *ph = p->fp16 ? (size_t)(G.Kh / 2) * G.Np * 4 : 0;
+  };
   for (int g = 0; g < count; g++) {
     BatchGraph& G = p->host[g];
     G.n = n[g];
     G.Mp = round_up(std::max(n[g], 1), kBM);
     G.Kp = round_up(std::max(n[g], 1), kBK);
     G.Np = round_up(std::max(n[g], 1), kBN);
+    G.Kh = round_up(std::max(n[g], 1), kH2BK);
     G.user = X[g];
     G.ldu = ldx[g];
     const size_t xb = (size_t)G.Mp * G.Kp * 4, pb = (size_t)(G.Kp / 2) * 2 * G.Np * 4;
+    size_t xh, ph;
+    half_bytes(G, &xh, &ph);
     buf_off[g] = take(2 * xb + 2 * pb);
+    if (p->fp16) take(2 * xh + 2 * ph);
   }
   void* mem = nullptr;
   if (cudaMalloc(&mem, std::max(off, (size_t)kAlign)) != cudaSuccess) {
@@ -2151,6 +2318,7 @@ int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int
   p->d_maps = reinterpret_cast<BatchMaps*>(base + m_off);
   p->d_order = reinterpret_cast<int*>(base + o_off);
   p->d_queue = reinterpret_cast<int*>(base + q_off);
+  p->d_fp16_bad = reinterpret_cast<int*>(base + f_off);
   for (int g = 0; g < count; g++) {
     BatchGraph& G = p->host[g];
     const size_t xb = (size_t)G.Mp * G.Kp * 4, pb = (size_t)(G.Kp / 2) * 2 * G.Np * 4;
@@ -2159,6 +2327,17 @@ int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int
     G.X[1] = reinterpret_cast<float*>(b + xb);
     G.P[0] = reinterpret_cast<float*>(b + 2 * xb);
     G.P[1] = reinterpret_cast<float*>(b + 2 * xb + pb);
+    G.Xh[0] = G.Xh[1] = nullptr;
+    G.Ph[0] = G.Ph[1] = nullptr;
+    if (p->fp16) {
+      size_t xh, ph;
+      half_bytes(G, &xh, &ph);
+      uint8_t* h = b + align_up(2 * xb + 2 * pb, kAlign);
+      G.Xh[0] = reinterpret_cast<__half*>(h);
+      G.Xh[1] = reinterpret_cast<__half*>(h + xh);
+      G.Ph[0] = reinterpret_cast<uint32_t*>(h + 2 * xh);
+      G.Ph[1] = reinterpret_cast<uint32_t*>(h + 2 * xh + ph);
+    }
     G.iters = 0;
     G.changed = 0;
   }
@@ -2171,6 +2350,12 @@ int simd2_batched_plan_create(simd2_op op, int count, float* const* X, const int
       if (rc == SIMD2_OK)
         rc = make_map_f32(&hmaps[g].b[b], G.P[b], G.Kp / 2, 2LL * G.Np, 2LL * G.Np, 2 * kBN, kBK / 2,
                           CU_TENSOR_MAP_SWIZZLE_NONE, false);
+      if (p->fp16 && rc == SIMD2_OK)
+        rc = make_map_2d(&hmaps[g].ah[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, G.Xh[b], G.Mp, G.Kh, G.Kh, kH2BK, kBM,
+                         CU_TENSOR_MAP_SWIZZLE_128B);
+      if (p->fp16 && rc == SIMD2_OK)
+        rc = make_map_2d(&hmaps[g].bh[b], CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, G.Ph[b], G.Kh / 2, G.Np, G.Np, kBN,
+                         kH2BK / 2, CU_TENSOR_MAP_SWIZZLE_NONE);
     }
   }
   if (rc == SIMD2_OK && count > 0 &&

@@ -32,6 +32,10 @@ struct BatchGraph {
   int Np;       // columns padded to a multiple of 128 (interleaved layout)
   float* X[2];  // [Mp][Kp], ping-pong
   float* P[2];  // [Kp/2][2*Np] interleaved, ping-pong
+  // FP16 copies for the selection semirings (max_min, min_max), else null:
+  int Kh;           // columns (= k extent) padded to a multiple of 64
+  __half* Xh[2];    // [Mp][Kh], ping-pong
+  uint32_t* Ph[2];  // [Kh/2][Np] k-pair words (X[2p][j], X[2p+1][j]), ping-pong
   float* user;  // caller's matrix (result is copied back here)
   long long ldu;
   int iters;    // out: steps run (including the final unchanged one)
@@ -77,6 +81,8 @@ __device__ __forceinline__ void fence_proxy_async_global() {
 struct BatchMaps {
   CUtensorMap a[2];
   CUtensorMap b[2];
+  CUtensorMap ah[2];  // Xh[0], Xh[1]: 128 rows x 64 halves, 128-byte swizzle (FP16 path)
+  CUtensorMap bh[2];  // Ph[0], Ph[1]: 32 pair rows x 128 words (FP16 path)
 };
 
 // One k-tile of the 8 x 4 register tile; ROWS < 8 skips rows ty + 16i for
@@ -113,8 +119,10 @@ __device__ __forceinline__ void batched_mac_ktile(float (&acc)[8][4], const floa
 template <int OP>
 __global__ void __launch_bounds__(kSimtThreads, 1)
     closure_batched_kernel(BatchGraph* graphs, const BatchMaps* __restrict__ maps, const int* order, int count,
-                           int* queue, int max_iter, int conv_mode) {
+                           int* queue, int max_iter, int conv_mode, const int* fp16_bad) {
   constexpr int STAGES = kSimtStages;
+  // with the FP16 path enqueued too, this kernel runs only when some entry is not an FP16 value
+  if (fp16_bad && *fp16_bad == 0) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
@@ -268,8 +276,10 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
 
 // Prep: copy every graph into X[0] (normal) and P[0] (interleaved), NaN padding;
 // X[1], P[1] get the same padding (their valid region is written by step 1).
-// One CTA row per (graph, padded row); grid-stride over graphs.
-__global__ void batched_prep_kernel(BatchGraph* graphs, int count) {
+// One CTA row per (graph, padded row); grid-stride over graphs.  With the
+// FP16 path enqueued too, it runs only when some entry is not an FP16 value.
+__global__ void batched_prep_kernel(BatchGraph* graphs, int count, const int* fp16_bad) {
+  if (fp16_bad && *fp16_bad == 0) return;
   const float nanv = __int_as_float(0x7fc00000);
   for (int g = blockIdx.y; g < count; g += gridDim.y) {
     BatchGraph& G = graphs[g];
@@ -295,17 +305,278 @@ __global__ void batched_prep_kernel(BatchGraph* graphs, int count) {
   }
 }
 
-// Copy every result X[iters & 1] back into the caller's matrix.
-__global__ void batched_finish_kernel(BatchGraph* graphs, int count) {
+// Copy every result X[iters & 1] (or its FP16 twin, when the FP16 path ran)
+// back into the caller's matrix.
+__global__ void batched_finish_kernel(BatchGraph* graphs, int count, const int* fp16_bad) {
+  const bool h = fp16_bad && *fp16_bad == 0;
   for (int g = blockIdx.y; g < count; g += gridDim.y) {
     BatchGraph& G = graphs[g];
-    const float* R = G.X[G.iters & 1];
-    const int n = G.n, Kp = G.Kp;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
-         t += (long long)gridDim.x * blockDim.x) {
-      const int i = (int)(t / n), j = (int)(t - (long long)i * n);
-      G.user[(long long)i * G.ldu + j] = R[(long long)i * Kp + j];
+    const int n = G.n;
+    if (h) {
+      const __half* R = G.Xh[G.iters & 1];
+      const int Kh = G.Kh;
+      for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+           t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / n), j = (int)(t - (long long)i * n);
+        G.user[(long long)i * G.ldu + j] = __half2float(R[(long long)i * Kh + j]);
+      }
+    } else {
+      const float* R = G.X[G.iters & 1];
+      const int Kp = G.Kp;
+      for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+           t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / n), j = (int)(t - (long long)i * n);
+        G.user[(long long)i * G.ldu + j] = R[(long long)i * Kp + j];
+      }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP16 path of the selection semirings (max_min, min_max).  Their closure only
+// ever selects among the input entries (and the identities), so when every
+// entry of every graph is exactly an FP16 value, every X_t is too, and the
+// packed min/max.f16x2 micro-kernel of srgemm_h2_kernel (two k per lane per
+// instruction: 2 ALU instructions per 2 (x),(+) pairs instead of 3) gives the
+// FP32 closure's bits.  batched_prep_h_kernel writes the FP16 copies and sets
+// *fp16_bad when an entry is not an FP16 value; the FP16 and FP32 closure
+// kernels are both enqueued, each gated by that flag, so the plan's run stays
+// asynchronous.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ __half batched_half_exact(float x, bool& bad) {
+  const __half h = __float2half_rn(x);
+  bad |= __float_as_uint(__half2float(h)) != __float_as_uint(x);
+  return h;
+}
+
+// Xh[0] = X as halves [Mp][Kh], Ph[0] = k-pair words [Kh/2][Np], NaN padding;
+// Xh[1], Ph[1] = NaN (their valid region is written by step 1).
+__global__ void batched_prep_h_kernel(BatchGraph* graphs, int count, int* fp16_bad) {
+  const __half nanh = __ushort_as_half(0x7e00);
+  const uint32_t nanw = 0x7e007e00u;
+  bool bad = false;
+  for (int g = blockIdx.y; g < count; g += gridDim.y) {
+    BatchGraph& G = graphs[g];
+    const int n = G.n, Kh = G.Kh, Np = G.Np, Mp = G.Mp;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)Mp * Kh;
+         t += (long long)gridDim.x * blockDim.x) {
+      const int i = (int)(t / Kh), k = (int)(t - (long long)i * Kh);
+      G.Xh[0][t] = (i < n && k < n) ? batched_half_exact(G.user[(long long)i * G.ldu + k], bad) : nanh;
+      G.Xh[1][t] = nanh;
+    }
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)(Kh / 2) * Np;
+         t += (long long)gridDim.x * blockDim.x) {
+      const int p = (int)(t / Np), j = (int)(t - (long long)p * Np);
+      const int k0 = 2 * p, k1 = 2 * p + 1;
+      const __half lo = (k0 < n && j < n) ? batched_half_exact(G.user[(long long)k0 * G.ldu + j], bad) : nanh;
+      const __half hi = (k1 < n && j < n) ? batched_half_exact(G.user[(long long)k1 * G.ldu + j], bad) : nanh;
+      G.Ph[0][t] = (uint32_t)__half_as_ushort(lo) | ((uint32_t)__half_as_ushort(hi) << 16);
+      G.Ph[1][t] = nanw;
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(fp16_bad, 1);
+}
+
+__device__ __forceinline__ uint32_t bh_min2(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("min.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t bh_max2(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("max.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+
+// One 64-k tile of the FP16 8 x 4 register tile (rows ty + 16i, i < ROWS):
+// A chunk q (k pairs 4q..4q+3 of a row, 16 bytes) sits at chunk q ^ (row & 7)
+// of the 128-byte row; B pair row pr holds 128 words.
+template <int OP, int ROWS>
+__device__ __forceinline__ void batched_h2_ktile(uint32_t (&acc)[8][4], const uint8_t* As, const uint32_t* Bs, int ty,
+                                                 int tx, int cbase, int swz) {
+#pragma unroll 2
+  for (int q = 0; q < 8; q++) {
+    uint4 a[ROWS];
+#pragma unroll
+    for (int i = 0; i < ROWS; i++) a[i] = *reinterpret_cast<const uint4*>(As + (ty + 16 * i) * 128 + ((q ^ swz) << 4));
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const int pr = 4 * q + h;
+      uint2 b[2];
+#pragma unroll
+      for (int c = 0; c < 2; c++) b[c] = *reinterpret_cast<const uint2*>(Bs + pr * kBN + cbase + 32 * c + 2 * tx);
+#pragma unroll
+      for (int i = 0; i < ROWS; i++) {
+        const uint32_t ap = h == 0 ? a[i].x : h == 1 ? a[i].y : h == 2 ? a[i].z : a[i].w;
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          if constexpr (OP == SIMD2_MAX_MIN) {
+            acc[i][2 * c] = bh_max2(acc[i][2 * c], bh_min2(ap, b[c].x));
+            acc[i][2 * c + 1] = bh_max2(acc[i][2 * c + 1], bh_min2(ap, b[c].y));
+          } else {
+            acc[i][2 * c] = bh_min2(acc[i][2 * c], bh_max2(ap, b[c].x));
+            acc[i][2 * c + 1] = bh_min2(acc[i][2 * c + 1], bh_max2(ap, b[c].y));
+          }
+        }
+      }
+    }
+  }
+}
+
+// The persistent batched closure on the FP16 copies: the scheduling, TMA
+// staging, padding skips, change test and proxy fence of
+// closure_batched_kernel, with 64-k tiles of halves and k-pair words.
+template <int OP>
+__global__ void __launch_bounds__(kSimtThreads, 1)
+    closure_batched_h2_kernel(BatchGraph* graphs, const BatchMaps* __restrict__ maps, const int* order, int count,
+                              int* queue, int max_iter, int conv_mode, const int* fp16_bad) {
+  static_assert(OP == SIMD2_MAX_MIN || OP == SIMD2_MIN_MAX, "selection semirings only");
+  constexpr int STAGES = kSimtStages;
+  if (*fp16_bad != 0) return;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
+  uint64_t* empty = full + STAGES;
+  __shared__ int s_graph;
+  __shared__ int s_changed;
+  __shared__ int s_failed;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int tx = lane & 15;
+  const int ty = (warp & 7) * 2 + (lane >> 4);
+  const int cbase = (warp >> 3) * 64;
+  const int swz = ty & 7;
+  const uint32_t ident = OP == SIMD2_MAX_MIN ? 0xfc00fc00u : 0x7c007c00u;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kSimtWarps);
+    }
+    fence_mbar_init();
+    s_failed = 0;
+  }
+  __syncthreads();
+  uint32_t gk = 0;  // running k-tile counter across tiles, steps and graphs
+
+  while (true) {
+    if (threadIdx.x == 0) {
+      const int q = atomicAdd(queue, 1);
+      s_graph = (q < count && !s_failed) ? order[q] : -1;
+    }
+    __syncthreads();
+    const int gi = s_graph;
+    if (gi < 0) break;
+    BatchGraph& G = graphs[gi];
+    const BatchMaps* mp = maps + gi;
+    const int n = G.n, Kh = G.Kh, Np = G.Np;
+    const int tiles_m = G.Mp / kBM, tiles_n = Np / kBN, ktiles = Kh / kH2BK;
+    int it = 0, changed_any = 1;
+    while (changed_any && it < max_iter) {
+      const int cur = it & 1, nxt = cur ^ 1;
+      const __half* X = G.Xh[cur];
+      __half* Xn = G.Xh[nxt];
+      __half* Pn = reinterpret_cast<__half*>(G.Ph[nxt]);
+      const CUtensorMap* tmA = &mp->ah[cur];
+      const CUtensorMap* tmB = &mp->bh[cur];
+      if (threadIdx.x == 0) s_changed = 0;
+      __syncthreads();
+      int changed = 0;
+      const int ntiles = tiles_m * tiles_n;
+      const int nloads = ntiles * ktiles;
+      auto issue = [&](int j) {
+        const uint32_t g = gk + j;
+        const int s = g % STAGES;
+        if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1)) {
+          report_timeout(25);
+          s_failed = 1;
+        }
+        const int tile = j / ktiles, kk = j - tile * ktiles;
+        uint8_t* sa = smem + s * kStageBytes;
+        mbar_arrive_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(sa, tmA, &full[s], kk * kH2BK, (tile % tiles_m) * kBM);
+        tma_load_2d(sa + kATileBytes, tmB, &full[s], (tile / tiles_m) * kBN, kk * (kH2BK / 2));
+      };
+      if (threadIdx.x == 0)
+        for (int j = 0; j < min(STAGES, nloads); j++) issue(j);
+      for (int t = 0; t < ntiles; t++) {
+        const int m0 = (t % tiles_m) * kBM;
+        const int n0 = (t / tiles_m) * kBN;
+        const int row_groups = min(8, (n - m0 + 15) / 16);
+        const bool idle_cols = n0 + 64 >= n && cbase == 64;
+        uint32_t acc[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[i][j] = ident;
+        for (int i = 0; i < ktiles; i++) {
+          const int j = t * ktiles + i;
+          const uint32_t g = gk + j;
+          const int s = g % STAGES;
+          if (threadIdx.x == 0 && j >= 1 && j - 1 + STAGES < nloads) issue(j - 1 + STAGES);
+          if (!mbar_wait(&full[s], (g / STAGES) & 1)) {
+            report_timeout(26);
+            s_failed = 1;
+          }
+          const uint8_t* As = smem + s * kStageBytes;
+          const uint32_t* Bs = reinterpret_cast<const uint32_t*>(As + kATileBytes);
+          if (!idle_cols) {
+            switch (row_groups) {
+              case 1: batched_h2_ktile<OP, 1>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 2: batched_h2_ktile<OP, 2>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 3: batched_h2_ktile<OP, 3>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 4: batched_h2_ktile<OP, 4>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 5: batched_h2_ktile<OP, 5>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 6: batched_h2_ktile<OP, 6>(acc, As, Bs, ty, tx, cbase, swz); break;
+              case 7: batched_h2_ktile<OP, 7>(acc, As, Bs, ty, tx, cbase, swz); break;
+              default: batched_h2_ktile<OP, 8>(acc, As, Bs, ty, tx, cbase, swz); break;
+            }
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&empty[s]);
+        }
+        // epilogue: X_{t+1} = X_t (+) acc in both FP16 layouts (exact: every
+        // value is an input entry or an identity), change test against X_t
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int row = m0 + ty + 16 * i;
+          if (row < n) {
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+              const int col0 = n0 + cbase + 32 * c + 2 * tx;
+#pragma unroll
+              for (int e = 0; e < 2; e++) {
+                const int col = col0 + e;
+                if (col < n) {
+                  const uint32_t w = acc[i][2 * c + e];
+                  const float lo = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+                  const float hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+                  const float old_v = __half2float(__ldcg(X + (long long)row * Kh + col));
+                  const float v = Semiring<OP>::add(Semiring<OP>::add(lo, hi), old_v);
+                  if (conv_changed(conv_mode, old_v, v)) changed = 1;
+                  const __half vh = __float2half_rn(v);
+                  Xn[(long long)row * Kh + col] = vh;
+                  Pn[(long long)(row >> 1) * (2LL * Np) + 2 * col + (row & 1)] = vh;
+                }
+              }
+            }
+          }
+        }
+      }
+      gk += nloads;
+      if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(&s_changed, 1);
+      // X_{t+1} was written through the generic proxy; the next step reads it with TMA.
+      fence_proxy_async_global();
+      __syncthreads();
+      changed_any = s_changed && !s_failed;
+      it++;
+    }
+    if (threadIdx.x == 0) {
+      G.iters = it;
+      G.changed = changed_any || s_failed;
+    }
+    __syncthreads();
   }
 }
 

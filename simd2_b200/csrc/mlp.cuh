@@ -1,10 +1,11 @@
-// mlp.cuh -- the cost model of the learned dispatch: a 12-32-32-1 ReLU MLP
-// that predicts log2(time in ms) of one closure step for a kernel
+// mlp.cuh -- the cost model of the learned dispatch: a 15-32-32-1 ReLU MLP
+// that predicts log2(time in ms) of one closure step for a step
 // configuration, with hand-written training and inference kernels.
 //
-// Input (kMlpIn = 12): seven step features computed on the device from the
-// block occupancy statistics (see mlp_features) followed by the configuration
-// encoding: one-hot split factor {1,2,4,8} and the skip flag.
+// Input (kMlpIn = 15): nine step features computed on the device from the
+// block occupancy and the entry counts of X_t (see mlp_features) followed by
+// the configuration encoding: one-hot split factor {1,2,4,8}, the skip flag
+// and the sparse flag (a CSR SpGEMM step, configuration kSparseConfig).
 // Parameters are one flat float array:
 //   W1[H][In] | b1[H] | W2[H][H] | b2[H] | W3[H] | b3
 #pragma once
@@ -12,8 +13,8 @@
 
 namespace simd2 {
 
-constexpr int kMlpIn = 12;
-constexpr int kMlpFeat = 7;
+constexpr int kMlpIn = 15;
+constexpr int kMlpFeat = 9;
 constexpr int kMlpH = 32;
 constexpr int kMlpW1 = 0;
 constexpr int kMlpB1 = kMlpW1 + kMlpH * kMlpIn;
@@ -21,8 +22,9 @@ constexpr int kMlpW2 = kMlpB1 + kMlpH;
 constexpr int kMlpB2 = kMlpW2 + kMlpH * kMlpH;
 constexpr int kMlpW3 = kMlpB2 + kMlpH;
 constexpr int kMlpB3 = kMlpW3 + kMlpH;
-constexpr int kMlpParams = kMlpB3 + 1;  // 1505
-constexpr int kNumConfigs = 8;          // split {1,2,4,8} x skip {0,1}
+constexpr int kMlpParams = kMlpB3 + 1;  // 1601
+constexpr int kNumConfigs = 8;          // dense: split {1,2,4,8} x skip {0,1}
+constexpr int kSparseConfig = 8;        // a CSR SpGEMM step
 constexpr int kLearnedMinN = 1024;      // the learned policy runs the plain path up to this n,
 constexpr int kLearnedLoopMinN = 2048;  // then a sparse opening, and per-step MLP choices above this n
 
@@ -30,8 +32,10 @@ __host__ __device__ inline int config_split(int c) { return 1 << (c & 3); }
 __host__ __device__ inline int config_skip(int c) { return c >> 2; }
 
 __device__ __forceinline__ void mlp_encode_config(int c, float* x /* kMlpIn */) {
-  for (int j = 0; j < 4; j++) x[kMlpFeat + j] = (c & 3) == j ? 1.f : 0.f;
-  x[kMlpFeat + 4] = (float)config_skip(c);
+  const bool sparse = c == kSparseConfig;
+  for (int j = 0; j < 4; j++) x[kMlpFeat + j] = !sparse && (c & 3) == j ? 1.f : 0.f;
+  x[kMlpFeat + 4] = sparse ? 0.f : (float)config_skip(c);
+  x[kMlpFeat + 5] = sparse ? 1.f : 0.f;
 }
 
 // Forward pass of one sample; z1, z2 receive the pre-activations when non-null.
@@ -118,42 +122,58 @@ __global__ void adam_kernel(float* __restrict__ P, const float* __restrict__ gra
   }
 }
 
-// The seven step features from the occupancy statistics
-// stats = {surviving (tm,tn,kt) triples, occupied A blocks, occupied B blocks}.
+// The nine step features from the statistics of X_t:
+// stats = {surviving (tm,tn,kt) triples, occupied A panels, occupied B
+// panels, stored entries, Gustavson products sum_k rowcnt(k) colcnt(k)}.
 __host__ __device__ inline void mlp_features(int n, int tiles_m, int tiles_n, int ktiles,
-                                             unsigned long long triples, unsigned long long occa,
-                                             unsigned long long occb, int sms, float* f) {
+                                             const unsigned long long* st, int sms, float* f) {
   const double tiles = (double)tiles_m * tiles_n;
-  f[0] = (float)(log2((double)n) / 16.0);
-  f[1] = (float)((double)triples / (tiles * ktiles));
-  f[2] = (float)((double)occa / ((double)tiles_m * ktiles));
-  f[3] = (float)((double)occb / ((double)ktiles * tiles_n));
+  const double ln = log2((double)n);
+  f[0] = (float)(ln / 16.0);
+  f[1] = (float)((double)st[0] / (tiles * ktiles));
+  f[2] = (float)((double)st[1] / ((double)tiles_m * ktiles));
+  f[3] = (float)((double)st[2] / ((double)ktiles * tiles_n));
   f[4] = (float)(log2(tiles) / 16.0);
   f[5] = (float)fmin(tiles / sms, 16.0) / 16.f;
-  f[6] = (float)(log2((double)triples + 1.0) / 32.0);
+  f[6] = (float)(log2((double)st[0] + 1.0) / 32.0);
+  f[7] = (float)((double)st[3] / ((double)n * n));
+  f[8] = (float)(log2((double)st[4] + 1.0) / (3.0 * ln));
 }
 
-// Picks the configuration with the smallest predicted time for one step.
-// out[0] = chosen config, out[1..8] = predictions (as float bits).
+// Picks the configuration with the smallest predicted time for one step:
+// the dense ones allowed by allow_skip / max_split, and the sparse step when
+// allow_sparse.  Thread c evaluates configuration c; out[0] = chosen config
+// (the lowest id among equal predictions), out[1 + c] = prediction for
+// config c (as float bits), c = 0..kSparseConfig.  Launch with 32 threads.
 __global__ void mlp_choose_kernel(const float* __restrict__ P, const unsigned long long* __restrict__ stats, int n,
                                   int tiles_m, int tiles_n, int ktiles, int sms, int allow_skip, int max_split,
-                                  int* __restrict__ out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  float x[kMlpIn];
-  mlp_features(n, tiles_m, tiles_n, ktiles, stats[0], stats[1], stats[2], sms, x);
-  int best = 0;
-  float best_t = 3.0e38f;
-  for (int c = 0; c < kNumConfigs; c++) {
+                                  int allow_sparse, int* __restrict__ out) {
+  const int c = threadIdx.x;
+  float t = 3.0e38f;
+  if (blockIdx.x == 0 && c <= kSparseConfig) {
+    unsigned long long st[5];
+    for (int i = 0; i < 5; i++) st[i] = stats[i];
+    float x[kMlpIn];
+    mlp_features(n, tiles_m, tiles_n, ktiles, st, sms, x);
     mlp_encode_config(c, x);
-    const float t = mlp_forward_one(P, x, nullptr, nullptr);
-    out[1 + c] = __float_as_int(t);
-    const bool allowed = (allow_skip || !config_skip(c)) && config_split(c) <= max_split;
-    if (allowed && t < best_t) {
-      best_t = t;
-      best = c;
+    const float p = mlp_forward_one(P, x, nullptr, nullptr);
+    out[1 + c] = __float_as_int(p);
+    const bool allowed = c == kSparseConfig ? allow_sparse != 0
+                                            : (allow_skip || !config_skip(c)) && config_split(c) <= max_split;
+    if (allowed) t = p;
+  }
+  // argmin over the lanes, lower config id on ties
+  int best = c;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float t2 = __shfl_xor_sync(0xffffffffu, t, o);
+    const int b2 = __shfl_xor_sync(0xffffffffu, best, o);
+    if (t2 < t || (t2 == t && b2 < best)) {
+      t = t2;
+      best = b2;
     }
   }
-  out[0] = best;
+  if (blockIdx.x == 0 && c == 0) out[0] = t < 3.0e38f ? best : 0;
 }
 
 }  // namespace simd2

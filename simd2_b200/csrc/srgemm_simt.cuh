@@ -533,23 +533,130 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
   }
 }
 
-// Block occupancy for the skip lists: occ32[bi][bj] = 1 when the 32 x 32
-// block (rows 32 bi.., cols 32 bj..) of X holds an entry that is neither NaN
-// nor `annihilator` (the value whose (x)-product is the (+)-identity).
-__global__ void occupancy32_kernel(const float* __restrict__ X, long long ldx, int rows, int cols, float annihilator,
-                                   uint8_t* __restrict__ occ32, int bcols) {
-  const int bi = blockIdx.y, bj = blockIdx.x;
-  const int r = bi * 32 + threadIdx.y, c0 = bj * 32;
-  bool f = false;
-  for (int rr = r; rr < min(bi * 32 + 32, rows); rr += blockDim.y) {
-    const int c = c0 + threadIdx.x;
-    if (c < cols) {
-      const float v = X[(long long)rr * ldx + c];
-      f |= (v == v) && (v != annihilator);
+// Block occupancy of X (rows x cols) in wide strips, optionally with entry
+// counts.  A CTA of 256 threads covers 128 rows x 512 columns: warp w reads
+// rows w, w + 8, ..., w + 120 and, per 128-column segment, each lane four
+// consecutive columns (one 16-byte load when X's rows allow it), so every
+// thread keeps 64 loads in flight.  occ32[bi][bj] = 1 when the 32 x 32 block
+// holds an entry that is neither NaN nor `annihilator`.  With COUNTS,
+// rowcnt[r] and colcnt[c] receive the entries that differ bitwise from the add
+// identity `ident` (the entries a CSR copy of X stores): one atomic add per row
+// and 512 columns, and per column and 128 rows (both zeroed before).
+constexpr int kOccRows = 128;
+constexpr int kOccCols = 512;
+
+template <bool COUNTS>
+__global__ void __launch_bounds__(256) occupancy_strip_kernel(const float* __restrict__ X, long long ldx, int rows,
+                                                             int cols, float annihilator, float ident,
+                                                             uint8_t* __restrict__ occ32, int bcols,
+                                                             int* __restrict__ rowcnt, int* __restrict__ colcnt) {
+  __shared__ int s_occ[kOccRows / 32][kOccCols / 32];
+  __shared__ int s_col[COUNTS ? kOccCols : 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = blockIdx.y * kOccRows, c0 = blockIdx.x * kOccCols;
+  for (int i = threadIdx.x; i < (kOccRows / 32) * (kOccCols / 32); i += 256) (&s_occ[0][0])[i] = 0;
+  if (COUNTS)
+    for (int i = threadIdx.x; i < kOccCols; i += 256) s_col[i] = 0;
+  __syncthreads();
+  const bool vec = (ldx % 4 == 0) && (reinterpret_cast<uintptr_t>(X) % 16 == 0);
+  const uint32_t id = __float_as_uint(ident);
+  uint32_t flags = 0;  // bit rb * 4 + seg: an occupied entry in row block rb, segment seg
+  int ccount[16];      // per segment seg, column e: entries of column c0 + 128 seg + 4 lane + e
+#pragma unroll
+  for (int i = 0; i < 16; i++) ccount[i] = 0;
+  for (int rr = warp; rr < kOccRows; rr += 8) {
+    const int r = r0 + rr;
+    if (r >= rows) break;
+    const float* xr = X + (long long)r * ldx;
+    int rcount = 0;
+#pragma unroll
+    for (int seg = 0; seg < 4; seg++) {
+      const int c = c0 + seg * 128 + lane * 4;
+      float v[4];
+      bool in[4];
+      if (vec && c + 3 < cols) {
+        const float4 u = __ldg(reinterpret_cast<const float4*>(xr + c));
+        v[0] = u.x, v[1] = u.y, v[2] = u.z, v[3] = u.w;
+#pragma unroll
+        for (int e = 0; e < 4; e++) in[e] = true;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          in[e] = c + e < cols;
+          v[e] = in[e] ? __ldg(xr + c + e) : annihilator;
+        }
+      }
+      bool f = false;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        f |= in[e] && (v[e] == v[e]) && (v[e] != annihilator);
+        if (COUNTS) {
+          const int st = in[e] && __float_as_uint(v[e]) != id;
+          rcount += st;
+          ccount[seg * 4 + e] += st;
+        }
+      }
+      if (f) flags |= 1u << ((rr >> 5) * 4 + seg);
+    }
+    if (COUNTS) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) rcount += __shfl_xor_sync(0xffffffffu, rcount, o);
+      if (lane == 0 && rcount) atomicAdd(&rowcnt[r], rcount);
     }
   }
-  const int any = __syncthreads_or(f);
-  if (threadIdx.x == 0 && threadIdx.y == 0) occ32[(long long)bi * bcols + bj] = (uint8_t)any;
+  // a lane's four columns of segment seg lie in column block 4 seg + lane / 8
+  for (uint32_t m = flags; m; m &= m - 1) {
+    const int b = __ffs(m) - 1;
+    atomicOr(&s_occ[b >> 2][(b & 3) * 4 + (lane >> 3)], 1);
+  }
+  if (COUNTS) {
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+      if (ccount[i]) atomicAdd(&s_col[(i >> 2) * 128 + lane * 4 + (i & 3)], ccount[i]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < (kOccRows / 32) * (kOccCols / 32); i += 256) {
+    const int bi = blockIdx.y * (kOccRows / 32) + i / (kOccCols / 32);
+    const int bj = blockIdx.x * (kOccCols / 32) + i % (kOccCols / 32);
+    if (bi * 32 < rows && bj * 32 < cols) occ32[(long long)bi * bcols + bj] = (uint8_t)(&s_occ[0][0])[i];
+  }
+  if (COUNTS)
+    for (int i = threadIdx.x; i < kOccCols; i += 256)
+      if (s_col[i] && c0 + i < cols) atomicAdd(&colcnt[c0 + i], s_col[i]);
+}
+
+// occ32[r / 32][c / 32] = 1 for every stored entry (r, c) of a CSR matrix
+// (occ32 zeroed before); one warp per row.
+__global__ void csr_occupancy32_kernel(int n, const int* __restrict__ rp, const int* __restrict__ cj,
+                                       uint8_t* __restrict__ occ32, int bcols) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
+    uint8_t* row = occ32 + (long long)(r >> 5) * bcols;
+    for (int e = rp[r] + lane; e < rp[r + 1]; e += 32) {
+      const int c = cj[e];
+      if ((unsigned)c < (unsigned)n) row[c >> 5] = 1;
+    }
+  }
+}
+
+// stats[3] = sum_r rowcnt[r] (stored entries), stats[4] = sum_k rowcnt[k] *
+// colcnt[k] (the products a Gustavson X (x) X forms); both zeroed before.
+__global__ void count_products_kernel(int n, const int* __restrict__ rowcnt, const int* __restrict__ colcnt,
+                                      unsigned long long* __restrict__ stats) {
+  unsigned long long s = 0, p = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    s += (unsigned long long)rowcnt[k];
+    p += (unsigned long long)rowcnt[k] * (unsigned long long)colcnt[k];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    p += __shfl_xor_sync(0xffffffffu, p, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (s) atomicAdd(&stats[3], s);
+    if (p) atomicAdd(&stats[4], p);
+  }
 }
 
 // occA[tm][kt] = OR of occ32 over rows 4tm..4tm+3 at column block kt;

@@ -126,3 +126,44 @@ def rmat_graph(n: int, avg_degree: float, seed: int, a: float = 0.57, b: float =
     x[src[order], dst[order]] = w[order]
     np.fill_diagonal(x, 0.0)
     return x
+
+
+def rmat_graph_device(n: int, avg_degree: float, seed: int, device, a: float = 0.57, b: float = 0.19,
+                      c: float = 0.19, wmin: int = 1, wmax: int = 100):
+    """The R-MAT graph of ``rmat_graph`` drawn on the GPU with torch's seeded
+    generator (another random stream, so other graphs than the numpy
+    version's): n * avg_degree edge draws, integer weights, duplicate draws
+    keep the smallest weight, +inf non-edges, 0 diagonal.  Returns an n x n
+    float32 CUDA tensor; n must be a power of two."""
+    import torch
+    levels = int(np.log2(n))
+    assert 1 << levels == n
+    m = int(n * avg_degree)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    src = torch.zeros(m, dtype=torch.int64, device=device)
+    dst = torch.zeros(m, dtype=torch.int64, device=device)
+    for _ in range(levels):
+        u = torch.rand(m, generator=g, device=device)
+        right = ((u >= a) & (u < a + b)) | (u >= a + b + c)
+        down = u >= a + b
+        src = src * 2 + down
+        dst = dst * 2 + right
+        del u, right, down
+    w = torch.randint(wmin, wmax + 1, (m,), generator=g, device=device).float()
+    x = torch.full((n * n,), float("inf"), dtype=torch.float32, device=device)
+    x.scatter_reduce_(0, src * n + dst, w, reduce="amin")
+    del src, dst, w
+    x = x.view(n, n)
+    x.fill_diagonal_(0.0)
+    return x
+
+
+def rmat_mixed_set(count: int = 64, seed: int = 5):
+    """The mixed-density R-MAT workload: (n, average degree, seed) for
+    ``count`` graphs, n cycling through 4096, 8192, 16384 and the degree
+    log-uniform in [4, 4096]."""
+    rng = np.random.default_rng(seed)
+    degs = np.exp(rng.uniform(np.log(4.0), np.log(4096.0), size=count))
+    seeds = rng.integers(0, 2**31 - 1, size=count)
+    return [((4096, 8192, 16384)[i % 3], float(round(float(d), 2)), int(s)) for i, (d, s) in enumerate(zip(degs, seeds))]

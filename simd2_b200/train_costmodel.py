@@ -3,11 +3,14 @@
     python -m simd2_b200.train_costmodel [--out PATH] [--steps N]
 
 Profiles min_plus closures of a fixed set of seeded R-MAT and Erdos-Renyi
-graphs (n 512..4096, average degree 2..512) under all eight kernel
-configurations (autotune.profile_closure), trains the MLP on the GPU with
-libsimd2's own kernels, and stores the weights plus a summary of the
-training data next to this file.  The dispatcher (simd2_closure_ex with
-dispatch="learned") takes these weights.
+graphs (n 2048..16384, average degree 2..2048) under all eight dense kernel
+configurations and the sparse (CSR SpGEMM) configuration
+(autotune.profile_closure), trains the MLP on the GPU with libsimd2's own
+kernels, and stores the weights plus a summary of the training data next to
+this file.  The dispatcher (simd2_closure_ex with dispatch="learned") takes
+these weights; the summary's best fixed dense configuration is the one the
+hand-written rules policy (dispatch="rules") runs.  The graphs are drawn
+with other seeds than the mixed-density benchmark set.
 """
 from __future__ import annotations
 
@@ -23,14 +26,16 @@ from . import autotune, costmodel, datagen
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "costmodel_weights.json")
 
-TRAIN_SET = ([("rmat", n, d) for n in (512, 1024, 2048, 4096) for d in (2, 4, 16, 64, 512)]
-             + [("er", n, p) for n in (1024, 4096) for p in (0.001, 0.01)])
+TRAIN_SET = ([("rmat", n, d) for n in (2048, 4096) for d in (2, 4, 16, 64, 512)]
+             + [("rmat", 8192, d) for d in (3, 8, 24, 96, 1024)]
+             + [("rmat", 16384, d) for d in (4, 20, 300)]
+             + [("er", 4096, 0.001), ("er", 8192, 0.0005)])
 
 
-def make_graph(kind, n, param, seed):
+def make_graph(kind, n, param, seed, dev):
     if kind == "rmat":
-        return datagen.rmat_graph(n, float(param), seed=seed)
-    return datagen.er_graph(n, float(param), seed=seed)
+        return datagen.rmat_graph_device(n, float(param), seed=seed, device=dev)
+    return torch.from_numpy(datagen.er_graph(n, float(param), seed=seed)).to(dev)
 
 
 def main():
@@ -43,15 +48,17 @@ def main():
     t0 = time.time()
     recs = []
     for i, (kind, n, param) in enumerate(TRAIN_SET):
-        g = torch.from_numpy(make_graph(kind, n, param, seed=1000 + i)).to(dev)
+        g = make_graph(kind, n, param, seed=1000 + i, dev=dev)
         recs.append(autotune.profile_closure("min_plus", g))
+        del g
     if args.records:
         autotune.save(recs, args.records)
     X, y = autotune.dataset(recs)
     params, losses = costmodel.train(X.to(dev), y.to(dev), steps=args.steps, lr=3e-3)
     costmodel.save(params, args.out)
     summary = {"graphs": len(recs), "rows": int(X.shape[0]), "loss_first": losses[0], "loss_last": losses[-1],
-               "best_fixed": autotune.describe(recs), "seconds": round(time.time() - t0, 1)}
+               "best_fixed": autotune.describe(recs), "best_fixed_config": int(autotune.best_fixed(recs)[0]),
+               "seconds": round(time.time() - t0, 1)}
     with open(args.out) as f:
         d = json.load(f)
     d["training"] = summary

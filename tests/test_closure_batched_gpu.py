@@ -93,3 +93,47 @@ def test_batched_not_converged_and_empty(cuda):
     with pytest.raises(s2.NotConverged):
         s2.closure_batched("min_plus", [m], max_iter=2)
     assert s2.closure_batched("min_plus", []) == []
+
+
+@pytest.mark.parametrize("op", ["max_min", "min_max"])
+@pytest.mark.parametrize("case", ["fp16", "one-off", "overflow", "tol"])
+def test_batched_selection_fp16_and_fp32_paths(cuda, op, case):
+    """max_min / min_max close every graph on FP16 copies when every entry of
+    every graph is an FP16 value (integer weights), else on FP32: one entry
+    that is not (1.0001, or 70000 past the FP16 range) sends the whole batch
+    to FP32.  Same bits and step counts as the oracle either way, under the
+    bitwise and the |delta| > 1e-4 change tests; also replayed from a
+    captured CUDA graph."""
+    rng = np.random.default_rng(17)
+    sizes = [5, 64, 65, 127, 128, 129, 191, 200, 256, 300, 33, 1]
+    graphs = [datagen.closure_graph(op if op == "max_min" else "min_plus", int(n), float(rng.uniform(0.02, 0.3)),
+                                    seed=40 + i) for i, n in enumerate(sizes)]
+    if case == "one-off":
+        graphs[3][5, 7] = np.float32(1.0001)
+    elif case == "overflow":
+        graphs[7][2, 3] = np.float32(70000.0)
+    conv = "tol" if case == "tol" else "exact"
+    mats = [torch.from_numpy(g.copy()).to(cuda) for g in graphs]
+    plan = s2.BatchedClosure(op, mats, conv=conv)
+    s = torch.cuda.Stream()
+    plan.run(stream=s)
+    s.synchronize()
+    for rep in range(2):
+        if rep == 1:  # the second run replays a captured CUDA graph on restored inputs
+            cg = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(cg, stream=s):
+                plan.run(stream=s)
+            for m, g in zip(mats, graphs):
+                m.copy_(torch.from_numpy(g))
+            cg.replay()
+            torch.cuda.synchronize()
+        its, nc = plan.iters()
+        assert nc == 0
+        for g, m, it in zip(graphs, mats, its):
+            want, it_want = oracle.closure(op, g, tol_mode=1 if conv == "tol" else 0)
+            assert it == it_want, (case, g.shape, it, it_want)
+            np.testing.assert_array_equal(bits(m.cpu().numpy()), bits(want), err_msg=f"{case} n={g.shape[0]}")
+        if rep == 1:
+            del cg
+    plan.close()
+    assert s2.device_status() == 0

@@ -6,9 +6,9 @@ from oracle import mlp
 
 def test_oracle_gradient_matches_finite_differences():
     rng = np.random.default_rng(0)
-    P = 32 * 12 + 32 + 32 * 32 + 32 + 32 + 1
+    P = 32 * mlp.N_IN + 32 + 32 * 32 + 32 + 32 + 1
     p = rng.standard_normal(P) * 0.3
-    X = rng.standard_normal((9, 12))
+    X = rng.standard_normal((9, mlp.N_IN))
     y = rng.standard_normal(9)
 
     def loss(q):
