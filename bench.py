@@ -430,6 +430,56 @@ def learned_dispatch_mixed(dev, params, weights_path, count=64):
                    "drawn on the GPU (datagen.rmat_mixed_set / rmat_graph_device), weights 1..100"}
 
 
+def or_and_step(dev, n=16384, reps=3):
+    """One or_and srgemm D = X (x) X (+) X at N = 16384 on a 0/1 byte matrix of
+    density 0.5 (a squaring step after the closure has filled in): kernel time
+    from the library's CUDA events; and, as the roofline's denominator, the
+    INT8 tensor rate torch._int_mm (cuBLAS) reaches at 8192^3 on this GPU."""
+    import torch
+
+    import simd2_b200 as s2
+
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(16384)
+    X = (torch.rand((n, n), device=dev, generator=gen) < 0.5).to(torch.uint8)
+    D = torch.empty_like(X)
+    s2.srgemm("or_and", X, X, X, do_epilogue=True, D=D)
+    torch.cuda.synchronize()
+    with s2.KernelTimer() as kt:
+        for _ in range(reps):
+            s2.srgemm("or_and", X, X, X, do_epilogue=True, D=D)
+        torch.cuda.synchronize()
+    kms, launches, _ = kt.by_kind["tensor"]
+    kms /= max(launches, 1)
+    tops = 2.0 * n ** 3 / kms / 1e9
+    del X, D
+    peak = None
+    try:
+        m = 8192
+        a = torch.randint(-128, 127, (m, m), dtype=torch.int8, device=dev, generator=gen)
+        b = torch.randint(-128, 127, (m, m), dtype=torch.int8, device=dev, generator=gen)
+        torch._int_mm(a, b)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = None
+        for _ in range(5):
+            ev0.record()
+            torch._int_mm(a, b)
+            ev1.record()
+            torch.cuda.synchronize()
+            t = ev0.elapsed_time(ev1)
+            best = t if best is None else min(best, t)
+        peak = 2.0 * m ** 3 / best / 1e9
+        del a, b
+    except RuntimeError:
+        peak = None
+    peaks, _ = measured_peaks()
+    return {"kernel_ms": kms, "tops": tops, "int8_peak_tops_measured": peak,
+            "frac_of_measured_int8": tops / peak if peak else None,
+            "frac_of_2x_bf16": tops / (2.0 * float(peaks.get("bf16_tflops", 1590.0))),
+            "how": "tc_gemm2_kernel<1> (tcgen05 kind::i8 on SM pairs), 0/1 bytes of density 0.5 with C, kernel time "
+                   "from CUDA events; int8 peak: torch._int_mm 8192^3 best of 5 (cuBLAS, measurement only)"}
+
+
 def extra_measurements(args, dev):
     """The metric's other two parts, on one GPU: batched APSP graphs/s against
     per-graph launches, and the learned dispatch against the plain dense path
@@ -512,6 +562,9 @@ def extra_measurements(args, dev):
 
     # --- the headline size: min_plus srgemm at 8192^3 on the sweep's value distribution
     out["min_plus_8192"] = min_plus_8192(dev)
+    # --- or_and on the INT8 tensor cores: one dense squaring step at N=16384 against the
+    # measured INT8 GEMM rate of the library (cuBLAS through torch), the denominator
+    out["or_and_16384_step"] = or_and_step(dev)
 
     # --- dense-contraction workloads at full size (tensor cores)
     cfg4 = {}

@@ -2600,8 +2600,19 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   int dev = 0, sms = 148;
   SIMD2_CUDA_TRY(cudaGetDevice(&dev));
   SIMD2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int chunks = knn_fused_chunks(qblocks, tiles, sms, max_lists);
-  const int tpc = (tiles + chunks - 1) / chunks;
+  // A pilot chunk of a few tiles per query block when the units fill more
+  // than one wave (see knn_unit_tiles); the other chunks share the rest.
+  int pilot = 0;
+  int main_chunks = knn_fused_chunks(qblocks, tiles, sms, max_lists);
+  if (tiles >= 64 && max_lists >= 6) {
+    const int mc = knn_fused_chunks(qblocks, tiles - 4, sms, max_lists - 2);
+    if ((long long)qblocks * mc > sms) {
+      pilot = 4;
+      main_chunks = mc;
+    }
+  }
+  const int tpc = (tiles - pilot + main_chunks - 1) / main_chunks;
+  const int chunks = main_chunks + (pilot ? 1 : 0);
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes, kAlign); return o; };
   const size_t qhi = take((size_t)Q * Dp * 2), qlo = take((size_t)Q * Dp * 2);
@@ -2648,6 +2659,7 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   a.panels = (Dp + 63) / 64;
   a.chunks = chunks;
   a.tiles_per_chunk = tpc;
+  a.pilot_tiles = pilot;
   a.num_tiles = tiles;
   a.norm_q = n_q;
   a.norm_r = n_r;

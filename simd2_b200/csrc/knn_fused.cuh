@@ -59,8 +59,9 @@ constexpr size_t kKfSmemBytes =
 struct KnnFusedArgs {
   int Q, R, D;
   int panels;             // ceil(round_up(D, 8) / 64), 1 or 2
-  int chunks;             // reference chunks (units per 128 queries)
-  int tiles_per_chunk;    // reference tiles of 256 per chunk
+  int chunks;             // reference chunks (units per 128 queries), the pilot included
+  int tiles_per_chunk;    // reference tiles of 256 per chunk (after the pilot)
+  int pilot_tiles;        // > 0: chunk 0 is a short pilot of this many tiles (see knn_unit_tiles)
   int num_tiles;          // ceil(R / 256)
   const float* norm_q;    // [Q]
   const float* norm_r;    // [num_tiles * 256], +inf past R
@@ -100,20 +101,39 @@ __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Reference tiles [t0, t0 + ntiles) of a chunk.  With a pilot, chunk 0 is
+// the first pilot_tiles tiles: its units are the first of the grid and run
+// only a few tiles, so every later unit of the query block soon has a pruning
+// bound (the units of the first wave otherwise start with none, and the first
+// tiles of a list without a bound take most of the insertions).
+__device__ __forceinline__ void knn_unit_tiles(const KnnFusedArgs& a, int chunk, int* t0, int* ntiles) {
+  if (a.pilot_tiles > 0) {
+    *t0 = chunk == 0 ? 0 : a.pilot_tiles + (chunk - 1) * a.tiles_per_chunk;
+    *ntiles = min(a.num_tiles, chunk == 0 ? a.pilot_tiles : *t0 + a.tiles_per_chunk) - *t0;
+  } else {
+    *t0 = chunk * a.tiles_per_chunk;
+    *ntiles = min(a.num_tiles, *t0 + a.tiles_per_chunk) - *t0;
+  }
+}
+
 // Pruning bound from the finished units of earlier chunks of this query
-// block: each of their lists holds K pairs no larger than its last distance,
-// all at lower reference indices than this chunk's, so a candidate of this
-// chunk at or above that distance is outranked K times and cannot be
-// selected.  +inf when no earlier unit of the query block has finished.
+// block (the four before this one, and the pilot): each of their lists holds
+// K pairs no larger than its last distance, all at lower reference indices
+// than this chunk's, so a candidate of this chunk at or above that distance
+// is outranked K times and cannot be selected.  +inf when no earlier unit of
+// the query block has finished.
 template <int K>
 __device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblock, int chunk, int row) {
   float T = __int_as_float(0x7f800000);
-  for (int cc = chunk - 1; cc >= 0 && cc >= chunk - 4; cc--) {
+  auto take = [&](int cc) {
     if (ld_acquire_gpu(a.ready + (long long)qblock * a.chunks + cc)) {
       const long long base = ((long long)row * (2 * a.chunks) + 2 * cc) * K;
       T = fminf(T, fminf(__ldcg(a.part_d + base + K - 1), __ldcg(a.part_d + base + 2 * K - 1)));
     }
-  }
+  };
+  const int lo = max(0, chunk - 4);
+  for (int cc = chunk - 1; cc >= lo; cc--) take(cc);
+  if (a.pilot_tiles > 0 && lo > 0) take(0);
   return T;
 }
 
@@ -138,8 +158,8 @@ __global__ void __launch_bounds__(kKfThreads, 1)
   const int qblocks = (a.Q + kKfBM - 1) / kKfBM;
   const int chunk = blockIdx.x / qblocks;
   const int m0 = (blockIdx.x - chunk * qblocks) * kKfBM;
-  const int t0 = chunk * a.tiles_per_chunk;
-  const int ntiles = min(a.num_tiles, t0 + a.tiles_per_chunk) - t0;
+  int t0, ntiles;
+  knn_unit_tiles(a, chunk, &t0, &ntiles);
   const int P = a.panels;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -262,7 +282,10 @@ __global__ void __launch_bounds__(kKfThreads, 1)
     float prior = __int_as_float(0x7f800000);  // bound from earlier chunks' lists
     for (int t = 0; t < ntiles; t++) {
       const int acc = t & 1;
-      if (row_ok && (t & 7) == 0) prior = fminf(prior, knn_prior_bound<K>(a, qblock, chunk, row));
+      // the bound is refreshed every tile while the unit is young (a pilot
+      // unit may finish meanwhile), then every 8 tiles
+      if (row_ok && chunk > 0 && (t < 8 || (t & 7) == 0))
+        prior = fminf(prior, knn_prior_bound<K>(a, qblock, chunk, row));
       if (ok && !mbar_wait(&acc_full[acc], (t >> 1) & 1)) {
         report_timeout(115);
         ok = false;
@@ -297,18 +320,25 @@ __global__ void __launch_bounds__(kKfThreads, 1)
           // Hot pass: the distance of each of the 32 columns and a bit per
           // column that may enter the list.  The insertion code exists once per
           // half, below, so the loop body stays small for the instruction cache.
+          // Packed FP32 pairs: each lane of __fadd2_rn / __ffma2_rn rounds
+          // like the scalar na + |r|^2 and fma(-2, q.r, .), so v keeps the
+          // materialised epilogue's bits.
           const float4* nb4 = reinterpret_cast<const float4*>(a.norm_r + cbase + c * 32);
+          const float2 na2 = make_float2(na, na), m2 = make_float2(-2.0f, -2.0f);
           uint32_t mask = 0;
 #pragma unroll
           for (int q4 = 0; q4 < 8; q4++) {
             const float4 nb = __ldg(nb4 + q4);
-            const float nbv[4] = {nb.x, nb.y, nb.z, nb.w};
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
+            for (int e = 0; e < 4; e += 2) {
               const int jj = q4 * 4 + e;
-              const float v = __fmaf_rn(-2.0f, __uint_as_float(r[jj]), na + nbv[e]);
-              r[jj] = __float_as_uint(v);
-              mask |= (v < lim ? 1u : 0u) << jj;
+              const float2 s2 = __fadd2_rn(na2, e == 0 ? make_float2(nb.x, nb.y) : make_float2(nb.z, nb.w));
+              const float2 v2 =
+                  __ffma2_rn(m2, make_float2(__uint_as_float(r[jj]), __uint_as_float(r[jj + 1])), s2);
+              r[jj] = __float_as_uint(v2.x);
+              r[jj + 1] = __float_as_uint(v2.y);
+              mask |= (v2.x < lim ? 1u : 0u) << jj;
+              mask |= (v2.y < lim ? 1u : 0u) << (jj + 1);
             }
           }
           // Rare pass, in increasing column order.

@@ -187,17 +187,51 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
     // the clamps keep every access inside the arrays whatever they hold.
     const int e1 = min(a.ap[r + 1], a.a_nnz);
     if constexpr (kWarpK) {
-      // one warp per A entry (k), its lanes over B's row k; no order between k
-      for (int e = max(a.ap[r], 0) + warp; e < e1; e += kSpThreads / 32) {
-        const int k = a.aj[e];
-        if ((unsigned)k >= (unsigned)a.K) continue;  // uniform across the warp
-        const float av = COUNT ? 0.f : a.av[e];
-        const int f1 = min(a.bp[k + 1], a.b_nnz);
-        for (int f = max(a.bp[k], 0) + lane; f < f1; f += 32) {
-          const int j = a.bj[f];
-          if ((unsigned)j >= (unsigned)a.N) continue;
+      // One warp per A entry (k), its lanes over B's row k; no order between k.
+      // The loads form a chain (A's column k, then B's row offsets, then B's
+      // columns and values), so the next entry's k and offsets are fetched
+      // before the current B row is walked, and the walk keeps four loads of
+      // B's columns (and values) in flight per lane.
+      constexpr int kStride = kSpThreads / 32;
+      int e = max(a.ap[r], 0) + warp;
+      int kn = -1, f0n = 0, f1n = 0;
+      float avn = 0.f;
+      auto fetch = [&](int ee) {
+        kn = -1;
+        if (ee < e1) {
+          const int k = a.aj[ee];
+          if ((unsigned)k < (unsigned)a.K) {  // uniform across the warp
+            kn = k;
+            f0n = max(a.bp[k], 0);
+            f1n = min(a.bp[k + 1], a.b_nnz);
+            if constexpr (!COUNT) avn = a.av[ee];
+          }
+        }
+      };
+      fetch(e);
+      for (; e < e1; e += kStride) {
+        const int k = kn, f0 = f0n, f1 = f1n;
+        const float av = avn;
+        fetch(e + kStride);
+        if (k < 0) continue;
+        auto put = [&](int j, float bvv) {
+          if ((unsigned)j >= (unsigned)a.N) return;
           atomicOr(&bitmap[j >> 5], 1u << (j & 31));
-          if constexpr (!COUNT) KY::fold(acck + j, O::mul(av, a.bv[f]));
+          if constexpr (!COUNT) KY::fold(acck + j, O::mul(av, bvv));
+        };
+        // four predicated loads per lane per round trip, so a row under 128
+        // entries costs one round trip too
+        for (int f = f0 + lane; f < f1; f += 128) {
+          int j[4];
+          float bvv[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int ff = f + 32 * u;
+            j[u] = ff < f1 ? a.bj[ff] : -1;
+            bvv[u] = (COUNT || ff >= f1) ? 0.f : a.bv[ff];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++) put(j[u], bvv[u]);
         }
       }
     } else {

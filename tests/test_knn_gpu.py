@@ -67,12 +67,14 @@ def test_knn_ties_keep_lower_index(cuda):
 
 @pytest.mark.parametrize("shape", [(300, 1000, 128, 16), (129, 257, 37, 5), (64, 4096, 128, 32), (1, 3, 8, 3),
                                    (1000, 5000, 64, 8), (257, 70001, 100, 16), (130, 512, 128, 4),
-                                   (4096, 65536, 128, 16)])
+                                   (4096, 65536, 128, 16), (8192, 65536, 128, 16), (9000, 40000, 96, 8)])
 def test_knn_fused_matches_materialised(cuda, shape):
     """The fused kernel (selection in the MMA epilogue) and the materialised
-    path (distance blocks, then selection) return identical bits.  The last
-    shape runs the fused grid in two waves, so second-wave units prune with
-    the lists of finished earlier chunks."""
+    path (distance blocks, then selection) return identical bits.  From
+    4096 x 65536 on, units prune with the lists of finished earlier chunks;
+    the last two shapes fill more than one wave, so the fused grid opens with
+    a pilot chunk of four reference tiles per query block (whose lists bound
+    every later unit), the second with a ragged last tile and D = 96."""
     Q, R, D, k = shape
     q, r = datagen.point_cloud(Q, R, D, seed=Q * 7 + R, dup_frac=0.05)
     Qt, Rt = torch.from_numpy(q).to(cuda), torch.from_numpy(r).to(cuda)
