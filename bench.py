@@ -57,6 +57,9 @@ def parse_args():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the batched-closure / learned-dispatch / APSP-512 measurements")
     p.add_argument("--batched-count", type=int, default=4096)
+    p.add_argument("--batched-n", type=int, default=0,
+                   help="with --workload batched: every graph of this size (ER, p = 0.1) instead of the mixed set "
+                        "(one size class)")
     p.add_argument("--knn-q", type=int, default=16384)
     p.add_argument("--knn-r", type=int, default=65536)
     p.add_argument("--workload", choices=("sweep", "batched", "knn", "rowpanel"), default="sweep",
@@ -224,7 +227,10 @@ def batched_sharded(args, dev, rank, world, op="min_plus", reps=3):
     from simd2_b200 import datagen
     from simd2_b200.shard import assign_graphs, max_over_ranks
 
-    graphs = datagen.batched_graphs(args.batched_count, 32, 1024, seed=3, op=op)
+    if getattr(args, "batched_n", 0):
+        graphs = [datagen.closure_graph(op, args.batched_n, 0.1, seed=i) for i in range(args.batched_count)]
+    else:
+        graphs = datagen.batched_graphs(args.batched_count, 32, 1024, seed=3, op=op)
     mine = assign_graphs([g.shape[0] for g in graphs], world)[rank]
     mats = [torch.from_numpy(graphs[g]).to(dev) for g in mine]
     origs = [m.clone() for m in mats]
@@ -750,7 +756,9 @@ def main():
     if args.workload == "batched":
         res = {op: batched_sharded(args, dev, rank, world, op=op)[0] for op in ("min_plus", "max_min")}
         if rank == 0:
-            print(json.dumps({"workload": "batched closure", **res}), flush=True)
+            what = (f"batched closure, {args.batched_count} ER graphs of n={args.batched_n}, p=0.1" if args.batched_n
+                    else "batched closure")
+            print(json.dumps({"workload": what, **res}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return 0

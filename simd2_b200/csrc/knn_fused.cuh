@@ -116,24 +116,49 @@ __device__ __forceinline__ void knn_unit_tiles(const KnnFusedArgs& a, int chunk,
   }
 }
 
+__device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
 // Pruning bound from the finished units of earlier chunks of this query
 // block (the four before this one, and the pilot): each of their lists holds
 // K pairs no larger than its last distance, all at lower reference indices
 // than this chunk's, so a candidate of this chunk at or above that distance
-// is outranked K times and cannot be selected.  +inf when no earlier unit of
-// the query block has finished.
+// is outranked K times and cannot be selected.
+//
+// The ready flags of those (at most five) chunks are read with relaxed loads,
+// all in flight together, and only a chunk seen ready for the first time
+// (bit c of *seen: chunk - 1 - c, bit 4: the pilot) costs a fence -- which,
+// after the flag read, orders the list loads after the writer's release --
+// and the loads of its two K-th distances.  Returns the updated bound.
 template <int K>
-__device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblock, int chunk, int row) {
-  float T = __int_as_float(0x7f800000);
-  auto take = [&](int cc) {
-    if (ld_acquire_gpu(a.ready + (long long)qblock * a.chunks + cc)) {
-      const long long base = ((long long)row * (2 * a.chunks) + 2 * cc) * K;
-      T = fminf(T, fminf(__ldcg(a.part_d + base + K - 1), __ldcg(a.part_d + base + 2 * K - 1)));
-    }
-  };
+__device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblock, int chunk, int row, float T,
+                                                 unsigned* seen) {
+  const unsigned* flags = a.ready + (long long)qblock * a.chunks;
   const int lo = max(0, chunk - 4);
-  for (int cc = chunk - 1; cc >= lo; cc--) take(cc);
-  if (a.pilot_tiles > 0 && lo > 0) take(0);
+  const bool pilot = a.pilot_tiles > 0 && lo > 0;
+  unsigned f[5];
+#pragma unroll
+  for (int c = 0; c < 4; c++) f[c] = chunk - 1 - c >= lo ? ld_relaxed_gpu(flags + chunk - 1 - c) : 0u;
+  f[4] = pilot ? ld_relaxed_gpu(flags) : 0u;
+  unsigned fresh = 0;
+#pragma unroll
+  for (int c = 0; c < 5; c++) fresh |= (f[c] != 0u ? 1u : 0u) << c;
+  fresh &= ~*seen;
+  if (fresh) {
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    *seen |= fresh;
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      if (fresh & (1u << c)) {
+        const int cc = c < 4 ? chunk - 1 - c : 0;
+        const long long base = ((long long)row * (2 * a.chunks) + 2 * cc) * K;
+        T = fminf(T, fminf(__ldcg(a.part_d + base + K - 1), __ldcg(a.part_d + base + 2 * K - 1)));
+      }
+    }
+  }
   return T;
 }
 
@@ -280,12 +305,12 @@ __global__ void __launch_bounds__(kKfThreads, 1)
     bool ok = true;
     const int qblock = m0 / kKfBM;
     float prior = __int_as_float(0x7f800000);  // bound from earlier chunks' lists
+    unsigned seen = 0;                          // earlier chunks already folded into it
     for (int t = 0; t < ntiles; t++) {
       const int acc = t & 1;
       // the bound is refreshed every tile while the unit is young (a pilot
       // unit may finish meanwhile), then every 8 tiles
-      if (row_ok && chunk > 0 && (t < 8 || (t & 7) == 0))
-        prior = fminf(prior, knn_prior_bound<K>(a, qblock, chunk, row));
+      if (row_ok && chunk > 0 && (t < 8 || (t & 7) == 0)) prior = knn_prior_bound<K>(a, qblock, chunk, row, prior, &seen);
       if (ok && !mbar_wait(&acc_full[acc], (t >> 1) & 1)) {
         report_timeout(115);
         ok = false;
@@ -347,8 +372,9 @@ __global__ void __launch_bounds__(kKfThreads, 1)
             mask &= mask - 1;
             const int col = cbase + c * 32 + j;
             float v = __uint_as_float(pick32(r, j));
-            const float nsum = na + a.norm_r[col];
-            if (v < a.band * nsum) v = exact_minus_square(qrow, a.r32, a.ldr, col, a.D, 1);
+            // blim >= band * (|q|^2 + |r|^2) for every column of the tile, so
+            // only v < blim can be in the cancellation band
+            if (v < blim && v < a.band * (na + a.norm_r[col])) v = exact_minus_square(qrow, a.r32, a.ldr, col, a.D, 1);
             if (v < thr) {
               topk_insert<K>(bd, bi, v, col);
               thr = fminf(bd[K - 1], prior);
