@@ -235,7 +235,22 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
         }
-        // epilogue: X_{t+1} = X_t (+) acc in both layouts, change test against X_t
+        // epilogue: X_{t+1} = X_t (+) acc in both layouts, change test against
+        // X_t.  The thread's 32 old values are loaded first, as 8-byte pairs
+        // (col is even and Kp a multiple of 32, so a pair starting below n
+        // lies inside the padded row) all in flight together, then combined.
+        float2 oldv[8][WN];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int row = m0 + ty + 16 * i;
+#pragma unroll
+          for (int c = 0; c < WN; c++) {
+            const int col = n0 + cbase + 32 * c + 2 * tx;
+            oldv[i][c] = (row < n && col < n)
+                             ? __ldcg(reinterpret_cast<const float2*>(X + (long long)row * Kp + col))
+                             : make_float2(0.f, 0.f);
+          }
+        }
 #pragma unroll
         for (int i = 0; i < 8; i++) {
           const int row = m0 + ty + 16 * i;
@@ -246,7 +261,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
 #pragma unroll
               for (int e = 0; e < 2; e++) {
                 if (col + e < n) {
-                  const float old_v = __ldcg(X + (long long)row * Kp + col + e);
+                  const float old_v = e == 0 ? oldv[i][c].x : oldv[i][c].y;
                   float v = Mac<OP>::add(acc[i][2 * c + e], old_v);
                   if (conv_mode == SIMD2_CONV_APLP && v > -1.0f && v < 1.0f) v = -3.402823466e+38f;
                   if (conv_changed(conv_mode, old_v, v)) changed = 1;
@@ -537,7 +552,21 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
           if (lane == 0) mbar_arrive(&empty[s]);
         }
         // epilogue: X_{t+1} = X_t (+) acc in both FP16 layouts (exact: every
-        // value is an input entry or an identity), change test against X_t
+        // value is an input entry or an identity), change test against X_t.
+        // The 32 old values are loaded first, as 4-byte half pairs (col even,
+        // Kh a multiple of 64), all in flight together.
+        uint32_t oldw[8][2];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int row = m0 + ty + 16 * i;
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            const int col0 = n0 + cbase + 32 * c + 2 * tx;
+            oldw[i][c] = (row < n && col0 < n)
+                             ? __ldcg(reinterpret_cast<const unsigned int*>(X + (long long)row * Kh + col0))
+                             : 0u;
+          }
+        }
 #pragma unroll
         for (int i = 0; i < 8; i++) {
           const int row = m0 + ty + 16 * i;
@@ -552,7 +581,8 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
                   const uint32_t w = acc[i][2 * c + e];
                   const float lo = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
                   const float hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
-                  const float old_v = __half2float(__ldcg(X + (long long)row * Kh + col));
+                  const float old_v =
+                      __half2float(__ushort_as_half((unsigned short)(e == 0 ? oldw[i][c] & 0xffffu : oldw[i][c] >> 16)));
                   const float v = Semiring<OP>::add(Semiring<OP>::add(lo, hi), old_v);
                   if (conv_changed(conv_mode, old_v, v)) changed = 1;
                   const __half vh = __float2half_rn(v);

@@ -350,7 +350,12 @@ __global__ void __launch_bounds__(kKfThreads, 1)
           // materialised epilogue's bits.
           const float4* nb4 = reinterpret_cast<const float4*>(a.norm_r + cbase + c * 32);
           const float2 na2 = make_float2(na, na), m2 = make_float2(-2.0f, -2.0f);
-          uint32_t mask = 0;
+          // The mask bits are formed as 1.0 / 0.0 and summed with packed FMAs
+          // into four accumulators of 16 bit positions each (exact: every sum
+          // stays below 2^16), which leaves one compare per column on the ALU
+          // pipe (the selection warps keep that pipe busy) and moves the rest
+          // to the FMA pipe.
+          float2 mlo = make_float2(0.f, 0.f), mhi = make_float2(0.f, 0.f);
 #pragma unroll
           for (int q4 = 0; q4 < 8; q4++) {
             const float4 nb = __ldg(nb4 + q4);
@@ -362,10 +367,14 @@ __global__ void __launch_bounds__(kKfThreads, 1)
                   __ffma2_rn(m2, make_float2(__uint_as_float(r[jj]), __uint_as_float(r[jj + 1])), s2);
               r[jj] = __float_as_uint(v2.x);
               r[jj + 1] = __float_as_uint(v2.y);
-              mask |= (v2.x < lim ? 1u : 0u) << jj;
-              mask |= (v2.y < lim ? 1u : 0u) << (jj + 1);
+              const float2 b2 = make_float2(v2.x < lim ? 1.f : 0.f, v2.y < lim ? 1.f : 0.f);
+              const int pos = jj & 15;
+              const float2 w2 = make_float2((float)(1u << pos), (float)(2u << pos));
+              if (jj < 16) mlo = __ffma2_rn(b2, w2, mlo);
+              else mhi = __ffma2_rn(b2, w2, mhi);
             }
           }
+          uint32_t mask = (uint32_t)(mlo.x + mlo.y) | ((uint32_t)(mhi.x + mhi.y) << 16);
           // Rare pass, in increasing column order.
           while (mask) {
             const int j = __ffs(mask) - 1;

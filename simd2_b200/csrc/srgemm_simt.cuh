@@ -299,6 +299,20 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
 
   if constexpr (SPLIT == 1) {
     const int vec2 = ep.vec2;
+    // The thread's C pairs are loaded first, all in flight together (each
+    // load-then-use pair in turn would wait out the memory latency 16 times).
+    float2 cpre[8][WN];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int row = m0 + ty + 16 * i;
+#pragma unroll
+      for (int c = 0; c < WN; c++) {
+        const int col = n0 + cbase + 32 * c + 2 * tx;
+        cpre[i][c] = (do_epi && vec2 && row < M && col + 1 < N)
+                         ? *reinterpret_cast<const float2*>(Cbase + (long long)row * ldc + col)
+                         : make_float2(0.f, 0.f);
+      }
+    }
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int row = m0 + ty + 16 * i;
@@ -309,8 +323,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
         for (int c = 0; c < WN; c++) {
           const int col = n0 + cbase + 32 * c + 2 * tx;
           if (vec2 && col + 1 < N) {
-            float2 cv = make_float2(0.f, 0.f);
-            if (do_epi) cv = *reinterpret_cast<const float2*>(crow + col);
+            const float2 cv = cpre[i][c];
             float2 v;
             v.x = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c], cv.x, changed);
             v.y = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + 1], cv.y, changed);
