@@ -479,11 +479,15 @@ def or_and_step(dev, n=16384, reps=3):
     except RuntimeError:
         peak = None
     peaks, _ = measured_peaks()
-    return {"kernel_ms": kms, "tops": tops, "int8_peak_tops_measured": peak,
-            "frac_of_measured_int8": tops / peak if peak else None,
-            "frac_of_2x_bf16": tops / (2.0 * float(peaks.get("bf16_tflops", 1590.0))),
+    # The library INT8 GEMM and twice the measured BF16 rate both stay below what this kernel
+    # reaches, so neither bounds it; the peak stated is the nominal dense INT8 rate (twice the
+    # nominal dense BF16 2.25 PFLOP/s), with the measured rates beside it.
+    nominal = 4500.0
+    return {"kernel_ms": kms, "tops": tops, "peak_tops": nominal, "frac": tops / nominal,
+            "peak_source": "nominal dense INT8 (4.5 POPS per B200); no measured reference reaches it",
+            "int8_library_tops_measured": peak, "twice_measured_bf16_tops": 2.0 * float(peaks.get("bf16_tflops", 1590.0)),
             "how": "tc_gemm2_kernel<1> (tcgen05 kind::i8 on SM pairs), 0/1 bytes of density 0.5 with C, kernel time "
-                   "from CUDA events; int8 peak: torch._int_mm 8192^3 best of 5 (cuBLAS, measurement only)"}
+                   "from CUDA events; library INT8: torch._int_mm 8192^3 best of 5 (cuBLAS, measurement only)"}
 
 
 def extra_measurements(args, dev):
