@@ -1543,7 +1543,9 @@ SpPlan sp_plan(int M, int N, size_t base) {
   // the FILL pass keeps the row's accumulators in shared memory up to 16384 columns
   p.smem_acc = N <= kSpSmemAccMaxN;
   p.smem_fill = bitmap + (p.smem_acc ? (size_t)N * 4 : 0);
-  int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / std::max<size_t>(p.smem_fill, 1)));
+  // CTAs per SM: by the FILL pass's shared memory and by the SM's 2048 threads
+  int per_sm = (int)std::max<size_t>(
+      1, std::min<size_t>(std::min<size_t>(8, 2048 / kSpThreads), (200u << 10) / std::max<size_t>(p.smem_fill, 1)));
   long long g = std::min<long long>((long long)M, 148LL * per_sm);
   // the accumulator slices stay below 1 GiB
   g = std::min<long long>(g, std::max<long long>(1, (1LL << 30) / (4LL * std::max(N, 1))));

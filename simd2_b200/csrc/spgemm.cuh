@@ -32,7 +32,7 @@
 
 namespace simd2 {
 
-constexpr int kSpThreads = 128;
+constexpr int kSpThreads = 512;
 
 template <int OP>
 struct SpOps;
