@@ -126,7 +126,9 @@ __device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
 // block (the four before this one, and the pilot): each of their lists holds
 // K pairs no larger than its last distance, all at lower reference indices
 // than this chunk's, so a candidate of this chunk at or above that distance
-// is outranked K times and cannot be selected.
+// is outranked K times and cannot be selected.  The bound taken from a chunk
+// is the K-th smallest distance of its two lists together (K pairs at lower
+// indices), tighter than the smaller of the two lists' K-th.
 //
 // The ready flags of those (at most five) chunks are read with relaxed loads,
 // all in flight together, and only a chunk seen ready for the first time
@@ -153,9 +155,21 @@ __device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblo
 #pragma unroll
     for (int c = 0; c < 5; c++) {
       if (fresh & (1u << c)) {
+        // the K-th smallest distance of the chunk's two sorted lists together:
+        // min over i of max(A[i-1], B[K-1-i]) (A[-1] = B[-1] = -inf)
         const int cc = c < 4 ? chunk - 1 - c : 0;
-        const long long base = ((long long)row * (2 * a.chunks) + 2 * cc) * K;
-        T = fminf(T, fminf(__ldcg(a.part_d + base + K - 1), __ldcg(a.part_d + base + 2 * K - 1)));
+        const float4* pa = reinterpret_cast<const float4*>(a.part_d + ((long long)row * (2 * a.chunks) + 2 * cc) * K);
+        float la[K], lb[K];
+#pragma unroll
+        for (int u = 0; u < K / 4; u++) {
+          const float4 x = __ldcg(pa + u), y = __ldcg(pa + K / 4 + u);
+          la[4 * u] = x.x, la[4 * u + 1] = x.y, la[4 * u + 2] = x.z, la[4 * u + 3] = x.w;
+          lb[4 * u] = y.x, lb[4 * u + 1] = y.y, lb[4 * u + 2] = y.z, lb[4 * u + 3] = y.w;
+        }
+        float kth = fminf(lb[K - 1], la[K - 1]);
+#pragma unroll
+        for (int i = 1; i < K; i++) kth = fminf(kth, fmaxf(la[i - 1], lb[K - 1 - i]));
+        T = fminf(T, kth);
       }
     }
   }
