@@ -505,6 +505,9 @@ def extra_measurements(args, dev):
     res = {}
     weights = os.path.join(ROOT, "simd2_b200", "costmodel_weights.json")
     params = costmodel.load(weights, dev) if os.path.exists(weights) else None
+    if params is not None:
+        # the plain dense path's split-K by size, as the autotuner measured it
+        s2.set_dense_configs(costmodel.load_dense_table(weights))
     for mode in ("dense", "learned") if params is not None else ("dense",):
         X = x.clone()
         r = s2.closure_ex("min_plus", X, dispatch=mode, mlp_params=params, record=True)  # configs, warm-up

@@ -198,6 +198,15 @@ int simd2_closure_ex(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_
                      int* iters_out, int* step_configs, float* step_ms, float* step_features,
                      cudaStream_t stream);
 
+/* The plain dense path's split-K factor by size, as the autotuner measured it
+ * (no reference counterpart).  Entry i (n_min ascending, config 0..3: split
+ * 1 << config, no skip) applies to closures of n_min[i] <= n < n_min[i + 1];
+ * below n_min[0] the dense path keeps its rule (the largest split with
+ * tiles * split <= SMs, at most 4).  count = 0 clears the table.  Applies to
+ * simd2_closure and to SIMD2_DISPATCH_DENSE of simd2_closure_ex in this
+ * process; same bits whatever the split. */
+int simd2_set_dense_configs(const int* n_min, const int* config, int count);
+
 /* Cost-model MLP (15-32-32-1, ReLU) kernels.  X: [batch][15] features+config,
  * y: [batch] targets (log2 ms).  simd2_mlp_gradient writes d/dparams of
  * mean((f(X)-y)^2) to grad (param_count floats) using sample_grads

@@ -85,6 +85,7 @@ def lib() -> ctypes.CDLL:
         L.simd2_batched_plan_destroy.argtypes = [P]
         L.simd2_closure_batched.argtypes = [I, I, ctypes.POINTER(P), PI, PI, I, I, PI, P]
         L.simd2_srgemm_f16.argtypes = [I, I, I, I, P, I, P, I, P, I, P, I, I, P]
+        L.simd2_set_dense_configs.argtypes = [ctypes.POINTER(I), ctypes.POINTER(I), I]
         L.simd2_knn.argtypes = [P, I, I, P, I, I, I, I, P, P, I, P]
         L.simd2_knn.restype = I
         L.simd2_knn_ex.argtypes = [P, I, I, P, I, I, I, I, P, P, I, I, P]
@@ -107,7 +108,7 @@ def lib() -> ctypes.CDLL:
                      "simd2_batched_plan_create", "simd2_batched_plan_run", "simd2_batched_plan_iters",
                      "simd2_batched_plan_destroy", "simd2_closure_batched", "simd2_srgemm_tuned",
                      "simd2_closure_ex", "simd2_mlp_param_count", "simd2_mlp_forward", "simd2_mlp_gradient",
-                     "simd2_mlp_adam", "simd2_srgemm_f16"):
+                     "simd2_mlp_adam", "simd2_srgemm_f16", "simd2_set_dense_configs"):
             getattr(L, name).restype = I
         _lib = L
     return _lib
@@ -225,6 +226,17 @@ def srgemm_tuned(op: str, A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | No
                                   ldc, D.data_ptr(), _mat(D, "D"), int(do_epilogue), int(config), _stream(stream))
     _check(rc, f"srgemm_tuned({op}, {config})")
     return D
+
+
+def set_dense_configs(table) -> None:
+    """Install the plain dense path's split-K factor by size: ``table`` is a
+    list of (n_min, config) with n_min ascending and config 0..3 (split
+    1 << config), as ``autotune.dense_table`` measures it; [] restores the
+    rule.  Every split gives the same bits."""
+    table = sorted((int(n), int(c)) for n, c in table)
+    ns = (ctypes.c_int * max(len(table), 1))(*[n for n, _ in table])
+    cs = (ctypes.c_int * max(len(table), 1))(*[c for _, c in table])
+    _check(lib().simd2_set_dense_configs(ns, cs, len(table)), "set_dense_configs")
 
 
 def closure_ex(op: str, X: torch.Tensor, dispatch: str = "dense", config: int = 0, mlp_params=None,

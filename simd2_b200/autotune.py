@@ -82,6 +82,19 @@ def best_fixed(records):
     return min(tot, key=tot.get), tot
 
 
+def dense_table(records):
+    """The plain dense path's split-K factor by size: for every n profiled, the
+    configuration without block skipping (split 1/2/4/8) with the smallest
+    total time over that n's records, as [(n, config)] ascending in n
+    (``simd2_b200.set_dense_configs`` installs it)."""
+    tot = {}
+    for rec in records:
+        for cfg in range(4):
+            t = tot.setdefault(int(rec["n"]), {})
+            t[cfg] = t.get(cfg, 0.0) + sum(rec["ms"][cfg])
+    return [(n, min(t, key=t.get)) for n, t in sorted(tot.items())]
+
+
 def save(records, path):
     with open(path, "w") as f:
         json.dump(records, f)

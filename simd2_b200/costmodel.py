@@ -96,6 +96,12 @@ def save(params: torch.Tensor, path: str):
         json.dump({"hidden": HIDDEN, "inputs": N_IN, "params": params.cpu().tolist()}, f)
 
 
+def load_dense_table(path: str):
+    """The autotuner's dense split table stored with the weights ([] if none)."""
+    with open(path) as f:
+        return [tuple(x) for x in json.load(f).get("training", {}).get("dense_configs", [])]
+
+
 def load(path: str, device="cuda") -> torch.Tensor:
     """Weights saved by ``save``; raises unless they fit this network (the
     dispatcher reads simd2_mlp_param_count() floats from the array)."""

@@ -835,9 +835,23 @@ int srgemm_orand(int M, int N, int K, const T* A, long long lda, const T* B, lon
 // ---------------------------------------------------------------------------
 namespace {
 
-// Split-K factor of the dense path: the largest power of two (at most 4)
-// with tiles * split <= SM count, so small problems still fill the GPU.
+// Split-K factors the autotuner measured best for the dense closure step, by
+// size: entry i applies from n = g_dense_n[i] up to the next entry's n (set by
+// simd2_set_dense_configs; empty until then).
+std::mutex g_dense_mu;
+std::vector<int> g_dense_n, g_dense_split;
+
+// Split-K factor of the dense path: the autotuned table's entry for n when
+// one applies, else the largest power of two (at most 4) with
+// tiles * split <= SM count, so small problems still fill the GPU.
 int dense_split(int n, int sms) {
+  {
+    std::lock_guard<std::mutex> lk(g_dense_mu);
+    int pick = 0;
+    for (size_t i = 0; i < g_dense_n.size(); i++)
+      if (g_dense_n[i] <= n) pick = g_dense_split[i];
+    if (pick) return pick;
+  }
   const long long tiles = (long long)((n + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
   int s = 1;
   while (s < 4 && tiles * s * 2 <= sms) s *= 2;
@@ -2471,6 +2485,19 @@ int simd2_closure_ex(simd2_op op, int n, float* X, int ldx, int max_iter, simd2_
   if (conv < SIMD2_CONV_EXACT || conv > SIMD2_CONV_APLP) return SIMD2_ERR_INVALID_ARG;
   return closure_f32_ex(op, n, X, ldx, max_iter, conv, (int)dispatch, fixed_config, mlp_params, iters_out,
                         step_configs, step_ms, step_features, stream);
+}
+
+int simd2_set_dense_configs(const int* n_min, const int* config, int count) {
+  if (count < 0 || (count > 0 && (!n_min || !config))) return SIMD2_ERR_INVALID_ARG;
+  for (int i = 0; i < count; i++) {
+    if (n_min[i] < 1 || config[i] < 0 || config[i] > 3 || (i > 0 && n_min[i] <= n_min[i - 1]))
+      return SIMD2_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_dense_mu);
+  g_dense_n.assign(n_min, n_min + count);
+  g_dense_split.resize(count);
+  for (int i = 0; i < count; i++) g_dense_split[i] = config_split(config[i]);
+  return SIMD2_OK;
 }
 
 int simd2_mlp_param_count(void) { return kMlpParams; }

@@ -58,6 +58,7 @@ def main():
     costmodel.save(params, args.out)
     summary = {"graphs": len(recs), "rows": int(X.shape[0]), "loss_first": losses[0], "loss_last": losses[-1],
                "best_fixed": autotune.describe(recs), "best_fixed_config": int(autotune.best_fixed(recs)[0]),
+               "dense_configs": autotune.dense_table(recs),
                "seconds": round(time.time() - t0, 1)}
     with open(args.out) as f:
         d = json.load(f)

@@ -60,3 +60,19 @@ def test_shim_header_compiles(tmp_path):
            "-c", os.path.join(ROOT, "tests", "compat", "cuasr_app.cu"), "-o", str(out)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+
+
+def test_dense_configs_table_arguments(lib):
+    """simd2_set_dense_configs validates its table (ascending sizes, configs
+    0..3 without block skipping) without touching the GPU; an empty table
+    restores the rule."""
+    L = lib
+    L.simd2_set_dense_configs.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    L.simd2_set_dense_configs.restype = ctypes.c_int
+    arr = lambda *v: (ctypes.c_int * len(v))(*v)
+    assert L.simd2_set_dense_configs(arr(2048, 4096), arr(0, 1), 2) == 0
+    assert L.simd2_set_dense_configs(arr(4096, 2048), arr(0, 1), 2) == 1   # not ascending
+    assert L.simd2_set_dense_configs(arr(2048), arr(4), 1) == 1             # a skip config
+    assert L.simd2_set_dense_configs(arr(0), arr(1), 1) == 1                # size below 1
+    assert L.simd2_set_dense_configs(None, None, -1) == 1
+    assert L.simd2_set_dense_configs(None, None, 0) == 0

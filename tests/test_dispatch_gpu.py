@@ -251,3 +251,32 @@ def test_shipped_costmodel_on_held_out_graphs(cuda):
             assert torch.equal(out[a][1].view(torch.int32), out["dense"][1].view(torch.int32)), (a, n, d)
     assert tot["dense"] >= 1.1 * tot["learned"], tot
     assert tot["learned"] <= 1.05 * tot["rules"], tot
+
+
+def test_autotuned_dense_configs(cuda):
+    """The plain dense path takes the split-K factor the autotuner installed
+    for the closure's size (recorded per step), with the same bits as the
+    rule's split; the shipped table is read from the weights file."""
+    import os
+    path = os.path.join(os.path.dirname(s2.__file__), "costmodel_weights.json")
+    shipped = costmodel.load_dense_table(path)
+    assert shipped and all(0 <= c <= 3 for _, c in shipped)
+    x = datagen.rmat_graph(2048, 16.0, seed=61)
+    Xa = torch.from_numpy(x.copy()).to(cuda)
+    ra = s2.closure_ex("min_plus", Xa, dispatch="dense", record=True)
+    assert all(c == 0 for c in ra["configs"])  # the rule: 256 tiles >= 148 SMs, split 1
+    try:
+        s2.set_dense_configs([(1024, 1), (4096, 2)])
+        Xb = torch.from_numpy(x.copy()).to(cuda)
+        rb = s2.closure_ex("min_plus", Xb, dispatch="dense", record=True)
+        assert all(c == 1 for c in rb["configs"])  # n = 2048 falls in the entry from 1024: split 2
+        assert rb["iters"] == ra["iters"]
+        assert torch.equal(Xa.view(torch.int32), Xb.view(torch.int32))
+        Xc = torch.from_numpy(x.copy()).to(cuda)
+        assert s2.closure("min_plus", Xc) == ra["iters"]
+        assert torch.equal(Xa.view(torch.int32), Xc.view(torch.int32))
+    finally:
+        s2.set_dense_configs([])
+    Xd = torch.from_numpy(x.copy()).to(cuda)
+    rd = s2.closure_ex("min_plus", Xd, dispatch="dense", record=True)
+    assert rd["configs"] == ra["configs"]

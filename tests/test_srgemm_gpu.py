@@ -256,3 +256,22 @@ def test_tensor_core_partial_rounds(cuda, op, shape):
             + np.abs(c[rows])
     assert np.all(np.abs(g - want) <= (4 * 2.0 ** -16 + 2 * K * 2.0 ** -24) * S + 1e-6)
     assert s2.device_status() == 0
+
+
+@pytest.mark.parametrize("op", SUMS)
+def test_summing_semirings_error_level(cuda, op):
+    """The BF16 hi/lo path's measured error against FP64, at the sweep's
+    values and K = 4096, stays at the level the split gives, far inside the
+    worst-case bound above: per product the dropped lo*lo term and the two
+    split residuals are each at most 2^-18 |a||b|, and FP32 accumulation over
+    K terms of random sign adds about sqrt(K) * 2^-24 (4x margin here).  A
+    split that lost its hi*lo or lo*hi term would miss this by orders of
+    magnitude."""
+    m, n, k = 384, 512, 4096
+    a, b, c = datagen.semiring_operands(op, m, n, k, seed=4096 + len(op))
+    got = run_gpu(op, a, b, c, True, cuda).astype(np.float64)
+    want = oracle.srgemm_f64(op, a, b, c, do_epilogue=True)
+    S = abs_sum(op, a, b, c, True)
+    level = 3 * 2.0 ** -18 + 4 * np.sqrt(k) * 2.0 ** -24
+    ratio = (np.abs(got - want) / S).max()
+    assert ratio <= level, (op, ratio, level)
