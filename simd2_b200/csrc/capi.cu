@@ -2573,34 +2573,70 @@ int knn_fused_chunks(int qblocks, int tiles, int sms, long long max_lists) {
   return best;
 }
 
-template <int KT>
-int knn_fused_launch(const CUtensorMap& mqh, const CUtensorMap& mql, const CUtensorMap& mrh, const CUtensorMap& mrl,
-                     const KnnFusedArgs& args, int qblocks, float* od, int32_t* oi, long long ldo, int kout,
-                     cudaStream_t stream) {
+// One fused pass: knn_fused_kernel<KL> over every (query block, chunk) unit,
+// then the per-query merge of its lists of KL into kout results (lane lists
+// of KT).  flags / gate: see knn_merge_kernel.
+template <int KL, int KT>
+int knn_fused_pass(const CUtensorMap& mqh, const CUtensorMap& mql, const CUtensorMap& mrh, const CUtensorMap& mrl,
+                   const KnnFusedArgs& args, int qblocks, float* od, int32_t* oi, long long ldo, int kout, int* flags,
+                   cudaStream_t stream) {
   static bool configured[64] = {};
   int dev = 0;
   SIMD2_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return SIMD2_ERR_NO_DEVICE;
   if (!configured[dev]) {
     SIMD2_CUDA_TRY(
-        cudaFuncSetAttribute(knn_fused_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kKfSmemBytes));
+        cudaFuncSetAttribute(knn_fused_kernel<KL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kKfSmemBytes));
     configured[dev] = true;
   }
-  auto* ev = prof_slot(2LL * args.Q * args.R * args.D, kProfTensor);
+  // the second pass's time counts, its operations were counted by the first
+  auto* ev = prof_slot(args.gate ? 0LL : 2LL * args.Q * args.R * args.D, kProfTensor);
   if (ev) cudaEventRecord(ev->first, stream);
-  knn_fused_kernel<KT><<<qblocks * args.chunks, kKfThreads, kKfSmemBytes, stream>>>(mqh, mql, mrh, mrl, args);
+  knn_fused_kernel<KL><<<qblocks * args.chunks, kKfThreads, kKfSmemBytes, stream>>>(mqh, mql, mrh, mrl, args);
   count_launch();
   if (ev) cudaEventRecord(ev->second, stream);
   SIMD2_CUDA_TRY(cudaGetLastError());
   const int lists = 2 * args.chunks;
   const int G = lists <= 2 ? 2 : lists <= 4 ? 4 : lists <= 8 ? 8 : lists <= 16 ? 16 : 32;
   const int grid = grid_for((long long)(args.Q + 32 / G - 1) / (32 / G) * 32);
-  auto merge = G == 2 ? knn_merge_kernel<KT, 2> : G == 4 ? knn_merge_kernel<KT, 4> : G == 8 ? knn_merge_kernel<KT, 8>
-             : G == 16 ? knn_merge_kernel<KT, 16> : knn_merge_kernel<KT, 32>;
-  merge<<<grid, 256, 0, stream>>>(args.part_d, args.part_i, args.Q, lists, od, oi, ldo, kout);
+  auto merge = G == 2 ? knn_merge_kernel<KL, KT, 2> : G == 4 ? knn_merge_kernel<KL, KT, 4>
+             : G == 8 ? knn_merge_kernel<KL, KT, 8> : G == 16 ? knn_merge_kernel<KL, KT, 16>
+             : knn_merge_kernel<KL, KT, 32>;
+  merge<<<grid, 256, 0, stream>>>(args.part_d, args.part_i, args.Q, lists, od, oi, ldo, kout, flags, args.gate);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   return SIMD2_OK;
+}
+
+// The fused k-NN in up to two passes.  For k > 8 the first pass keeps lists
+// of KT / 2 per (query, chunk half) -- about half the insertion work, and
+// enough unless one half of one chunk holds more than KT / 2 of a query's
+// neighbours; the merge flags every query block where that may have cut a
+// list short, and the second pass redoes just those blocks with lists of KT
+// (its CTAs and merge rows of unflagged blocks exit at once).  Both passes
+// are enqueued; the call stays asynchronous and the result is the one-pass
+// result bit for bit.  Lists of 4 for k = 5..8 are cut short in most blocks
+// of 128 random queries (one of the ~30 lists holding 4 of the top 8 is
+// common), so those k run one pass.
+template <int KT>
+int knn_fused_launch(const CUtensorMap& mqh, const CUtensorMap& mql, const CUtensorMap& mrh, const CUtensorMap& mrl,
+                     KnnFusedArgs a, int qblocks, float* od, int32_t* oi, long long ldo, int kout, float* pd2,
+                     int32_t* pi2, unsigned* ready2, int* flags, cudaStream_t stream) {
+  if constexpr (KT >= 16) {
+    if (kout > KT / 2) {
+      SIMD2_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)qblocks * sizeof(int), stream));
+      int rc = knn_fused_pass<KT / 2, KT>(mqh, mql, mrh, mrl, a, qblocks, od, oi, ldo, kout, flags, stream);
+      if (rc) return rc;
+      KnnFusedArgs b = a;
+      b.part_d = pd2;
+      b.part_i = pi2;
+      b.ready = ready2;
+      b.gate = flags;
+      SIMD2_CUDA_TRY(cudaMemsetAsync(ready2, 0, (size_t)qblocks * a.chunks * 4, stream));
+      return knn_fused_pass<KT, KT>(mqh, mql, mrh, mrl, b, qblocks, od, oi, ldo, kout, nullptr, stream);
+    }
+  }
+  return knn_fused_pass<KT, KT>(mqh, mql, mrh, mrl, a, qblocks, od, oi, ldo, kout, nullptr, stream);
 }
 
 // Query rows per chunk so that one chunk's distance block stays near 1 GiB.
@@ -2649,6 +2685,9 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   const size_t nq = take((size_t)Q * 4), nr = take((size_t)tiles * kKfBN * 4), tm = take((size_t)tiles * 4);
   const size_t pd = take((size_t)Q * 2 * chunks * KT * 4), pi = take((size_t)Q * 2 * chunks * KT * 4);
   const size_t rf = take((size_t)qblocks * chunks * 4);
+  // the second pass's lists, ready flags, and the first pass's block flags
+  const size_t pd2 = take((size_t)Q * 2 * chunks * KT * 4), pi2 = take((size_t)Q * 2 * chunks * KT * 4);
+  const size_t rf2 = take((size_t)qblocks * chunks * 4), qf = take((size_t)qblocks * 4);
   void* p = nullptr;
   int rc = get_workspace(stream, off, &p);
   if (rc) return rc;
@@ -2701,12 +2740,24 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   a.part_d = reinterpret_cast<float*>(ws + pd);
   a.part_i = reinterpret_cast<int32_t*>(ws + pi);
   a.ready = reinterpret_cast<unsigned*>(ws + rf);
+  a.kout = k;
+  a.gate = nullptr;
   SIMD2_CUDA_TRY(cudaMemsetAsync(a.ready, 0, (size_t)qblocks * chunks * 4, stream));
+  float* p_d2 = reinterpret_cast<float*>(ws + pd2);
+  int32_t* p_i2 = reinterpret_cast<int32_t*>(ws + pi2);
+  unsigned* r2 = reinterpret_cast<unsigned*>(ws + rf2);
+  int* flags = reinterpret_cast<int*>(ws + qf);
   switch (KT) {
-    case 4: return knn_fused_launch<4>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
-    case 8: return knn_fused_launch<8>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
-    case 16: return knn_fused_launch<16>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
-    default: return knn_fused_launch<32>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, stream);
+    case 4:
+      return knn_fused_launch<4>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, p_d2, p_i2, r2, flags, stream);
+    case 8:
+      return knn_fused_launch<8>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, p_d2, p_i2, r2, flags, stream);
+    case 16:
+      return knn_fused_launch<16>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, p_d2, p_i2, r2, flags,
+                                  stream);
+    default:
+      return knn_fused_launch<32>(mqh, mql, mrh, mrl, a, qblocks, out_dist, out_idx, ldo, k, p_d2, p_i2, r2, flags,
+                                  stream);
   }
 }
 

@@ -74,6 +74,8 @@ struct KnnFusedArgs {
   float* part_d;          // [Q][2 * chunks][K]
   int32_t* part_i;
   unsigned* ready;        // [query blocks][chunks]: 1 once the unit's lists are written (zeroed per call)
+  int kout;               // neighbours asked for, at most 2K (K < kout: half-length lists, see knn_fused)
+  const int* gate;        // nullable: a query block whose gate[block] is 0 is skipped (the second pass)
 };
 
 // 32-way register select by a runtime index: a 5-level tree of selects, so
@@ -155,8 +157,10 @@ __device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblo
 #pragma unroll
     for (int c = 0; c < 5; c++) {
       if (fresh & (1u << c)) {
-        // the K-th smallest distance of the chunk's two sorted lists together:
-        // min over i of max(A[i-1], B[K-1-i]) (A[-1] = B[-1] = -inf)
+        // A rank-r distance of the chunk's two sorted lists together, r >= kout:
+        // the K-th smallest, min over i of max(A[i-1], B[K-1-i]) (A[-1] =
+        // B[-1] = -inf), when the lists are at least kout long; with half-length
+        // lists (K < kout <= 2K) the 2K-th, max(A[K-1], B[K-1]).
         const int cc = c < 4 ? chunk - 1 - c : 0;
         const float4* pa = reinterpret_cast<const float4*>(a.part_d + ((long long)row * (2 * a.chunks) + 2 * cc) * K);
         float la[K], lb[K];
@@ -166,9 +170,14 @@ __device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblo
           la[4 * u] = x.x, la[4 * u + 1] = x.y, la[4 * u + 2] = x.z, la[4 * u + 3] = x.w;
           lb[4 * u] = y.x, lb[4 * u + 1] = y.y, lb[4 * u + 2] = y.z, lb[4 * u + 3] = y.w;
         }
-        float kth = fminf(lb[K - 1], la[K - 1]);
+        float kth;
+        if (a.kout <= K) {
+          kth = fminf(lb[K - 1], la[K - 1]);
 #pragma unroll
-        for (int i = 1; i < K; i++) kth = fminf(kth, fmaxf(la[i - 1], lb[K - 1 - i]));
+          for (int i = 1; i < K; i++) kth = fminf(kth, fmaxf(la[i - 1], lb[K - 1 - i]));
+        } else {
+          kth = fmaxf(la[K - 1], lb[K - 1]);
+        }
         T = fminf(T, kth);
       }
     }
@@ -197,6 +206,8 @@ __global__ void __launch_bounds__(kKfThreads, 1)
   const int qblocks = (a.Q + kKfBM - 1) / kKfBM;
   const int chunk = blockIdx.x / qblocks;
   const int m0 = (blockIdx.x - chunk * qblocks) * kKfBM;
+  // second pass: only the query blocks the merge flagged
+  if (a.gate && a.gate[m0 / kKfBM] == 0) return;
   int t0, ntiles;
   knn_unit_tiles(a, chunk, &t0, &ntiles);
   const int P = a.panels;
@@ -451,26 +462,38 @@ __device__ __forceinline__ void topk_insert_lex(float (&bd)[K], int (&bi)[K], fl
   }
 }
 
-// Merges each query's `lists` sorted lists of K candidates into the kout
+// Merges each query's `lists` sorted lists of KL candidates into the kout
 // smallest by (distance, index), writes their square roots and indices (-1
-// where fewer than kout references exist).
+// where fewer than kout references exist).  K (>= kout) is the capacity of a
+// lane's list.
 // G = lanes per query (a power of two, 32 / G queries per warp).  When
 // lists <= G, lane l of a group loads list l whole into registers (16-byte
 // loads) and the group takes kout rounds of a (distance, index) argmin over
 // the lanes' heads, the winner shifting its list by one.  Otherwise each lane
 // first folds lists l, l+G, ... into one sorted list by insertion.
-template <int K, int G>
+//
+// flags (KL < kout, the first pass of knn_fused): a list of KL entries that
+// is full may have left out candidates at or above its last entry (its unit
+// pruned with its own KL-th).  Those could belong to the result only when
+// that last entry precedes the result's kout-th in (distance, index) order;
+// then flags[query block] is set and the block is redone with full-length
+// lists.  gate (the second pass): only the query blocks with gate[block] set
+// are merged and written.
+template <int KL, int K, int G>
 __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict__ part_d,
                                                         const int32_t* __restrict__ part_i, int rows, int lists,
                                                         float* __restrict__ out_d, int32_t* __restrict__ out_i,
-                                                        long long ldo, int kout) {
+                                                        long long ldo, int kout, int* __restrict__ flags,
+                                                        const int* __restrict__ gate) {
+  static_assert(KL <= K, "input lists fit a lane's list");
   const int lane = threadIdx.x & 31;
   const int sub = lane & (G - 1);
   const float inf = __int_as_float(0x7f800000);
-  constexpr int kGroups = 32 / G;  // queries per warp
+  constexpr int kGroups = 32 / G;  // queries per warp, all in one block of 128 rows
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   // the loop bound is uniform across the warp, so every lane takes the shuffles
   for (int r0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kGroups; r0 < rows; r0 += nwarps * kGroups) {
+    if (gate && gate[r0 / kKfBM] == 0) continue;  // uniform across the warp
     const int r = r0 + lane / G;
     const bool live = r < rows;
     float bd[K];
@@ -480,23 +503,35 @@ __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict_
       bd[t] = inf;
       bi[t] = 0x7fffffff;
     }
+    // the smallest last entry of a full input list this lane holds
+    float fl = inf;
+    int fli = 0x7fffffff;
     if (live && lists <= G) {
       if (sub < lists) {
-        const float4* ld = reinterpret_cast<const float4*>(part_d + ((long long)r * lists + sub) * K);
-        const int4* li = reinterpret_cast<const int4*>(part_i + ((long long)r * lists + sub) * K);
+        const float4* ld = reinterpret_cast<const float4*>(part_d + ((long long)r * lists + sub) * KL);
+        const int4* li = reinterpret_cast<const int4*>(part_i + ((long long)r * lists + sub) * KL);
 #pragma unroll
-        for (int u = 0; u < K / 4; u++) {
+        for (int u = 0; u < KL / 4; u++) {
           const float4 v = ld[u];
           const int4 w = li[u];
           bd[4 * u] = v.x, bd[4 * u + 1] = v.y, bd[4 * u + 2] = v.z, bd[4 * u + 3] = v.w;
           bi[4 * u] = w.x, bi[4 * u + 1] = w.y, bi[4 * u + 2] = w.z, bi[4 * u + 3] = w.w;
         }
+        if (bi[KL - 1] != 0x7fffffff) {
+          fl = bd[KL - 1];
+          fli = bi[KL - 1];
+        }
       }
     } else if (live) {
       for (int l = sub; l < lists; l += G) {
-        const float* ld = part_d + ((long long)r * lists + l) * K;
-        const int32_t* li = part_i + ((long long)r * lists + l) * K;
-        for (int e = 0; e < K; e++) {
+        const float* ld = part_d + ((long long)r * lists + l) * KL;
+        const int32_t* li = part_i + ((long long)r * lists + l) * KL;
+        const int last = li[KL - 1];
+        if (last != 0x7fffffff && lex_less(ld[KL - 1], last, fl, fli)) {
+          fl = ld[KL - 1];
+          fli = last;
+        }
+        for (int e = 0; e < KL; e++) {
           const float v = ld[e];
           const int ix = li[e];
           if (!lex_less(v, ix, bd[K - 1], bi[K - 1])) break;  // the list is sorted
@@ -504,9 +539,11 @@ __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict_
         }
       }
     }
+    float v = inf;
+    int ix = 0x7fffffff;
     for (int t = 0; t < kout; t++) {
-      float v = bd[0];
-      int ix = bi[0];
+      v = bd[0];
+      ix = bi[0];
 #pragma unroll
       for (int o = G / 2; o > 0; o >>= 1) {
         const float v2 = __shfl_xor_sync(0xffffffffu, v, o);
@@ -530,6 +567,8 @@ __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict_
         out_i[(long long)r * ldo + t] = ix == 0x7fffffff ? -1 : ix;
       }
     }
+    // (v, ix) is now the kout-th result, the same in every lane of the group
+    if (flags && live && lex_less(fl, fli, v, ix)) atomicOr(&flags[r / kKfBM], 1);
   }
 }
 
