@@ -601,17 +601,29 @@ def extra_measurements(args, dev):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for mode in ("fused", "materialised"):
         s2.knn(Q, R, 16, mode=mode)  # warm-up at full size (workspace growth stays outside the timing)
-        ev0.record()
-        kd, ki = s2.knn(Q, R, 16, mode=mode)
-        ev1.record()
         torch.cuda.synchronize()
+        with s2.KernelTimer() as kt:
+            ev0.record()
+            kd, ki = s2.knn(Q, R, 16, mode=mode)
+            ev1.record()
+            torch.cuda.synchronize()
         kms = ev0.elapsed_time(ev1)
+        dist_ms = kt.by_kind.get("tensor", (0, 0, 0))[0]
         cfg4[f"knn_16384x65536x128_k16_{mode}"] = {
             "ms": kms, "queries_per_s": 16384 / kms * 1e3, "gops": 2.0 * 16384 * 65536 * 128 / kms / 1e6,
             "how": "simd2_knn_ex, CUDA events: " + (
                 "selection inside the BF16 hi/lo distance MMA's epilogue, then a per-query merge" if mode == "fused"
                 else "BF16 hi/lo minus_square blocks of 1 GiB written, then top-k + sqrt")}
+        # distance kernels' own time (both passes of the fused mode); BF16 hi/lo = 3 MMAs per product
+        peaks, peak_source = measured_peaks()
+        bf16_tf = 3 * 2.0 * 16384 * 65536 * 128 / dist_ms / 1e9 if dist_ms > 0 else None
+        cfg4[f"knn_16384x65536x128_k16_{mode}"]["distance_kernel"] = {
+            "ms": dist_ms, "bf16_tflops": bf16_tf,
+            "frac": bf16_tf / float(peaks["bf16_tflops"]) if bf16_tf else None,
+            "peak": float(peaks["bf16_tflops"]), "peak_source": f"{peak_source} bf16_tflops (cuBLAS burst)"}
         if mode == "fused":
+            cfg4[f"knn_16384x65536x128_k16_{mode}"]["distance_kernel"]["traffic"] = traffic_from_profile(
+                "knn_fused_kernel<8> Q=16384 R=65536 D=128 k=16")
             cfg4[f"knn_16384x65536x128_k16_{mode}"]["fp64_error"] = knn_errors(Q, R, kd, ki)
         del kd, ki
     del Q, R
