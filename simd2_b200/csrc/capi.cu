@@ -1544,7 +1544,8 @@ constexpr int kSpSmemAccMaxN = 16384;
 
 struct SpPlan {
   int grid;            // persistent CTAs
-  size_t smem;         // bitmap bytes (COUNT)
+  size_t smem;         // bitmap bytes (COUNT and FILL past kSpSmemAccMaxN columns)
+  size_t smem_count;   // COUNT up to kSpSmemAccMaxN columns: one flag byte per column
   bool smem_acc;       // FILL accumulators in shared memory
   size_t smem_fill;    // FILL: bitmap + accumulators
   size_t acc_off, cnt_off, ctr_off, flag_off, tot_off, total;
@@ -1554,6 +1555,7 @@ SpPlan sp_plan(int M, int N, size_t base) {
   SpPlan p{};
   const size_t bitmap = (size_t)sp_bitmap_words(N) * 4;
   p.smem = bitmap;
+  p.smem_count = (size_t)sp_flag_bytes(N);
   // the FILL pass keeps the row's accumulators in shared memory up to 16384 columns
   p.smem_acc = N <= kSpSmemAccMaxN;
   p.smem_fill = bitmap + (p.smem_acc ? (size_t)N * 4 : 0);
@@ -1577,10 +1579,10 @@ SpPlan sp_plan(int M, int N, size_t base) {
 
 template <bool COUNT, bool DENSE = false, bool SMEM = false>
 int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t stream) {
-  if constexpr (!COUNT && !SMEM) {
+  if constexpr (!SMEM) {
     if (plan.smem_acc) return spgemm_launch<COUNT, DENSE, true>(op, args, plan, stream);
   }
-  const size_t smem = SMEM ? plan.smem_fill : plan.smem;
+  const size_t smem = SMEM ? (COUNT ? plan.smem_count : plan.smem_fill) : plan.smem;
   auto pick = [&](auto kern) -> int {
     if (smem > (48u << 10))
       SIMD2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -117,21 +117,28 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* s_warp, int* tot
 // min/max adds fold in any order on non-NaN values, so their FILL runs
 // without the per-k barrier: values live in the scratch as order-preserving
 // unsigned keys (larger float, larger key) folded with atomicMin / atomicMax.
-// -0.0 (excluded by the precondition, and no product of other values is
-// -0.0) is the one value whose key differs from an equal float's.
+// -0.0 is the one value whose key differs from an equal float's; operands
+// hold none (the precondition), and a sum of two values that are not -0.0,
+// or the selection of one of them, is never -0.0.
+// kUntouched lies past every float's key on the side the fold moves away
+// from (all ones for min, zero for max), so a key still at kUntouched marks a
+// column no product reached.
 template <int OP>
 struct SpKey {
   static constexpr bool kUnordered = OP != SIMD2_PLUS_MUL;
   static constexpr bool kMin = OP == SIMD2_MIN_PLUS || OP == SIMD2_MIN_MAX;
+  static constexpr uint32_t kUntouched = kMin ? 0xffffffffu : 0u;
   __device__ static uint32_t key(float f) {
     const uint32_t u = __float_as_uint(f);
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
   }
   __device__ static float value(uint32_t k) { return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k); }
-  __device__ static void fold(uint32_t* p, float v) {
-    if (v != v) return;  // a NaN product is dropped, as the dense min / max drops it
-    if constexpr (kMin) atomicMin(p, key(v));
-    else atomicMax(p, key(v));
+  // A NaN product is dropped, as the dense min / max drops it; it still
+  // reaches its column, so the add identity is folded in its place.
+  __device__ static void fold(uint32_t* p, float v, float ident) {
+    const uint32_t k = key(v != v ? ident : v);
+    if constexpr (kMin) atomicMin(p, k);
+    else atomicMax(p, k);
   }
 };
 
@@ -139,16 +146,31 @@ struct SpKey {
 // after it in shared memory starts 16-byte aligned.
 __host__ __device__ constexpr int sp_bitmap_words(int n) { return ((n + 31) / 32 + 3) & ~3; }
 
-// SMEM: the row's accumulators live in shared memory after the bitmap (N
-// floats or keys), else in the CTA's slice of the global scratch.
+// Bytes of shared memory for the COUNT pass's column flags (one byte per
+// column, rounded to 16 bytes for the vector clears).
+__host__ __device__ constexpr int sp_flag_bytes(int n) { return (n + 15) & ~15; }
+
+// SMEM (N <= 16384): the row's state lives in shared memory --
+//   COUNT: one flag byte per column, set with plain stores (every writer
+//     stores 1, so no atomics: the lanes of a warp that reach neighbouring
+//     columns of a near-dense B row would serialise on one bitmap word);
+//   FILL, min/max adds: the accumulator keys alone (a key at kUntouched is a
+//     column no product reached; no bitmap, no atomicOr per product);
+//   FILL, plus_mul: the bitmap and the N accumulators after it.
+// Otherwise the bitmap sits in shared memory and the accumulators in the
+// CTA's slice of the global scratch.
 template <int OP, bool COUNT, bool DENSE = false, bool SMEM = false>
-__global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
+__global__ void __launch_bounds__(kSpThreads, 2048 / kSpThreads) spgemm_rows_kernel(SpArgs a) {
   using O = SpOps<OP>;
   using KY = SpKey<OP>;
   // warp-parallel over k: COUNT always, FILL for the order-independent adds
   constexpr bool kWarpK = COUNT || KY::kUnordered;
-  extern __shared__ uint32_t sp_smem[];
+  constexpr bool kBytes = SMEM && COUNT;                      // flag bytes
+  constexpr bool kKeysOnly = SMEM && !COUNT && KY::kUnordered;  // keys, no bitmap
+  constexpr uint32_t kUntouched = KY::kUntouched;
+  extern __shared__ __align__(16) uint32_t sp_smem[];
   uint32_t* bitmap = sp_smem;  // ceil(N / 32) words
+  uint8_t* flags = reinterpret_cast<uint8_t*>(sp_smem);
   __shared__ int s_row;
   __shared__ int s_warp[kSpThreads / 32];
   const int words = (a.N + 31) >> 5;
@@ -157,8 +179,9 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
   uint32_t* acck = reinterpret_cast<uint32_t*>(acc);
   const float ident = O::ident();
   if constexpr (!COUNT && KY::kUnordered) {
-    // the accumulators start at the identity; every row puts back what it touched
-    const uint32_t ik = KY::key(ident);
+    // the accumulators start untouched (keys only) or at the identity; every
+    // row puts back what it touched
+    const uint32_t ik = kKeysOnly ? kUntouched : KY::key(ident);
     for (int j = threadIdx.x; j < a.N; j += kSpThreads) acck[j] = ik;
   }
   // the value of touched column j once the row's folds are done
@@ -179,7 +202,12 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
   };
   while (true) {
     if (threadIdx.x == 0) s_row = atomicAdd(a.next_row, 1);
-    for (int w = threadIdx.x; w < words; w += kSpThreads) bitmap[w] = 0u;
+    if constexpr (kBytes) {
+      for (int w = threadIdx.x; w < sp_flag_bytes(a.N) / 16; w += kSpThreads)
+        reinterpret_cast<uint4*>(flags)[w] = make_uint4(0u, 0u, 0u, 0u);
+    } else if constexpr (!kKeysOnly) {
+      for (int w = threadIdx.x; w < words; w += kSpThreads) bitmap[w] = 0u;
+    }
     __syncthreads();
     const int r = s_row;
     if (r >= a.M) break;
@@ -216,8 +244,9 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
         if (k < 0) continue;
         auto put = [&](int j, float bvv) {
           if ((unsigned)j >= (unsigned)a.N) return;
-          atomicOr(&bitmap[j >> 5], 1u << (j & 31));
-          if constexpr (!COUNT) KY::fold(acck + j, O::mul(av, bvv));
+          if constexpr (kBytes) flags[j] = 1;
+          else if constexpr (!kKeysOnly) atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+          if constexpr (!COUNT) KY::fold(acck + j, O::mul(av, bvv), ident);
         };
         // four predicated loads per lane per round trip, so a row under 128
         // entries costs one round trip too
@@ -257,16 +286,76 @@ __global__ void __launch_bounds__(kSpThreads) spgemm_rows_kernel(SpArgs a) {
       for (int f = max(a.cp[r], 0) + threadIdx.x; f < g1; f += kSpThreads) {
         const int j = a.cj[f];
         if ((unsigned)j >= (unsigned)a.N) continue;
-        const uint32_t bit = 1u << (j & 31);
-        const uint32_t old = atomicOr(&bitmap[j >> 5], bit);
-        if constexpr (!COUNT) {
-          if constexpr (KY::kUnordered) KY::fold(acck + j, a.cv[f]);
-          else acc[j] = O::add((old & bit) ? acc[j] : ident, a.cv[f]);
+        if constexpr (kBytes) {
+          flags[j] = 1;
+        } else if constexpr (kKeysOnly) {
+          KY::fold(acck + j, a.cv[f], ident);
+        } else {
+          const uint32_t bit = 1u << (j & 31);
+          const uint32_t old = atomicOr(&bitmap[j >> 5], bit);
+          if constexpr (!COUNT) {
+            if constexpr (KY::kUnordered) KY::fold(acck + j, a.cv[f], ident);
+            else acc[j] = O::add((old & bit) ? acc[j] : ident, a.cv[f]);
+          }
         }
       }
     }
     __syncthreads();
-    if constexpr (COUNT) {
+    if constexpr (kBytes) {
+      // flag bytes are 0 or 1, so a word's popcount is its flag count
+      int cnt = 0;
+      for (int w = threadIdx.x; w < sp_flag_bytes(a.N) / 16; w += kSpThreads) {
+        const uint4 f = reinterpret_cast<const uint4*>(flags)[w];
+        cnt += __popc(f.x) + __popc(f.y) + __popc(f.z) + __popc(f.w);
+      }
+      int total;
+      block_exclusive_scan(cnt, s_warp, &total);
+      if (threadIdx.x == 0) a.row_nnz[r] = total;
+    } else if constexpr (kKeysOnly && DENSE) {
+      // the touched columns straight into the dense row (the rest holds the identity)
+      float* drow = a.dense_u8 ? nullptr : a.dense + (long long)r * a.ldd;
+      uint8_t* brow = a.dense_u8 ? a.dense_u8 + (long long)r * a.ldd : nullptr;
+      for (int j = threadIdx.x; j < a.N; j += kSpThreads) {
+        const uint32_t k = acck[j];
+        if (k != kUntouched) {
+          acck[j] = kUntouched;
+          if (brow) brow[j] = 1;
+          else drow[j] = KY::value(k);
+        }
+      }
+    } else if constexpr (kKeysOnly) {
+      // columns in increasing order: warp w owns the contiguous column range
+      // [w * span, (w + 1) * span), counts it with ballots, and writes it at
+      // the row offset plus the counts of the warps before it
+      constexpr int kWarps = kSpThreads / 32;
+      const int span = ((a.N + kWarps * 32 - 1) / (kWarps * 32)) * 32;
+      const int c0 = warp * span, c1 = min(a.N, c0 + span);
+      int cnt = 0;
+      for (int jb = c0; jb < c1; jb += 32) {
+        const int j = jb + lane;
+        cnt += __popc(__ballot_sync(0xffffffffu, j < c1 && acck[j] != kUntouched));
+      }
+      if (lane == 0) s_warp[warp] = cnt;
+      __syncthreads();
+      long long pos = a.dp[r];
+      for (int w = 0; w < warp; w++) pos += s_warp[w];
+      const long long out_end = min((long long)a.dp[r + 1], a.d_cap);
+      for (int jb = c0; jb < c1; jb += 32) {
+        const int j = jb + lane;
+        const uint32_t k = j < c1 ? acck[j] : kUntouched;
+        const bool t = k != kUntouched;
+        const uint32_t m = __ballot_sync(0xffffffffu, t);
+        if (t) {
+          const long long at = pos + __popc(m & ((1u << lane) - 1u));
+          acck[j] = kUntouched;
+          if (at >= 0 && at < out_end) {
+            a.dj[at] = j;
+            a.dv[at] = KY::value(k);
+          }
+        }
+        pos += __popc(m);
+      }
+    } else if constexpr (COUNT) {
       int cnt = 0;
       for (int w = threadIdx.x; w < words; w += kSpThreads) cnt += __popc(bitmap[w]);
       int total;
