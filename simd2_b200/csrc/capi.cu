@@ -1558,7 +1558,7 @@ SpPlan sp_plan(int M, int N, size_t base) {
   p.smem_count = (size_t)sp_flag_bytes(N);
   // the FILL pass keeps the row's accumulators in shared memory up to 16384 columns
   p.smem_acc = N <= kSpSmemAccMaxN;
-  p.smem_fill = bitmap + (p.smem_acc ? (size_t)N * 4 : 0);
+  p.smem_fill = bitmap + (p.smem_acc ? (size_t)sp_acc_words(N) * 4 : 0);
   // CTAs per SM: by the FILL pass's shared memory and by the SM's 2048 threads
   int per_sm = (int)std::max<size_t>(
       1, std::min<size_t>(std::min<size_t>(8, 2048 / kSpThreads), (200u << 10) / std::max<size_t>(p.smem_fill, 1)));

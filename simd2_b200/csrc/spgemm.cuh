@@ -149,6 +149,9 @@ __host__ __device__ constexpr int sp_bitmap_words(int n) { return ((n + 31) / 32
 // Bytes of shared memory for the COUNT pass's column flags (one byte per
 // column, rounded to 16 bytes for the vector clears).
 __host__ __device__ constexpr int sp_flag_bytes(int n) { return (n + 15) & ~15; }
+// Shared-memory accumulators: N rounded up to 4, so that the keys-only
+// write-out reads them 4 at a time (the padding stays untouched).
+__host__ __device__ constexpr int sp_acc_words(int n) { return (n + 3) & ~3; }
 
 // SMEM (N <= 16384): the row's state lives in shared memory --
 //   COUNT: one flag byte per column, set with plain stores (every writer
@@ -182,7 +185,8 @@ __global__ void __launch_bounds__(kSpThreads, 2048 / kSpThreads) spgemm_rows_ker
     // the accumulators start untouched (keys only) or at the identity; every
     // row puts back what it touched
     const uint32_t ik = kKeysOnly ? kUntouched : KY::key(ident);
-    for (int j = threadIdx.x; j < a.N; j += kSpThreads) acck[j] = ik;
+    const int n_acc = kKeysOnly ? sp_acc_words(a.N) : a.N;
+    for (int j = threadIdx.x; j < n_acc; j += kSpThreads) acck[j] = ik;
   }
   // the value of touched column j once the row's folds are done
   auto result = [&](int j) -> float {
@@ -315,45 +319,68 @@ __global__ void __launch_bounds__(kSpThreads, 2048 / kSpThreads) spgemm_rows_ker
       // the touched columns straight into the dense row (the rest holds the identity)
       float* drow = a.dense_u8 ? nullptr : a.dense + (long long)r * a.ldd;
       uint8_t* brow = a.dense_u8 ? a.dense_u8 + (long long)r * a.ldd : nullptr;
-      for (int j = threadIdx.x; j < a.N; j += kSpThreads) {
-        const uint32_t k = acck[j];
-        if (k != kUntouched) {
-          acck[j] = kUntouched;
-          if (brow) brow[j] = 1;
-          else drow[j] = KY::value(k);
+      // four keys per thread and load (the padding past N is untouched)
+      for (int j = 4 * threadIdx.x; j < a.N; j += 4 * kSpThreads) {
+        const uint4 k4 = *reinterpret_cast<const uint4*>(acck + j);
+        const uint32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+          if (kk[s] != kUntouched) {
+            acck[j + s] = kUntouched;
+            if (brow) brow[j + s] = 1;
+            else drow[j + s] = KY::value(kk[s]);
+          }
         }
       }
     } else if constexpr (kKeysOnly) {
       // columns in increasing order: warp w owns the contiguous column range
-      // [w * span, (w + 1) * span), counts it with ballots, and writes it at
-      // the row offset plus the counts of the warps before it
+      // [w * span, (w + 1) * span) (span a multiple of 128), lane l the keys
+      // 4l..4l+3 of each 128-column step, read with one 16-byte load.  A first
+      // pass counts the range, a second writes it at the row offset plus the
+      // counts of the warps before it, skipping steps with nothing touched.
       constexpr int kWarps = kSpThreads / 32;
-      const int span = ((a.N + kWarps * 32 - 1) / (kWarps * 32)) * 32;
+      const int span = ((a.N + kWarps * 128 - 1) / (kWarps * 128)) * 128;
       const int c0 = warp * span, c1 = min(a.N, c0 + span);
       int cnt = 0;
-      for (int jb = c0; jb < c1; jb += 32) {
-        const int j = jb + lane;
-        cnt += __popc(__ballot_sync(0xffffffffu, j < c1 && acck[j] != kUntouched));
+      for (int jb = c0; jb < c1; jb += 128) {
+        const int j = jb + 4 * lane;
+        if (j < c1) {
+          const uint4 k4 = *reinterpret_cast<const uint4*>(acck + j);
+          cnt += (k4.x != kUntouched) + (k4.y != kUntouched) + (k4.z != kUntouched) + (k4.w != kUntouched);
+        }
       }
+      cnt = __reduce_add_sync(0xffffffffu, cnt);
       if (lane == 0) s_warp[warp] = cnt;
       __syncthreads();
       long long pos = a.dp[r];
       for (int w = 0; w < warp; w++) pos += s_warp[w];
       const long long out_end = min((long long)a.dp[r + 1], a.d_cap);
-      for (int jb = c0; jb < c1; jb += 32) {
-        const int j = jb + lane;
-        const uint32_t k = j < c1 ? acck[j] : kUntouched;
-        const bool t = k != kUntouched;
-        const uint32_t m = __ballot_sync(0xffffffffu, t);
-        if (t) {
-          const long long at = pos + __popc(m & ((1u << lane) - 1u));
-          acck[j] = kUntouched;
-          if (at >= 0 && at < out_end) {
-            a.dj[at] = j;
-            a.dv[at] = KY::value(k);
+      for (int jb = c0; jb < c1; jb += 128) {
+        const int j = jb + 4 * lane;
+        uint4 k4 = make_uint4(kUntouched, kUntouched, kUntouched, kUntouched);
+        if (j < c1) k4 = *reinterpret_cast<const uint4*>(acck + j);
+        const uint32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+        const int c = (kk[0] != kUntouched) + (kk[1] != kUntouched) + (kk[2] != kUntouched) + (kk[3] != kUntouched);
+        if (!__any_sync(0xffffffffu, c != 0)) continue;  // uniform across the warp
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        long long at = pos + incl - c;
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+          if (kk[s] != kUntouched) {
+            acck[j + s] = kUntouched;
+            if (at >= 0 && at < out_end) {
+              a.dj[at] = j + s;
+              a.dv[at] = KY::value(kk[s]);
+            }
+            at++;
           }
         }
-        pos += __popc(m);
+        pos += __shfl_sync(0xffffffffu, incl, 31);
       }
     } else if constexpr (COUNT) {
       int cnt = 0;
