@@ -1620,12 +1620,12 @@ int spgemm_count(int op, int M, int N, int K, const int* ap, const int* aj, int 
                  const SpPlan& plan, cudaStream_t stream) {
   int* flag = reinterpret_cast<int*>(ws + plan.flag_off);
   SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, 8, stream));
-  csr_check_kernel<<<grid_for(M), 256, 0, stream>>>(M, K, ap, aj, a_nnz, flag);
-  csr_check_kernel<<<grid_for(K), 256, 0, stream>>>(K, N, bp, bj, b_nnz, flag);
+  csr_check_kernel<<<grid_for(32LL * M), 256, 0, stream>>>(M, K, ap, aj, a_nnz, flag);
+  csr_check_kernel<<<grid_for(32LL * K), 256, 0, stream>>>(K, N, bp, bj, b_nnz, flag);
   count_launch();
   count_launch();
   if (cp) {
-    csr_check_kernel<<<grid_for(M), 256, 0, stream>>>(M, N, cp, cj, c_nnz, flag);
+    csr_check_kernel<<<grid_for(32LL * M), 256, 0, stream>>>(M, N, cp, cj, c_nnz, flag);
     count_launch();
   }
   SIMD2_CUDA_TRY(cudaGetLastError());

@@ -431,65 +431,68 @@ __global__ void __launch_bounds__(kSpThreads, 2048 / kSpThreads) spgemm_rows_ker
 
 // CSR structure check: rowptr[0] == 0, rowptr[rows] == nnz, offsets
 // nondecreasing, columns in [0, ncols) and strictly increasing within a row.
-// Sets *bad on any violation.
+// Sets *bad on any violation.  One warp per row, its lanes over the row's
+// entries, each comparing its column with the one before it.
 __global__ void csr_check_kernel(int rows, int ncols, const int* __restrict__ rp, const int* __restrict__ cj, int nnz,
                                  int* __restrict__ bad) {
   int b = 0;
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  if (tid == 0 && (rp[0] != 0 || rp[rows] != nnz)) b = 1;
-  for (long long r = tid; r < rows; r += stride) {
+  const int lane = threadIdx.x & 31;
+  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  if (gw == 0 && lane == 0 && (rp[0] != 0 || rp[rows] != nnz)) b = 1;
+  for (long long r = gw; r < rows; r += nw) {
     const int s0 = rp[r], s1 = rp[r + 1];
-    if (s1 < s0 || s0 < 0 || s1 > nnz) {
+    if (s1 < s0 || s0 < 0 || s1 > nnz) {  // uniform across the warp
       b = 1;
       continue;
     }
-    int prev = -1;
-    for (int e = s0; e < s1; e++) {
+    for (int e = s0 + lane; e < s1; e += 32) {
       const int j = cj[e];
+      const int prev = e > s0 ? cj[e - 1] : -1;
       if (j <= prev || j >= ncols) b = 1;
-      prev = j;
     }
   }
-  if (b) atomicOr(bad, 1);
+  if (__any_sync(0xffffffffu, b) && lane == 0) atomicOr(bad, 1);
 }
 
-// Exclusive prefix sum of counts[0..n) into out[0..n], one block; *total
-// receives the exact sum, *overflow is set when it exceeds INT32 range.
+// Exclusive prefix sum of counts[0..n) into out[0..n], one block of 1024
+// threads, each over a contiguous chunk of counts: chunk sums, one block
+// scan of them, then each thread writes its chunk.  *total receives the
+// exact sum, *overflow is set when it exceeds INT32 range (the offsets from
+// there on hold INT32_MAX).
 __global__ void __launch_bounds__(1024) offsets_scan_kernel(const int* __restrict__ counts, int n,
                                                             int* __restrict__ out, int* __restrict__ overflow,
                                                             long long* __restrict__ total) {
   __shared__ long long s_part[32];
-  __shared__ long long s_base;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_base = 0;
-  __syncthreads();
-  for (int c0 = 0; c0 < n; c0 += 1024) {
-    const int i = c0 + threadIdx.x;
-    long long v = i < n ? counts[i] : 0;
-    const long long x = v;
+  const int chunk = (n + 1023) / 1024;
+  const long long b0 = (long long)threadIdx.x * chunk;
+  const long long b1 = min((long long)n, b0 + chunk);
+  long long sum = 0;
+  for (long long i = b0; i < b1; i++) sum += counts[i];
+  long long v = sum;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const long long y = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += y;
-    }
-    if (lane == 31) s_part[warp] = v;
-    __syncthreads();
-    long long wb = 0, tot = 0;
-    for (int w = 0; w < 32; w++) {
-      if (w < warp) wb += s_part[w];
-      tot += s_part[w];
-    }
-    const long long excl = s_base + wb + v - x;
-    if (i < n) out[i] = excl > 0x7fffffffLL ? 0x7fffffff : (int)excl;
-    __syncthreads();
-    if (threadIdx.x == 0) s_base += tot;
-    __syncthreads();
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) s_part[warp] = v;
+  __syncthreads();
+  long long base = 0, tot = 0;
+  for (int w = 0; w < 32; w++) {
+    const long long t = s_part[w];
+    if (w < warp) base += t;
+    tot += t;
+  }
+  long long run = base + v - sum;
+  for (long long i = b0; i < b1; i++) {
+    out[i] = run > 0x7fffffffLL ? 0x7fffffff : (int)run;
+    run += counts[i];
   }
   if (threadIdx.x == 0) {
-    out[n] = s_base > 0x7fffffffLL ? 0x7fffffff : (int)s_base;
-    if (s_base > 0x7fffffffLL) *overflow = 1;
-    *total = s_base;
+    out[n] = tot > 0x7fffffffLL ? 0x7fffffff : (int)tot;
+    if (tot > 0x7fffffffLL) *overflow = 1;
+    *total = tot;
   }
 }
 
