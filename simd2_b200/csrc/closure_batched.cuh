@@ -87,12 +87,16 @@ struct BatchMaps {
 
 // One k-tile of the 8 x 4 register tile; ROWS < 8 skips rows ty + 16i for
 // i >= ROWS (tile rows 16 ROWS..127), used when those rows lie past the graph.
-template <int OP, int ROWS>
+// Q = 8 runs the whole k-tile; Q = 0 runs its first qn groups of 4 k (the
+// graph's last k-tile: groups wholly past column n hold only NaN padding,
+// whose products min/max drop).
+template <int OP, int ROWS, int Q>
 __device__ __forceinline__ void batched_mac_ktile(float (&acc)[8][4], const float* As, const float* Bs, int ty,
-                                                  int tx, int cbase, int swz) {
+                                                  int tx, int cbase, int swz, int qn) {
   constexpr int WN = 2;
+  const int qe = Q ? Q : qn;
 #pragma unroll 2
-  for (int q = 0; q < kBK / 4; q++) {
+  for (int q = 0; q < qe; q++) {
     float4 a[ROWS];
 #pragma unroll
     for (int ii = 0; ii < ROWS; ii++)
@@ -113,6 +117,21 @@ __device__ __forceinline__ void batched_mac_ktile(float (&acc)[8][4], const floa
         }
       }
     }
+  }
+}
+
+template <int OP, int Q>
+__device__ __forceinline__ void batched_mac_rows(int row_groups, float (&acc)[8][4], const float* As, const float* Bs,
+                                                 int ty, int tx, int cbase, int swz, int qn) {
+  switch (row_groups) {
+    case 1: batched_mac_ktile<OP, 1, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 2: batched_mac_ktile<OP, 2, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 3: batched_mac_ktile<OP, 3, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 4: batched_mac_ktile<OP, 4, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 5: batched_mac_ktile<OP, 5, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 6: batched_mac_ktile<OP, 6, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 7: batched_mac_ktile<OP, 7, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    default: batched_mac_ktile<OP, 8, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
   }
 }
 
@@ -221,16 +240,10 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
           // the warps of the upper column half sit out a tile whose columns end
           // by column 64 -- what they would compute is never stored.
           if (!idle_cols) {
-            switch (row_groups) {
-              case 1: batched_mac_ktile<OP, 1>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 2: batched_mac_ktile<OP, 2>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 3: batched_mac_ktile<OP, 3>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 4: batched_mac_ktile<OP, 4>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 5: batched_mac_ktile<OP, 5>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 6: batched_mac_ktile<OP, 6>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 7: batched_mac_ktile<OP, 7>(acc, As, Bs, ty, tx, cbase, swz); break;
-              default: batched_mac_ktile<OP, 8>(acc, As, Bs, ty, tx, cbase, swz); break;
-            }
+            // groups of 4 k of this k-tile that hold graph columns
+            const int qn = min(kBK / 4, (n - i * kBK + 3) >> 2);
+            if (qn == kBK / 4) batched_mac_rows<OP, kBK / 4>(row_groups, acc, As, Bs, ty, tx, cbase, swz, qn);
+            else batched_mac_rows<OP, 0>(row_groups, acc, As, Bs, ty, tx, cbase, swz, qn);
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
@@ -405,12 +418,14 @@ __device__ __forceinline__ uint32_t bh_max2(uint32_t a, uint32_t b) {
 
 // One 64-k tile of the FP16 8 x 4 register tile (rows ty + 16i, i < ROWS):
 // A chunk q (k pairs 4q..4q+3 of a row, 16 bytes) sits at chunk q ^ (row & 7)
-// of the 128-byte row; B pair row pr holds 128 words.
-template <int OP, int ROWS>
+// of the 128-byte row; B pair row pr holds 128 words.  Q = 8: the whole
+// k-tile; Q = 0: its first qn chunks of 8 k (the rest is NaN padding).
+template <int OP, int ROWS, int Q>
 __device__ __forceinline__ void batched_h2_ktile(uint32_t (&acc)[8][4], const uint8_t* As, const uint32_t* Bs, int ty,
-                                                 int tx, int cbase, int swz) {
+                                                 int tx, int cbase, int swz, int qn) {
+  const int qe = Q ? Q : qn;
 #pragma unroll 2
-  for (int q = 0; q < 8; q++) {
+  for (int q = 0; q < qe; q++) {
     uint4 a[ROWS];
 #pragma unroll
     for (int i = 0; i < ROWS; i++) a[i] = *reinterpret_cast<const uint4*>(As + (ty + 16 * i) * 128 + ((q ^ swz) << 4));
@@ -435,6 +450,21 @@ __device__ __forceinline__ void batched_h2_ktile(uint32_t (&acc)[8][4], const ui
         }
       }
     }
+  }
+}
+
+template <int OP, int Q>
+__device__ __forceinline__ void batched_h2_rows(int row_groups, uint32_t (&acc)[8][4], const uint8_t* As,
+                                                const uint32_t* Bs, int ty, int tx, int cbase, int swz, int qn) {
+  switch (row_groups) {
+    case 1: batched_h2_ktile<OP, 1, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 2: batched_h2_ktile<OP, 2, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 3: batched_h2_ktile<OP, 3, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 4: batched_h2_ktile<OP, 4, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 5: batched_h2_ktile<OP, 5, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 6: batched_h2_ktile<OP, 6, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    case 7: batched_h2_ktile<OP, 7, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
+    default: batched_h2_ktile<OP, 8, Q>(acc, As, Bs, ty, tx, cbase, swz, qn); break;
   }
 }
 
@@ -537,16 +567,10 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
           const uint8_t* As = smem + s * kStageBytes;
           const uint32_t* Bs = reinterpret_cast<const uint32_t*>(As + kATileBytes);
           if (!idle_cols) {
-            switch (row_groups) {
-              case 1: batched_h2_ktile<OP, 1>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 2: batched_h2_ktile<OP, 2>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 3: batched_h2_ktile<OP, 3>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 4: batched_h2_ktile<OP, 4>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 5: batched_h2_ktile<OP, 5>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 6: batched_h2_ktile<OP, 6>(acc, As, Bs, ty, tx, cbase, swz); break;
-              case 7: batched_h2_ktile<OP, 7>(acc, As, Bs, ty, tx, cbase, swz); break;
-              default: batched_h2_ktile<OP, 8>(acc, As, Bs, ty, tx, cbase, swz); break;
-            }
+            // chunks of 8 k of this k-tile that hold graph columns
+            const int qn = min(8, (n - i * kH2BK + 7) >> 3);
+            if (qn == 8) batched_h2_rows<OP, 8>(row_groups, acc, As, Bs, ty, tx, cbase, swz, qn);
+            else batched_h2_rows<OP, 0>(row_groups, acc, As, Bs, ty, tx, cbase, swz, qn);
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
