@@ -1577,10 +1577,17 @@ SpPlan sp_plan(int M, int N, size_t base) {
   return p;
 }
 
-template <bool COUNT, bool DENSE = false, bool SMEM = false>
-int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t stream) {
+// keys = false (CSR FILL only): the min/max FILL keeps its bitmap, for results
+// sparser than 1/32 on average (the keys-only write-out reads all N keys of a row).
+template <bool COUNT, bool DENSE = false, bool SMEM = false, bool KEYS = true>
+int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t stream, bool keys = true) {
   if constexpr (!SMEM) {
-    if (plan.smem_acc) return spgemm_launch<COUNT, DENSE, true>(op, args, plan, stream);
+    if (plan.smem_acc) {
+      if constexpr (!COUNT && !DENSE) {
+        if (!keys) return spgemm_launch<COUNT, DENSE, true, false>(op, args, plan, stream);
+      }
+      return spgemm_launch<COUNT, DENSE, true>(op, args, plan, stream);
+    }
   }
   const size_t smem = SMEM ? (COUNT ? plan.smem_count : plan.smem_fill) : plan.smem;
   auto pick = [&](auto kern) -> int {
@@ -1592,11 +1599,11 @@ int spgemm_launch(int op, const SpArgs& args, const SpPlan& plan, cudaStream_t s
     return SIMD2_OK;
   };
   switch (op) {
-    case SIMD2_MIN_PLUS: return pick(spgemm_rows_kernel<SIMD2_MIN_PLUS, COUNT, DENSE, SMEM>);
-    case SIMD2_MAX_PLUS: return pick(spgemm_rows_kernel<SIMD2_MAX_PLUS, COUNT, DENSE, SMEM>);
-    case SIMD2_MAX_MIN: return pick(spgemm_rows_kernel<SIMD2_MAX_MIN, COUNT, DENSE, SMEM>);
-    case SIMD2_MIN_MAX: return pick(spgemm_rows_kernel<SIMD2_MIN_MAX, COUNT, DENSE, SMEM>);
-    case SIMD2_PLUS_MUL: return pick(spgemm_rows_kernel<SIMD2_PLUS_MUL, COUNT, DENSE, SMEM>);
+    case SIMD2_MIN_PLUS: return pick(spgemm_rows_kernel<SIMD2_MIN_PLUS, COUNT, DENSE, SMEM, KEYS>);
+    case SIMD2_MAX_PLUS: return pick(spgemm_rows_kernel<SIMD2_MAX_PLUS, COUNT, DENSE, SMEM, KEYS>);
+    case SIMD2_MAX_MIN: return pick(spgemm_rows_kernel<SIMD2_MAX_MIN, COUNT, DENSE, SMEM, KEYS>);
+    case SIMD2_MIN_MAX: return pick(spgemm_rows_kernel<SIMD2_MIN_MAX, COUNT, DENSE, SMEM, KEYS>);
+    case SIMD2_PLUS_MUL: return pick(spgemm_rows_kernel<SIMD2_PLUS_MUL, COUNT, DENSE, SMEM>);  // ordered: no keys
     default: return SIMD2_ERR_UNSUPPORTED;
   }
 }
@@ -1666,7 +1673,9 @@ int spgemm_fill(int op, int M, int N, int K, const int* ap, const int* aj, const
   a.acc = reinterpret_cast<float*>(ws + plan.acc_off);
   a.next_row = reinterpret_cast<int*>(ws + plan.ctr_off);
   SIMD2_CUDA_TRY(cudaMemsetAsync(a.next_row, 0, 4, stream));
-  return spgemm_launch<false>(op, a, plan, stream);
+  // d_cap is the result's entry count (every caller sizes D from COUNT)
+  const bool keys = d_cap > (long long)M * (N / 32);
+  return spgemm_launch<false>(op, a, plan, stream, keys);
 }
 
 // FILL pass into a dense M x N matrix D (pitch ldd) that holds the identity.

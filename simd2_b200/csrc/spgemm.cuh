@@ -162,14 +162,18 @@ __host__ __device__ constexpr int sp_acc_words(int n) { return (n + 3) & ~3; }
 //   FILL, plus_mul: the bitmap and the N accumulators after it.
 // Otherwise the bitmap sits in shared memory and the accumulators in the
 // CTA's slice of the global scratch.
-template <int OP, bool COUNT, bool DENSE = false, bool SMEM = false>
+//
+// KEYS = false keeps the bitmap in the min/max FILL too (marking it costs an
+// atomicOr per product, the write-out walks N/32 words instead of N keys):
+// the host picks it for results sparser than 1/32 on average.
+template <int OP, bool COUNT, bool DENSE = false, bool SMEM = false, bool KEYS = true>
 __global__ void __launch_bounds__(kSpThreads, 2048 / kSpThreads) spgemm_rows_kernel(SpArgs a) {
   using O = SpOps<OP>;
   using KY = SpKey<OP>;
   // warp-parallel over k: COUNT always, FILL for the order-independent adds
   constexpr bool kWarpK = COUNT || KY::kUnordered;
   constexpr bool kBytes = SMEM && COUNT;                      // flag bytes
-  constexpr bool kKeysOnly = SMEM && !COUNT && KY::kUnordered;  // keys, no bitmap
+  constexpr bool kKeysOnly = KEYS && SMEM && !COUNT && KY::kUnordered;  // keys, no bitmap
   constexpr uint32_t kUntouched = KY::kUntouched;
   extern __shared__ __align__(16) uint32_t sp_smem[];
   uint32_t* bitmap = sp_smem;  // ceil(N / 32) words

@@ -57,6 +57,26 @@ def test_spgemm_matches_dense_oracle(cuda, op, shape, with_c):
 
 
 @pytest.mark.parametrize("op", OPS)
+@pytest.mark.parametrize("density", [0.002, 0.05])
+def test_spgemm_sparse_and_dense_results(cuda, op, density):
+    """4096 columns (shared-memory accumulators) with results on both sides of
+    the 1/32 average row density at which the min/max fill switches between
+    its bitmap form (0.002: ~0.2 % dense) and its keys-only form (0.05:
+    ~70 % dense); with C, against the dense oracle bit for bit."""
+    M, N, K = 64, 4096, 512
+    rng = np.random.default_rng(int(density * 1000) + len(op))
+    a, _ = sparse_dense(op, M, K, density, rng)
+    b, _ = sparse_dense(op, K, N, density, rng)
+    c, _ = sparse_dense(op, M, N, density, rng)
+    D = s2.spgemm(op, to_csr(a, op, cuda), to_csr(b, op, cuda), N, C=to_csr(c, op, cuda))
+    nnz = D[1].numel()
+    assert (nnz <= M * N // 32) == (density < 0.01)
+    got = s2.csr_to_dense(D, N, op).cpu().numpy()
+    want = oracle.srgemm(op, a, b, c, do_epilogue=True)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("op", OPS)
 @pytest.mark.parametrize("n_cols", [300, 17000])
 def test_spgemm_dense_ties(cuda, op, n_cols):
     """Dense-ish operands with values in {1, 2}: many products meet on every
