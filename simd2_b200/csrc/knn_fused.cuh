@@ -136,17 +136,22 @@ __device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
 // all in flight together, and only a chunk seen ready for the first time
 // (bit c of *seen: chunk - 1 - c, bit 4: the pilot) costs a fence -- which,
 // after the flag read, orders the list loads after the writer's release --
-// and the loads of its two K-th distances.  Returns the updated bound.
-template <int K>
-__device__ __forceinline__ float knn_prior_bound(const KnnFusedArgs& a, int qblock, int chunk, int row, float T,
-                                                 unsigned* seen) {
+// and the loads of its two lists.  knn_prior_flags issues the flag loads,
+// knn_prior_fold folds the newly ready chunks into the bound.
+__device__ __forceinline__ void knn_prior_flags(const KnnFusedArgs& a, int qblock, int chunk, unsigned (&f)[5]) {
   const unsigned* flags = a.ready + (long long)qblock * a.chunks;
   const int lo = max(0, chunk - 4);
   const bool pilot = a.pilot_tiles > 0 && lo > 0;
-  unsigned f[5];
 #pragma unroll
   for (int c = 0; c < 4; c++) f[c] = chunk - 1 - c >= lo ? ld_relaxed_gpu(flags + chunk - 1 - c) : 0u;
   f[4] = pilot ? ld_relaxed_gpu(flags) : 0u;
+}
+
+// Folds the lists of the chunks that f shows ready and *seen does not yet
+// hold into the bound T.
+template <int K>
+__device__ __forceinline__ float knn_prior_fold(const KnnFusedArgs& a, int chunk, int row, float T, unsigned* seen,
+                                                const unsigned (&f)[5]) {
   unsigned fresh = 0;
 #pragma unroll
   for (int c = 0; c < 5; c++) fresh |= (f[c] != 0u ? 1u : 0u) << c;
@@ -331,11 +336,23 @@ __global__ void __launch_bounds__(kKfThreads, 1)
     const int qblock = m0 / kKfBM;
     float prior = __int_as_float(0x7f800000);  // bound from earlier chunks' lists
     unsigned seen = 0;                          // earlier chunks already folded into it
+    // The bound is refreshed every tile while the unit is young (a pilot unit
+    // may finish meanwhile), then every 8 tiles.  The flags a refresh folds
+    // were loaded at the refresh before it, so their latency hides behind a
+    // tile's selection (tile 0 loads and folds at once); flags seen a tile
+    // late only leave the bound looser meanwhile.
+    unsigned pf[5] = {0u, 0u, 0u, 0u, 0u};
+    const bool refreshing = row_ok && chunk > 0;
+    if (refreshing) {
+      knn_prior_flags(a, qblock, chunk, pf);
+      prior = knn_prior_fold<K>(a, chunk, row, prior, &seen, pf);
+    }
     for (int t = 0; t < ntiles; t++) {
       const int acc = t & 1;
-      // the bound is refreshed every tile while the unit is young (a pilot
-      // unit may finish meanwhile), then every 8 tiles
-      if (row_ok && chunk > 0 && (t < 8 || (t & 7) == 0)) prior = knn_prior_bound<K>(a, qblock, chunk, row, prior, &seen);
+      if (refreshing && (t < 8 || (t & 7) == 0)) {
+        if (t > 0) prior = knn_prior_fold<K>(a, chunk, row, prior, &seen, pf);
+        knn_prior_flags(a, qblock, chunk, pf);
+      }
       if (ok && !mbar_wait(&acc_full[acc], (t >> 1) & 1)) {
         report_timeout(115);
         ok = false;
