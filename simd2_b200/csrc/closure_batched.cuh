@@ -42,35 +42,6 @@ struct BatchGraph {
   int changed;  // out: 1 if the last step still changed something
 };
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Stage one k-tile (A rows m0..m0+127, k kt*32..+31; P rows kt*16..+15,
-// floats 2*n0..2*n0+255) into shared memory with the same layout the TMA path
-// produces: A with the 128-byte swizzle (16-byte chunk c of row r stored at
-// chunk c ^ (r & 7)), P dense.
-__device__ __forceinline__ void batch_stage_load(uint8_t* st, const float* X, int Kp, const float* P, int Np, int m0,
-                                                 int n0, int kt) {
-  float* As = reinterpret_cast<float*>(st);
-  float* Bs = reinterpret_cast<float*>(st + kATileBytes);
-  // A: 128 rows x 8 chunks of 16 bytes = 1024 copies
-  for (int c = threadIdx.x; c < kBM * (kBK / 4); c += kSimtThreads) {
-    const int r = c >> 3, q = c & 7;
-    cp_async16(As + r * kBK + ((q ^ (r & 7)) << 2), X + (long long)(m0 + r) * Kp + kt * kBK + q * 4);
-  }
-  // P: 16 rows x 64 chunks = 1024 copies
-  for (int c = threadIdx.x; c < (kBK / 2) * (2 * kBN / 4); c += kSimtThreads) {
-    const int r = c >> 6, q = c & 63;
-    cp_async16(Bs + r * (2 * kBN) + q * 4, P + (long long)(kt * (kBK / 2) + r) * (2LL * Np) + 2 * n0 + q * 4);
-  }
-}
-
 __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
