@@ -240,19 +240,6 @@ __global__ void bool_copy_kernel(const T* __restrict__ C, long long ldc, T* __re
   }
 }
 
-// float {-inf,0,1} -> 0/1 of type T (or_and result).
-template <typename T>
-__global__ void bool_out_kernel(const float* __restrict__ S, long long lds, T* __restrict__ D, long long ldd, int M,
-                                int N) {
-  const long long total = (long long)M * N;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / N);
-    const int j = (int)(t - (long long)i * N);
-    D[(long long)i * ldd + j] = S[(long long)i * lds + j] > 0.5f ? T(1) : T(0);
-  }
-}
-
 }  // namespace simd2
 
 namespace simd2 {
@@ -415,18 +402,6 @@ __global__ void row_norms_kernel(const float* __restrict__ A, long long lda, int
 // double -> float (norms accumulated in FP64).
 __global__ void round_norms_kernel(const double* __restrict__ in, int n, float* __restrict__ out) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) out[j] = (float)in[j];
-}
-
-// Squared column norms of B [K][N], accumulated in FP64, rounded to float.
-__global__ void col_norms_kernel(const float* __restrict__ B, long long ldb, int K, int N, float* __restrict__ out) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int k = 0; k < K; k++) {
-      const double v = B[(long long)k * ldb + j];
-      s += v * v;
-    }
-    out[j] = (float)s;
-  }
 }
 
 }  // namespace simd2
