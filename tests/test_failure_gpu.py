@@ -8,7 +8,6 @@ arguments, non-convergence) are checked too.
 """
 import ctypes
 
-import numpy as np
 import pytest
 import torch
 
