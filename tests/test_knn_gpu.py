@@ -111,29 +111,32 @@ def test_knn_fused_rejects_wide_points(cuda):
     assert torch.all(d == 0)
 
 
-@pytest.mark.parametrize("k", [16, 10, 32, 6])
-def test_knn_fused_half_lists_redo_flagged_blocks(cuda, k):
+@pytest.mark.parametrize("k,Q", [(16, 512), (10, 512), (32, 512), (6, 512), (16, 500), (12, 500)])
+def test_knn_fused_half_lists_redo_flagged_blocks(cuda, k, Q):
     """For k > 4 the fused path first keeps lists of half the size per chunk
     half and redoes, with full lists, every query block where one list may
     have been cut short.  Here the queries of blocks 1 and 3 have all their
     nearest references in one half of one reference tile (a tight cluster at
     indices 256..383), the other blocks' queries are spread out: the result
     must equal the materialised path bit for bit, with both kinds of block in
-    one call, and the oracle's neighbours."""
-    rng = np.random.default_rng(k)
-    D, R, Q = 64, 4096, 512
+    one call, and the oracle's neighbours.  Q = 500 makes the last, clustered
+    block a partial one (rows 384..499)."""
+    rng = np.random.default_rng(k + Q)
+    D, R = 64, 4096
     r = rng.standard_normal((R, D)).astype(np.float32) * 4
     center = rng.standard_normal(D).astype(np.float32) * 4
     r[256:384] = center + 0.05 * rng.standard_normal((128, D)).astype(np.float32)
     q = rng.standard_normal((Q, D)).astype(np.float32) * 4
     for blk in (1, 3):
-        q[blk * 128:(blk + 1) * 128] = center + 0.05 * rng.standard_normal((128, D)).astype(np.float32)
+        rows = min(Q, (blk + 1) * 128) - blk * 128
+        q[blk * 128:blk * 128 + rows] = center + 0.05 * rng.standard_normal((rows, D)).astype(np.float32)
     Qt, Rt = torch.from_numpy(q).to(cuda), torch.from_numpy(r).to(cuda)
     d1, i1 = s2.knn(Qt, Rt, k, mode="fused")
     d2, i2 = s2.knn(Qt, Rt, k, mode="materialised")
     assert torch.equal(i1, i2)
     assert torch.equal(d1.view(torch.int32), d2.view(torch.int32))
     ii = i1.cpu().numpy()
-    assert np.all((ii[128:256] >= 256) & (ii[128:256] < 384))  # the clustered blocks' neighbours
+    for lo, hi in ((128, 256), (384, Q)):  # the clustered blocks' neighbours
+        assert np.all((ii[lo:hi] >= 256) & (ii[lo:hi] < 384))
     check(q, r, k, d1.cpu().numpy(), ii)
     assert s2.device_status() == 0
