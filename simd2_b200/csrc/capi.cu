@@ -1038,7 +1038,17 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   const size_t f_off = x_off + align_up((size_t)n * n * 4, kAlign);
   // flag word + learned decision (256 bytes), then one change flag per step
   const size_t o_off = f_off + align_up(256 + (size_t)(max_iter + 1) * sizeof(int), kAlign);
-  const size_t total = o_off + (need_occ ? align_up(occ.total, kAlign) : 0);
+  // Delta steps (see srgemm_simt_kernel, SKIP): the learned and rules loops of
+  // a min_plus / max_plus closure with the exact change test keep, per step,
+  // which 32 x 32 blocks changed, in two ping-pong pairs of maps laid out as
+  // the occupancy maps.  Recording runs (autotuner timings per configuration)
+  // and fixed configurations keep the plain steps.
+  const bool use_delta = (op == SIMD2_MIN_PLUS || op == SIMD2_MAX_PLUS) && conv == SIMD2_CONV_EXACT && can_skip &&
+                         (dispatch == 2 || dispatch == 3) && step_feat == nullptr;
+  const size_t cmA = align_up((size_t)occ.tiles_m * occ.ktiles, kAlign);
+  const size_t cmB = align_up((size_t)occ.ktiles * occ.tiles_n, kAlign);
+  const size_t c_off = o_off + (need_occ ? align_up(occ.total, kAlign) : 0);
+  const size_t total = c_off + (use_delta ? 2 * (cmA + cmB) : 0);
   void* p = nullptr;
   if ((rc = get_workspace(stream, total, &p))) return rc;
   uint8_t* ws = static_cast<uint8_t*>(p);
@@ -1046,6 +1056,12 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   int* flag = reinterpret_cast<int*>(ws + f_off);
   int* decision = flag + 8;  // [0] config, [1 + c] prediction of config c
   uint8_t* obase = ws + o_off;
+  uint8_t* chg[2][2] = {};  // [parity][A map, B map]
+  if (use_delta)
+    for (int q = 0; q < 2; q++) {
+      chg[q][0] = ws + c_off + q * (cmA + cmB);
+      chg[q][1] = chg[q][0] + cmA;
+    }
 
   // The opening: sparse steps while X is sparse, under the dispatch's policy
   // (bitwise change test only).
@@ -1150,14 +1166,22 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   // without skipping (feature recording keeps the pass).
   const unsigned long long all_triples = (unsigned long long)occ.tiles_m * occ.tiles_n * occ.ktiles;
   bool occ_on = need_occ;
+  // occ_fresh: the occupancy maps hold this step's input; occ_full: every
+  // block triple was occupied, so the maps are all ones and stay valid (a
+  // closure only fills X in).  A delta step needs one or the other.
+  bool occ_fresh = false, occ_full = false;
+  bool prev_chg = false;  // the previous step wrote change maps (chg[par ^ 1])
+  int par = 0;
   auto settle = [&]() {
     if ((dispatch == 2 || dispatch == 3) && !step_feat && hst[0] >= all_triples) {
       occ_on = false;
+      occ_full = true;
       cfg_id &= 3;
     }
   };
   if (need_occ) {
     if ((rc = enqueue_occ(cur, ldcur)) || (rc = read_back(false, true))) return rc;
+    occ_fresh = true;
     if (dispatch == 2) cfg_id = hbuf[8];  // decision[0]
     if (step_feat) mlp_features(n, occ.tiles_m, occ.tiles_n, occ.ktiles, hst, sms, step_feat);
     settle();
@@ -1165,7 +1189,8 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
   while (changed && it < max_iter) {
     SimtConfig cfg;
     cfg.split = config_split(cfg_id);
-    cfg.skip = config_skip(cfg_id) && can_skip && occ_on;
+    const bool delta = use_delta && prev_chg && (occ_fresh || occ_full);
+    cfg.skip = can_skip && ((config_skip(cfg_id) && occ_on) || delta);
     if (cfg.skip) {
       cfg.occA = obase + occ.occA;
       cfg.occB = obase + occ.occB;
@@ -1179,14 +1204,29 @@ int closure_f32_ex(int op, int n, float* X, long long ldx, int max_iter, int con
     if (step_ms) cudaEventRecord(ev[0], stream);
     const bool pk = !a_tma_ok(cur, ldcur);
     const Plan pl = make_plan(n, n, n, pk, selection_op(op));
-    const EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, flag, conv);
+    EpilogueArgs ep = make_epilogue(cur, ldcur, nxt, ldnxt, 1, flag, conv);
+    if (use_delta) {
+      if (cudaMemsetAsync(chg[par][0], 0, cmA + cmB, stream) != cudaSuccess) {
+        rc = SIMD2_ERR_CUDA;
+        break;
+      }
+      ep.chgA = chg[par][0];
+      ep.chgB = chg[par][1];
+      if (delta && cfg.skip) {
+        ep.dA = chg[par ^ 1][0];
+        ep.dB = chg[par ^ 1][1];
+      }
+    }
     rc = srgemm_core<float, 0>(op, n, n, n, cur, ldcur, cur, ldcur, ep, ws, pl, pk, stream, cfg);
     if (rc) break;
     if (step_ms) cudaEventRecord(ev[1], stream);
     it++;
+    prev_chg = use_delta;
+    par ^= 1;
     // the rules policy needs no statistics for a configuration that does not skip
     const bool next = occ_on && it < max_iter && (dispatch != 3 || config_skip(cfg_id) || step_feat);
     if (next && (rc = enqueue_occ(nxt, ldnxt))) break;
+    occ_fresh = next;
     float srg_ms = 0.f;
     if ((rc = read_back(true, next))) break;
     if (step_ms) {

@@ -87,6 +87,16 @@ struct EpilogueArgs {
   const int* gate;  // nullable: when *gate == 0 the kernel does nothing (closure
                     // step enqueued after the fixed point was reached)
   const int* gate2;  // nullable second gate (the FP16 / FP32 path choice)
+  // Closure delta steps (square M = N = K, srgemm_simt_kernel only): chgA /
+  // chgB, when set, receive a 1 for every 32 x 32 block of D that differs from
+  // C, in the layouts of the occupancy maps (chgA[tile row][k-tile] for the
+  // block's rows as an A block, chgB[k-tile][tile column] as a B block); dA /
+  // dB, when set, are the previous step's maps, and a SKIP kernel keeps only
+  // the k-tiles whose A or B block changed in that step.
+  uint8_t* chgA;
+  uint8_t* chgB;
+  const uint8_t* dA;
+  const uint8_t* dB;
 };
 
 __device__ __forceinline__ bool conv_changed(int mode, float old_v, float new_v) {
@@ -132,7 +142,12 @@ __device__ __forceinline__ float ld_dsmem_f32(const float* local_ptr, uint32_t r
 //   SKIP      : the k list holds only the k-tiles whose A block (128 rows x
 //               32 k) and B block (32 k x 128 columns) both contain an entry
 //               other than the (x)-annihilator (occupancy maps occA, occB);
-//               a skipped block can only produce identity products.
+//               a skipped block can only produce identity products.  With
+//               ep.dA / ep.dB (a closure step X_{t+1} = X_t (+) X_t (x) X_t
+//               whose C is X_t) it also needs the A or the B block to have
+//               changed in step t: every product of unchanged blocks was a
+//               product of step t too and is already folded into X_t, so with
+//               a min / max (+) it cannot change the result.
 template <int OP, int STAGES, int SPLIT, bool SKIP>
 __global__ void __launch_bounds__(kSimtThreads, 1)
     srgemm_simt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M,
@@ -180,7 +195,8 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     int running = 0;
     for (int base = 0; base < ktiles; base += kSimtThreads) {
       const int kt = base + threadIdx.x;
-      const bool f = kt < ktiles && occA[(long long)tm * ktiles + kt] && occB[(long long)kt * tiles_n + tn];
+      const bool f = kt < ktiles && occA[(long long)tm * ktiles + kt] && occB[(long long)kt * tiles_n + tn] &&
+                     (!ep.dA || ep.dA[(long long)tm * ktiles + kt] || ep.dB[(long long)kt * tiles_n + tn]);
       const unsigned ballot = __ballot_sync(0xffffffffu, f);
       if (lane == 0) s_warp_cnt[warp] = __popc(ballot);
       __syncthreads();
@@ -296,6 +312,9 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
   float* Dbase = ep.D;
   const long long ldc = ep.ldc, ldd = ep.ldd;
   int changed = 0;
+  // bit 4 g + c: an element of the tile's 32 x 32 block (row group g, column
+  // group c) changed (used only when ep.chgA is set)
+  uint32_t bmask = 0;
 
   if constexpr (SPLIT == 1) {
     const int vec2 = ep.vec2;
@@ -322,20 +341,25 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
 #pragma unroll
         for (int c = 0; c < WN; c++) {
           const int col = n0 + cbase + 32 * c + 2 * tx;
+          int ch = 0;
           if (vec2 && col + 1 < N) {
             const float2 cv = cpre[i][c];
             float2 v;
-            v.x = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c], cv.x, changed);
-            v.y = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + 1], cv.y, changed);
+            v.x = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c], cv.x, ch);
+            v.y = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + 1], cv.y, ch);
             *reinterpret_cast<float2*>(drow + col) = v;
           } else {
 #pragma unroll
             for (int e = 0; e < 2; e++) {
               if (col + e < N) {
                 const float cv = do_epi ? crow[col + e] : 0.0f;
-                drow[col + e] = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + e], cv, changed);
+                drow[col + e] = epilogue_value<OP>(do_epi, conv_mode, track, acc[i][2 * c + e], cv, ch);
               }
             }
+          }
+          if (ch) {
+            changed = 1;
+            bmask |= 1u << (((i >> 1) << 2) | ((cbase >> 5) + c));  // row ty + 16 i lies in group i / 2
           }
         }
       }
@@ -365,13 +389,30 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
       const int row = m0 + r, gcol = n0 + col;
       if (ok && row < M && gcol < N) {
         const float cv = do_epi ? Cbase[(long long)row * ldc + gcol] : 0.0f;
-        Dbase[(long long)row * ldd + gcol] = epilogue_value<OP>(do_epi, conv_mode, track, v, cv, changed);
+        int ch = 0;
+        Dbase[(long long)row * ldd + gcol] = epilogue_value<OP>(do_epi, conv_mode, track, v, cv, ch);
+        if (ch) {
+          changed = 1;
+          bmask |= 1u << (((r >> 5) << 2) | (col >> 5));
+        }
       }
     }
     cluster_sync_all();  // peers stay resident until every CTA has read their partials
   }
   if (track) {
     if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
+  }
+  if (ep.chgA) {
+    // every writer stores 1, so no atomics; a set bit implies an element
+    // inside the matrix, so both indices are in range
+    const uint32_t m = __reduce_or_sync(0xffffffffu, bmask);
+    if (lane == 0 && m) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (m & (0x1111u << q)) ep.chgA[(long long)tm * ktiles + 4 * tn + q] = 1;  // column group q
+        if (m & (0xfu << (4 * q))) ep.chgB[(long long)(4 * tm + q) * tiles_n + tn] = 1;  // row group q
+      }
+    }
   }
 }
 
