@@ -280,3 +280,36 @@ def test_autotuned_dense_configs(cuda):
     Xd = torch.from_numpy(x.copy()).to(cuda)
     rd = s2.closure_ex("min_plus", Xd, dispatch="dense", record=True)
     assert rd["configs"] == ra["configs"]
+
+
+@pytest.mark.parametrize("case", ["min_plus_rmat", "max_plus_dag"])
+def test_delta_steps_identical(cuda, case):
+    """The rules and learned loops of a min_plus / max_plus closure skip, from
+    the second dense step on, the k-tiles whose A and B 32 x 32 blocks both
+    stayed unchanged in the step before (their products are already folded in,
+    so a min / max cannot change).  Unrecorded closures (recording keeps plain
+    steps) must equal the plain dense closure bit for bit, with the same step
+    count: an R-MAT graph for min_plus, and for max_plus (longest paths) a
+    random DAG whose closure takes a dozen steps of shrinking change."""
+    import os
+    path = os.path.join(os.path.dirname(s2.__file__), "costmodel_weights.json")
+    params = costmodel.load(path, cuda)
+    if case == "min_plus_rmat":
+        op, n = "min_plus", 4096
+        g = datagen.rmat_graph_device(n, 70.0, seed=4242, device=cuda)
+    else:
+        op, n = "max_plus", 3072
+        gen = torch.Generator(device=cuda).manual_seed(77)
+        w = torch.randint(1, 101, (n, n), device=cuda, generator=gen).float()
+        keep = (torch.rand((n, n), device=cuda, generator=gen) < 0.002) & torch.ones(n, n, device=cuda).triu(1).bool()
+        g = torch.where(keep, w, torch.full_like(w, float("-inf")))
+        g.fill_diagonal_(0.0)
+    Xd = g.clone()
+    it_d = s2.closure_ex(op, Xd, dispatch="dense")
+    assert it_d >= 3
+    for kw in ({"dispatch": "rules", "config": s2.config_id(1, True)}, {"dispatch": "learned", "mlp_params": params}):
+        X = g.clone()
+        it = s2.closure_ex(op, X, **kw)
+        assert it == it_d, kw["dispatch"]
+        assert torch.equal(X.view(torch.int32), Xd.view(torch.int32)), kw["dispatch"]
+    assert s2.device_status() == 0
