@@ -699,10 +699,18 @@ int srgemm_tc_sum(int op, int M, int N, int K, const float* A, long long lda, co
   return launch_tc<0>(M, N, K, ma0, ma1, mb0, mb1, ep, stream);
 }
 
+// delta (or_and closure, pair kernel only): the maps of TcEpilogue.
+struct TcDelta {
+  uint8_t* chg_row = nullptr;
+  uint8_t* chg_col = nullptr;
+  const uint8_t* need_row = nullptr;
+  const uint8_t* need_col = nullptr;
+};
+
 template <typename T>
 int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, long long ldb, const T* C,
                     long long ldc, T* D, long long ldd, int do_epilogue, int* changed, uint8_t* ws,
-                    const TcPlan& plan, cudaStream_t stream) {
+                    const TcPlan& plan, cudaStream_t stream, const TcDelta& delta = TcDelta()) {
   const int Kp = plan.Kp;
   uint8_t* a8 = ws + plan.a0;
   uint8_t* b8 = ws + plan.b0;
@@ -730,7 +738,13 @@ int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, 
   ep.ldd = ldd;
   ep.out_u8 = sizeof(T) == 1;
   ep.changed = changed;
-  if (pair) return launch_tc2<1>(M, N, K, ma, ma, mb, mb, mbh, mbh, ep, stream);
+  if (pair) {
+    ep.chg_row = delta.chg_row;
+    ep.chg_col = delta.chg_col;
+    ep.need_row = delta.need_row;
+    ep.need_col = delta.need_col;
+    return launch_tc2<1>(M, N, K, ma, ma, mb, mb, mbh, mbh, ep, stream);
+  }
   return launch_tc<1>(M, N, K, ma, ma, mb, mb, ep, stream);
 }
 
@@ -1402,24 +1416,49 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
     }
     max_iter -= it0;
   }
-  // Workspace: [tensor-core operands][Xnew n x n bytes][change flag]
+  // Workspace: [tensor-core operands][Xnew n x n bytes][change flag][delta maps]
   const TcPlan plan = tc_plan_u8(n, n, n);
   const size_t x_off = align_up(plan.total, kAlign);
   const size_t f_off = x_off + align_up((size_t)n * n, kAlign);
+  // Delta steps (with the SM-pair kernel): X is squared in place -- the
+  // kernel reads its operands from the packed copies made at the start of the
+  // step, and each thread reads its C bytes before writing them -- so a tile
+  // whose 256 rows and 256 columns did not change in the previous step is
+  // skipped and keeps its bytes (step t's products of unchanged rows and
+  // columns are all in X already).  Ping-pong maps of changed tile rows and
+  // columns carry that from step to step.
+  const bool delta = use_tc2(n, n);
+  const int trows = (n + kTc2BM - 1) / kTc2BM, tcols = (n + kTcBN - 1) / kTcBN;
+  const size_t d_off = f_off + kAlign;
+  const size_t dmap = align_up((size_t)trows + tcols, kAlign);
   void* p = nullptr;
-  if ((rc = get_workspace(stream, f_off + kAlign, &p))) return rc;
+  if ((rc = get_workspace(stream, d_off + (delta ? 2 * dmap : 0), &p))) return rc;
   uint8_t* ws = static_cast<uint8_t*>(p);
   uint8_t* Xn = ws + x_off;
   int* flag = reinterpret_cast<int*>(ws + f_off);
   uint8_t* cur = X;
   long long ldcur = ldx;
-  uint8_t* nxt = Xn;
-  long long ldnxt = n;
-  int it = 0, changed = 1;
+  uint8_t* nxt = delta ? X : Xn;
+  long long ldnxt = delta ? ldx : n;
+  int it = 0, changed = 1, par = 0;
   while (changed && it < max_iter) {
-    it++;
     SIMD2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), stream));
-    rc = srgemm_tc_orand<uint8_t>(n, n, n, cur, ldcur, cur, ldcur, cur, ldcur, nxt, ldnxt, 1, flag, ws, plan, stream);
+    TcDelta dl;
+    if (delta) {
+      uint8_t* mine = ws + d_off + par * dmap;
+      SIMD2_CUDA_TRY(cudaMemsetAsync(mine, 0, (size_t)trows + tcols, stream));
+      dl.chg_row = mine;
+      dl.chg_col = mine + trows;
+      if (it > 0) {  // the first dense step has no previous maps
+        const uint8_t* prev = ws + d_off + (par ^ 1) * dmap;
+        dl.need_row = prev;
+        dl.need_col = prev + trows;
+      }
+      par ^= 1;
+    }
+    it++;
+    rc = srgemm_tc_orand<uint8_t>(n, n, n, cur, ldcur, cur, ldcur, cur, ldcur, nxt, ldnxt, 1, flag, ws, plan, stream,
+                                  dl);
     if (rc) return rc;
     int h = 0;
     SIMD2_CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, stream));

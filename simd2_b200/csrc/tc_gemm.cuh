@@ -174,6 +174,15 @@ struct TcEpilogue {
   float band;           // recompute when dist < band * (|a|^2 + |b|^2)
   int b_rows;           // 1: B32 holds B transposed ([N][K], e.g. k-NN reference points)
   int* changed;         // or_and closure: set to 1 when any D differs from C
+  // Delta steps of the or_and closure (tc_gemm2_kernel only): chg_row[i] /
+  // chg_col[j] receive a 1 when an element of 256-row tile row i / 256-column
+  // tile column j changed; with need_row / need_col (the previous step's maps)
+  // a tile whose tile row and tile column both stayed unchanged is skipped --
+  // every product it would form was formed in that step and is already in C.
+  uint8_t* chg_row;
+  uint8_t* chg_col;
+  const uint8_t* need_row;
+  const uint8_t* need_col;
 };
 
 // sum_k (a[k] - B[k][col])^2 in FP32; B is [K][N] (pitch ldb) or, when

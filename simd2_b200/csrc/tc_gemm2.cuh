@@ -161,6 +161,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   };
 
+  // Delta steps (or_and closure): every role skips the same items, an item
+  // whose tile row and tile column both stayed unchanged in the previous step.
+  auto skip_item = [&](int w) -> bool {
+    if (!ep.need_row) return false;
+    int m0, n0, ncols;
+    item_origin(w, m0, n0, ncols);
+    return !ep.need_row[m0 / kTc2BM] && !ep.need_col[n0 / kTcBN];
+  };
+
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; s++) {
       mbar_init(&full[s], 1);   // used on the even CTA: its producer's expect_tx
@@ -193,6 +202,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int j = 0;
       bool ok = true;
       for (int t = pair; t < items && ok; t += pairs) {
+        if (skip_item(t)) continue;
         int m0, n0, ncols;
         item_origin(t, m0, n0, ncols);
         // this CTA's ncols/2 rows of B^T: a 128-row box, or 64 rows for a half tile
@@ -227,7 +237,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int j = 0;
       bool ok = true;
       int lt = 0;
-      for (int t = pair; t < items && ok; t += pairs, lt++) {
+      // lt counts the items this pair processes (skipped ones excepted): the
+      // accumulator parity and barrier phases follow it
+      for (int t = pair; t < items && ok; t += pairs) {
+        if (skip_item(t)) continue;
         const int acc = lt & 1;
         const uint32_t idesc = t < whole ? tc2_idesc<KIND>() : tc2_idesc<KIND>(kTcBN / 2);
         if (!mbar_wait(&acc_empty[acc], ((lt >> 1) & 1) ^ 1)) {
@@ -263,6 +276,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tc2_commit_both(&empty[s]);  // stage s free in both CTAs once these MMAs have read it
         }
         if (ok) tc2_commit_both(&acc_full[acc]);
+        lt++;
       }
       tc2_commit_both(fin);
     }
@@ -273,7 +287,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint32_t* epi_tile = epi_smem + (warp - 2) * (32 * 33);
     bool ok = true;
     int lt = 0;
-    for (int t = pair; t < items; t += pairs, lt++) {
+    for (int t = pair; t < items; t += pairs) {
+      if (skip_item(t)) continue;
       const int acc = lt & 1;
       if (ok && !mbar_wait(&acc_full[acc], (lt >> 1) & 1)) {
         report_timeout(123);
@@ -289,11 +304,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int changed = 0;
       tc_tile_epilogue<KIND>(ep, M, N, n0, row0, trow, epi_tile, lane, changed, ncols);
       if (ep.changed && KIND == 1) {
-        if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(ep.changed, 1);
+        const bool any = __any_sync(0xffffffffu, changed);
+        if (any && lane == 0) {
+          atomicOr(ep.changed, 1);
+          if (ep.chg_row) {  // every writer stores 1
+            ep.chg_row[m0 / kTc2BM] = 1;
+            ep.chg_col[n0 / kTcBN] = 1;
+          }
+        }
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(map_to_rank(&acc_empty[acc], 0));
+      lt++;
     }
   }
 

@@ -81,3 +81,32 @@ def test_plus_mul_8192(cuda):
     want = oracle.srgemm_f64("plus_mul", a[rows], b)
     bound = (4 * 2.0 ** -16 + 2 * n * 2.0 ** -24) * (np.abs(a[rows]).astype(np.float64) @ np.abs(b))
     assert np.all(np.abs(got - want) <= bound)
+
+
+def test_orand_closure_delta_steps_match_plain_steps(cuda):
+    """The or_and closure squares X in place and, from its second dense step,
+    skips every 256 x 256 tile whose tile row and tile column did not change in
+    the step before.  The whole closed matrix and the step count must equal a
+    loop of plain or_and srgemm steps X <- X | X & X (fresh output each step,
+    no skipping) run until X stops changing."""
+    n = 12288
+    rng = np.random.default_rng(46)
+    m = 2 * n
+    src = torch.from_numpy(rng.integers(0, n, m)).to(cuda)
+    dst = torch.from_numpy(rng.integers(0, n, m)).to(cuda)
+    X0 = torch.zeros((n, n), dtype=torch.uint8, device=cuda)
+    X0[src, dst] = 1
+    X0.fill_diagonal_(1)
+    X = X0.clone()
+    it = s2.closure("or_and", X)
+    Y = X0.clone()
+    steps = 0
+    while True:
+        Z = s2.srgemm("or_and", Y, Y, Y, do_epilogue=True)
+        steps += 1
+        if torch.equal(Z, Y):
+            break
+        Y = Z
+    assert it == steps
+    assert torch.equal(X, Y)
+    assert s2.device_status() == 0
