@@ -1416,10 +1416,11 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
     }
     max_iter -= it0;
   }
-  // Workspace: [tensor-core operands][Xnew n x n bytes][change flag][delta maps]
+  // Workspace: [tensor-core operands][Xnew n x n bytes, without delta steps][change flag][delta maps]
   const TcPlan plan = tc_plan_u8(n, n, n);
+  const bool delta = use_tc2(n, n);
   const size_t x_off = align_up(plan.total, kAlign);
-  const size_t f_off = x_off + align_up((size_t)n * n, kAlign);
+  const size_t f_off = x_off + (delta ? 0 : align_up((size_t)n * n, kAlign));
   // Delta steps (with the SM-pair kernel): X is squared in place -- the
   // kernel reads its operands from the packed copies made at the start of the
   // step, and each thread reads its C bytes before writing them -- so a tile
@@ -1427,14 +1428,13 @@ int simd2_closure_orand_u8(int n, uint8_t* X, int ldx, int max_iter, int* iters_
   // skipped and keeps its bytes (step t's products of unchanged rows and
   // columns are all in X already).  Ping-pong maps of changed tile rows and
   // columns carry that from step to step.
-  const bool delta = use_tc2(n, n);
   const int trows = (n + kTc2BM - 1) / kTc2BM, tcols = (n + kTcBN - 1) / kTcBN;
   const size_t d_off = f_off + kAlign;
   const size_t dmap = align_up((size_t)trows + tcols, kAlign);
   void* p = nullptr;
   if ((rc = get_workspace(stream, d_off + (delta ? 2 * dmap : 0), &p))) return rc;
   uint8_t* ws = static_cast<uint8_t*>(p);
-  uint8_t* Xn = ws + x_off;
+  uint8_t* Xn = delta ? nullptr : ws + x_off;
   int* flag = reinterpret_cast<int*>(ws + f_off);
   uint8_t* cur = X;
   long long ldcur = ldx;
