@@ -2714,7 +2714,6 @@ int knn_fused_launch(const CUtensorMap& mqh, const CUtensorMap& mql, const CUten
                      int32_t* pi2, unsigned* ready2, int* flags, cudaStream_t stream) {
   if constexpr (KT >= 16) {
     if (kout > KT / 2) {
-      SIMD2_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)qblocks * sizeof(int), stream));
       int rc = knn_fused_pass<KT / 2, KT>(mqh, mql, mrh, mrl, a, qblocks, od, oi, ldo, kout, flags, stream);
       if (rc) return rc;
       KnnFusedArgs b = a;
@@ -2722,7 +2721,6 @@ int knn_fused_launch(const CUtensorMap& mqh, const CUtensorMap& mql, const CUten
       b.part_i = pi2;
       b.ready = ready2;
       b.gate = flags;
-      SIMD2_CUDA_TRY(cudaMemsetAsync(ready2, 0, (size_t)qblocks * a.chunks * 4, stream));
       return knn_fused_pass<KT, KT>(mqh, mql, mrh, mrl, b, qblocks, od, oi, ldo, kout, nullptr, stream);
     }
   }
@@ -2774,9 +2772,10 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   const size_t rhi = take((size_t)R * Dp * 2), rlo = take((size_t)R * Dp * 2);
   const size_t nq = take((size_t)Q * 4), nr = take((size_t)tiles * kKfBN * 4), tm = take((size_t)tiles * 4);
   const size_t pd = take((size_t)Q * 2 * chunks * KT * 4), pi = take((size_t)Q * 2 * chunks * KT * 4);
-  const size_t rf = take((size_t)qblocks * chunks * 4);
-  // the second pass's lists, ready flags, and the first pass's block flags
+  // the second pass's lists; then the ready flags of both passes and the
+  // first pass's block flags, side by side so that the prep kernel clears them
   const size_t pd2 = take((size_t)Q * 2 * chunks * KT * 4), pi2 = take((size_t)Q * 2 * chunks * KT * 4);
+  const size_t rf = take((size_t)qblocks * chunks * 4);
   const size_t rf2 = take((size_t)qblocks * chunks * 4), qf = take((size_t)qblocks * 4);
   void* p = nullptr;
   int rc = get_workspace(stream, off, &p);
@@ -2789,18 +2788,29 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   float* n_q = reinterpret_cast<float*>(ws + nq);
   float* n_r = reinterpret_cast<float*>(ws + nr);
   float* t_max = reinterpret_cast<float*>(ws + tm);
-  split_rows_bf16_kernel<<<grid_for((long long)Q * Dp / 8), 256, 0, stream>>>(query, ldq, Q, D, q_hi, q_lo, Dp);
-  split_rows_bf16_kernel<<<grid_for((long long)R * Dp / 8), 256, 0, stream>>>(ref, ldr, R, D, r_hi, r_lo, Dp);
-  row_norms_kernel<<<grid_for((long long)Q * 32), 256, 0, stream>>>(query, ldq, Q, D, n_q);
-  row_norms_kernel<<<grid_for((long long)R * 32), 256, 0, stream>>>(ref, ldr, R, D, n_r);
-  for (int i = 0; i < 4; i++) count_launch();
-  const int pad = tiles * kKfBN - R;
-  if (pad > 0) {
-    // references past R: +inf norm, so their distances never enter a list
-    fill_kernel<float><<<grid_for(pad), 256, 0, stream>>>(n_r + R, pad, 1, pad, __builtin_inff());
-    count_launch();
-  }
-  tile_max_kernel<<<grid_for((long long)tiles * 32), 256, 0, stream>>>(n_r, R, tiles, t_max);
+  // One launch: norms, BF16 splits, per-tile largest reference norm, +inf
+  // norms for the references past R (their distances never enter a list), and
+  // the cleared flags.
+  KnnPrepArgs pa{};
+  pa.q = query;
+  pa.ldq = ldq;
+  pa.Q = Q;
+  pa.r = ref;
+  pa.ldr = ldr;
+  pa.R = R;
+  pa.D = D;
+  pa.Dp = Dp;
+  pa.q_hi = q_hi;
+  pa.q_lo = q_lo;
+  pa.r_hi = r_hi;
+  pa.r_lo = r_lo;
+  pa.n_q = n_q;
+  pa.n_r = n_r;
+  pa.t_max = t_max;
+  pa.r_tiles = tiles;
+  pa.clear = reinterpret_cast<unsigned*>(ws + rf);
+  pa.clear_words = (long long)(qf + (size_t)qblocks * 4 - rf) / 4;
+  knn_prep_kernel<<<tiles + (Q + kKfBN - 1) / kKfBN, kKnnPrepThreads, 0, stream>>>(pa);
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   const auto BF = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
@@ -2832,7 +2842,6 @@ int knn_fused(const float* query, int Q, int ldq, const float* ref, int R, int l
   a.ready = reinterpret_cast<unsigned*>(ws + rf);
   a.kout = k;
   a.gate = nullptr;
-  SIMD2_CUDA_TRY(cudaMemsetAsync(a.ready, 0, (size_t)qblocks * chunks * 4, stream));
   float* p_d2 = reinterpret_cast<float*>(ws + pd2);
   int32_t* p_i2 = reinterpret_cast<int32_t*>(ws + pi2);
   unsigned* r2 = reinterpret_cast<unsigned*>(ws + rf2);

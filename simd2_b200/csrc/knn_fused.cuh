@@ -40,6 +40,7 @@
 #pragma once
 #include "common.cuh"
 #include "knn.cuh"
+#include "prep.cuh"
 #include "tc_gemm.cuh"
 
 namespace simd2 {
@@ -583,15 +584,109 @@ __global__ void __launch_bounds__(256) knn_merge_kernel(const float* __restrict_
   }
 }
 
-// Per 256-reference tile: the largest |r|^2 among its valid references.
-__global__ void tile_max_kernel(const float* __restrict__ nr, int R, int tiles, float* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tiles; t += (gridDim.x * blockDim.x) >> 5) {
-    float m = -__int_as_float(0x7f800000);
-    for (int c = t * kKfBN + lane; c < min(R, (t + 1) * kKfBN); c += 32) m = fmaxf(m, nr[c]);
+// Operand preparation of the fused k-NN in one launch.  Per row of the
+// queries and of the references: the squared norm in FP64 rounded to float
+// (lane l adds the squares of elements l, l+32, ... in that order, then a
+// butterfly over the warp: row_norms_kernel's order, so the same bits) and
+// the BF16 hi / lo split in split_rows_bf16_kernel's layout ([rows][Dp],
+// zeros past D).  Blocks [0, r_tiles) take one 256-reference tile each and
+// also write the tile's largest norm over its valid references, and +inf
+// norms for the padding references past R; the blocks after them take 256
+// queries each.  The grid also clears `clear_words` words at `clear` (the
+// passes' ready and block flags).  32 warps per block, 8 rows per warp: a
+// warp issues all its loads at once (lane l holds elements l, l+32, ... of
+// each row) and splits from the same registers.
+struct KnnPrepArgs {
+  const float* q;
+  long long ldq;
+  int Q;
+  const float* r;
+  long long ldr;
+  int R;
+  int D, Dp;  // D <= 32 * kKnnPrepMaxJ, Dp = D rounded up to 8
+  __nv_bfloat16 *q_hi, *q_lo, *r_hi, *r_lo;
+  float *n_q, *n_r, *t_max;
+  int r_tiles;
+  unsigned* clear;
+  long long clear_words;
+};
+
+constexpr int kKnnPrepMaxJ = kKfMaxPanels * 2;  // D <= 128: four elements per lane and row
+constexpr int kKnnPrepRows = 8;                 // rows per warp
+constexpr int kKnnPrepThreads = 1024;           // 32 warps x 8 rows = 256 rows per block
+static_assert(kKnnPrepThreads / 32 * kKnnPrepRows == kKfBN, "one reference tile per block");
+
+__global__ void __launch_bounds__(kKnnPrepThreads) knn_prep_kernel(KnnPrepArgs a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long long w = blockIdx.x * (long long)kKnnPrepThreads + threadIdx.x; w < a.clear_words;
+       w += (long long)gridDim.x * kKnnPrepThreads)
+    a.clear[w] = 0u;
+  const bool ref = blockIdx.x < a.r_tiles;
+  const float* A = ref ? a.r : a.q;
+  const long long lda = ref ? a.ldr : a.ldq;
+  const int M = ref ? a.R : a.Q;
+  const int rows = ref ? a.r_tiles * kKfBN : M;  // norms written for rows < rows
+  __nv_bfloat16* hi = ref ? a.r_hi : a.q_hi;
+  __nv_bfloat16* lo = ref ? a.r_lo : a.q_lo;
+  float* nrm = ref ? a.n_r : a.n_q;
+  const int row0 = (ref ? blockIdx.x : blockIdx.x - a.r_tiles) * kKfBN + warp * kKnnPrepRows;
+  const float inf = __int_as_float(0x7f800000);
+  float mx = -inf;  // the warp's largest norm over valid rows (reference tiles)
+  {
+    float v[kKnnPrepRows][kKnnPrepMaxJ];
+#pragma unroll
+    for (int u = 0; u < kKnnPrepRows; u++) {
+      const int i = row0 + u;
+#pragma unroll
+      for (int j = 0; j < kKnnPrepMaxJ; j++) {
+        const int k = lane + 32 * j;
+        v[u][j] = (i < M && k < a.D) ? __ldg(A + (long long)i * lda + k) : 0.f;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kKnnPrepRows; u++) {
+      const int i = row0 + u;
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < kKnnPrepMaxJ; j++) {
+        if (lane + 32 * j < a.D) {
+          const double x = v[u][j];
+          s += x * x;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      const float n = i < M ? (float)s : inf;
+      if (i < M) mx = fmaxf(mx, n);
+      if (lane == 0 && i < rows) nrm[i] = n;
+    }
+    // the BF16 split from the same registers: lane l writes elements l,
+    // l+32, ... of each row (zeros for D <= k < Dp)
+#pragma unroll
+    for (int u = 0; u < kKnnPrepRows; u++) {
+      const int i = row0 + u;
+      if (i >= M) continue;
+#pragma unroll
+      for (int j = 0; j < kKnnPrepMaxJ; j++) {
+        const int k = lane + 32 * j;
+        if (k < a.Dp) {
+          __nv_bfloat16 h, l;
+          split_bf16(v[u][j], h, l);
+          hi[(long long)i * a.Dp + k] = h;
+          lo[(long long)i * a.Dp + k] = l;
+        }
+      }
+    }
+  }
+  if (!ref) return;  // uniform across the block
+  __shared__ float wmax[kKnnPrepThreads / 32];
+  if (lane == 0) wmax[warp] = mx;
+  __syncthreads();
+  if (warp == 0) {
+    float m = wmax[lane];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) out[t] = m;
+    if (lane == 0) a.t_max[blockIdx.x] = m;
   }
 }
 

@@ -103,6 +103,28 @@ def test_knn_fused_ties_and_fewer_refs_than_k(cuda):
     assert torch.equal(i, i2) and torch.equal(d.view(torch.int32), d2.view(torch.int32))
 
 
+@pytest.mark.parametrize("D,pad,shift", [(128, 3, 1), (37, 5, 2), (64, 0, 0), (120, 4, 4)])
+def test_knn_fused_strided_and_unaligned_rows(cuda, D, pad, shift):
+    """Rows with a pitch past D and a base off the 16-byte boundary (the
+    operand prep then loads element by element): both modes agree bit for
+    bit, and with the oracle; R = 1000 leaves a ragged last reference tile."""
+    Q, R, k = 300, 1000, 16
+    q, r = datagen.point_cloud(Q, R, D, seed=D * 11 + pad, dup_frac=0.05)
+    qb = torch.zeros((Q, D + pad + shift), dtype=torch.float32, device=cuda)
+    rb = torch.zeros((R, D + pad + shift), dtype=torch.float32, device=cuda)
+    qb[:, shift:shift + D] = torch.from_numpy(q).to(cuda)
+    rb[:, shift:shift + D] = torch.from_numpy(r).to(cuda)
+    Qt, Rt = qb[:, shift:shift + D], rb[:, shift:shift + D]
+    d1, i1 = s2.knn(Qt, Rt, k, mode="fused")
+    d2, i2 = s2.knn(Qt, Rt, k, mode="materialised")
+    assert torch.equal(i1, i2)
+    assert torch.equal(d1.view(torch.int32), d2.view(torch.int32))
+    check(q, r, k, d1.cpu().numpy(), i1.cpu().numpy())
+    d3, i3 = s2.knn(torch.from_numpy(q).to(cuda), torch.from_numpy(r).to(cuda), k, mode="fused")
+    assert torch.equal(i1, i3) and torch.equal(d1.view(torch.int32), d3.view(torch.int32))
+    assert s2.device_status() == 0
+
+
 def test_knn_fused_rejects_wide_points(cuda):
     q = torch.zeros(4, 200, device=cuda)
     with pytest.raises(s2.Simd2Error):
