@@ -62,7 +62,7 @@ def parse_args():
                         "(one size class)")
     p.add_argument("--knn-q", type=int, default=16384)
     p.add_argument("--knn-r", type=int, default=65536)
-    p.add_argument("--workload", choices=("sweep", "batched", "knn", "rowpanel"), default="sweep",
+    p.add_argument("--workload", choices=("sweep", "batched", "knn", "rowpanel", "orand"), default="sweep",
                    help="sweep: the nine-semiring srgemm line (default); batched: only the batched closure "
                         "(used for profiling runs); knn: the k-NN modes; rowpanel: one or_and closure with "
                         "X's rows split across the ranks")
@@ -740,6 +740,41 @@ def main():
                          "distance_kernel_ms": kt.by_kind.get("tensor", (0, 0, 0))[0] / args.steps}
         if rank == 0:
             print(json.dumps(out), flush=True)
+        return 0
+
+    if args.workload == "orand":
+        # one or_and reachability closure per rank (independent replicas), the
+        # configuration-4 graph: CSR steps while X is sparse, then INT8 delta steps
+        n = args.rowpanel_n
+        rng = np.random.default_rng(44)
+        m = 2 * n
+        base = torch.zeros((n, n), dtype=torch.uint8, device=dev)
+        base[torch.from_numpy(rng.integers(0, n, m)).to(dev), torch.from_numpy(rng.integers(0, n, m)).to(dev)] = 1
+        base.fill_diagonal_(1)
+        X = base.clone()
+        s2.closure("or_and", X)  # warm-up
+        times, its = [], 0
+        for _ in range(max(args.steps, 1)):
+            X.copy_(base)
+            barrier()
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            its = s2.closure("or_and", X)
+            ev1.record()
+            torch.cuda.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+        ms = sorted(times)[len(times) // 2]
+        if world > 1:
+            from simd2_b200.shard import max_over_ranks
+            ms = max_over_ranks(ms, device=dev)
+        if rank == 0:
+            print(json.dumps({"workload": f"or_and closure n={n} (edge probability 2/n, seed 44)", "ms": ms,
+                              "iters": its, "gops_dense_equivalent": 2.0 * n ** 3 * its / ms / 1e6, "n_gpus": world,
+                              "how": "simd2_closure_orand_u8 on every rank; CUDA events, median of steps, max over "
+                                     "ranks"}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
         return 0
 
     if args.workload == "rowpanel":

@@ -716,8 +716,12 @@ int srgemm_tc_orand(int M, int N, int K, const T* A, long long lda, const T* B, 
   uint8_t* b8 = ws + plan.b0;
   bool_rows_u8_kernel<T><<<grid_for((long long)M * Kp / 16), 256, 0, stream>>>(A, lda, M, K, a8, Kp);
   count_launch();
-  dim3 tgrid((N + 31) / 32, (Kp + 31) / 32), tblock(32, 8);
-  transpose_prep_kernel<T, 1><<<tgrid, tblock, 0, stream>>>(B, ldb, K, N, b8, nullptr, Kp);
+  if constexpr (std::is_same_v<T, uint8_t>) {
+    transpose_bool_u8_kernel<<<dim3((N + 63) / 64, (Kp + 63) / 64), 256, 0, stream>>>(B, ldb, K, N, b8, Kp);
+  } else {
+    dim3 tgrid((N + 31) / 32, (Kp + 31) / 32), tblock(32, 8);
+    transpose_prep_kernel<T, 1><<<tgrid, tblock, 0, stream>>>(B, ldb, K, N, b8, nullptr, Kp);
+  }
   count_launch();
   SIMD2_CUDA_TRY(cudaGetLastError());
   CUtensorMap ma, mb;

@@ -385,6 +385,57 @@ __global__ void transpose_prep_kernel(const T* __restrict__ B, long long ldb, in
   }
 }
 
+// Per byte of x: 1 where the byte is nonzero, else 0 (no carry crosses a byte:
+// (b & 0x7f) + 0x7f <= 0xfe, and its top bit is set iff b & 0x7f != 0).
+__device__ __forceinline__ uint32_t bytes_nonzero_01(uint32_t x) {
+  return ((((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x) & 0x80808080u) >> 7;
+}
+
+// or_and's B operand for bytes: B [K][N] (pitch ldb) -> out [N][Kp], 1 where
+// B is nonzero, zeros for K <= k < Kp (transpose_prep_kernel<T, 1>'s result).
+// One 64 x 64 tile per block of 256 threads: a thread reads 16 bytes of a row
+// of B (one 16-byte load where B allows) and writes 16 bytes of a row of out;
+// the shared tile's 68-byte rows keep both phases at most 2-way bank
+// conflicted.  Kp is a multiple of 16, out 16-byte aligned; the grid covers
+// ceil(N / 64) x ceil(Kp / 64) tiles.
+__global__ void __launch_bounds__(256) transpose_bool_u8_kernel(const uint8_t* __restrict__ B, long long ldb, int K,
+                                                                int N, uint8_t* __restrict__ out, int Kp) {
+  __shared__ uint32_t tile[64][17];
+  const int t = threadIdx.x;
+  const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+  {
+    const int r = t >> 2, c0 = (t & 3) * 16;
+    const int k = k0 + r, j = j0 + c0;
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    if (k < K && j < N) {
+      const uint8_t* src = B + (long long)k * ldb + j;
+      if (j + 16 <= N && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
+        w[0] = v.x, w[1] = v.y, w[2] = v.z, w[3] = v.w;
+      } else {
+        for (int e = 0; e < 16 && j + e < N; e++) w[e >> 2] |= (uint32_t)src[e] << (8 * (e & 3));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) tile[r][(c0 >> 2) + q] = bytes_nonzero_01(w[q]);
+  }
+  __syncthreads();
+  const int jj = t >> 2, kc = (t & 3) * 16;
+  const int jo = j0 + jj, ko = k0 + kc;
+  if (jo < N && ko < Kp) {
+    const int sh = 8 * (jj & 3);
+    uint32_t o[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      uint32_t x = 0u;
+#pragma unroll
+      for (int b = 0; b < 4; b++) x |= ((tile[kc + 4 * q + b][jj >> 2] >> sh) & 0xffu) << (8 * b);
+      o[q] = x;
+    }
+    *reinterpret_cast<uint4*>(out + (long long)jo * Kp + ko) = make_uint4(o[0], o[1], o[2], o[3]);
+  }
+}
+
 // Squared row norms of A [M][K], accumulated in FP64, rounded to float.
 __global__ void row_norms_kernel(const float* __restrict__ A, long long lda, int M, int K, float* __restrict__ out) {
   const int warps = blockDim.x / 32;

@@ -104,6 +104,27 @@ def test_or_and(cuda, dtype):
             np.testing.assert_array_equal(got.astype(np.int32), want)
 
 
+@pytest.mark.parametrize("m,n,k,pad,shift", [(70, 300, 200, 20, 0), (33, 130, 100, 5, 1), (129, 64, 17, 0, 0),
+                                             (16, 1000, 77, 3, 7)])
+def test_or_and_bytes_any_nonzero_strided(cuda, m, n, k, pad, shift):
+    """Byte operands whose true entries include bytes with the top bit set
+    (0x80, 0xff), B with a pitch past n and a base off the 16-byte boundary
+    (B^T is formed 16 bytes at a time where B allows, byte by byte elsewhere),
+    ragged k and n: D = A (x) B (+) C against the oracle."""
+    rng = np.random.default_rng(m * 7 + n + k)
+    vals = np.array([1, 2, 127, 128, 255], np.uint8)
+    a = np.where(rng.random((m, k)) < 0.1, rng.choice(vals, (m, k)), 0).astype(np.uint8)
+    b = np.where(rng.random((k, n)) < 0.1, rng.choice(vals, (k, n)), 0).astype(np.uint8)
+    c = (rng.random((m, n)) < 0.05).astype(np.uint8)
+    Bbuf = torch.zeros((k, n + pad + shift), dtype=torch.uint8, device=cuda)
+    Bbuf[:, shift:shift + n] = torch.from_numpy(b).to(cuda)
+    A, B, C = torch.from_numpy(a).to(cuda), Bbuf[:, shift:shift + n], torch.from_numpy(c).to(cuda)
+    for epi in (False, True):
+        got = s2.srgemm("or_and", A, B, C, do_epilogue=epi).cpu().numpy()
+        want = oracle.srgemm("or_and", a.astype(np.int32), b.astype(np.int32), c.astype(np.int32), do_epilogue=epi)
+        np.testing.assert_array_equal(got.astype(np.int32), want)
+
+
 def test_k_zero_and_empty(cuda):
     for op in MINMAX + SUMS:
         a, b, c = datagen.semiring_operands(op, 9, 11, 0, seed=1)
