@@ -189,4 +189,10 @@ struct Semiring<SIMD2_MIN_MAX> : MinAdd {
   __device__ static float mul(float a, float b) { return max2f(a, b); }
 };
 
+// Per byte of x: 1 where the byte is nonzero, else 0 (no carry crosses a byte:
+// (b & 0x7f) + 0x7f <= 0xfe, and its top bit is set iff b & 0x7f != 0).
+__device__ __forceinline__ uint32_t bytes_nonzero_01(uint32_t x) {
+  return ((((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x) & 0x80808080u) >> 7;
+}
+
 }  // namespace simd2

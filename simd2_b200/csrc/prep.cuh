@@ -320,7 +320,7 @@ __global__ void bool_rows_u8_kernel(const T* __restrict__ A, long long lda, int 
       for (int q = 0; q < 4; q++) {
         // 0x01 in every byte that is nonzero, carry-free
         const uint32_t b = in[q];
-        w[q] = (((b & 0x7f7f7f7fu) + 0x7f7f7f7fu | b) & 0x80808080u) >> 7;
+        w[q] = bytes_nonzero_01(b);
       }
     } else {
 #pragma unroll
@@ -383,12 +383,6 @@ __global__ void transpose_prep_kernel(const T* __restrict__ B, long long ldb, in
       }
     }
   }
-}
-
-// Per byte of x: 1 where the byte is nonzero, else 0 (no carry crosses a byte:
-// (b & 0x7f) + 0x7f <= 0xfe, and its top bit is set iff b & 0x7f != 0).
-__device__ __forceinline__ uint32_t bytes_nonzero_01(uint32_t x) {
-  return ((((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x) & 0x80808080u) >> 7;
 }
 
 // or_and's B operand for bytes: B [K][N] (pitch ldb) -> out [N][Kp], 1 where

@@ -552,46 +552,65 @@ __global__ void dense_row_count_kernel(int rows, int cols, const float* __restri
   }
 }
 
-// Nonzero bytes of each row of a byte matrix; one warp per row, 4 bytes per
-// lane.  *non01 |= 1 when a byte is neither 0 nor 1.
+// Per row of a byte matrix: the nonzero entries (counts[r]); *non01 = 1 when
+// a byte other than 0 / 1 occurs.  One warp per row, 16 bytes per lane (one
+// 16-byte load where the pitch and base allow, else byte loads).
 __global__ void dense_row_count_u8_kernel(int rows, int cols, const uint8_t* __restrict__ X, long long ld,
                                           int* __restrict__ counts, int* __restrict__ non01) {
   const int lane = threadIdx.x & 31;
-  int bad = 0;
+  const bool vec = (ld % 16 == 0) && (reinterpret_cast<uintptr_t>(X) % 16 == 0);
+  uint32_t bad = 0;
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
     const uint8_t* xr = X + (long long)r * ld;
     int c = 0;
-    for (int j = 4 * lane; j < cols; j += 128)
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int v = j + e < cols ? xr[j + e] : 0;
-        c += v != 0;
-        bad |= v > 1;
+    for (int j = 16 * lane; j < cols; j += 512) {
+      uint32_t w[4] = {0u, 0u, 0u, 0u};
+      if (vec && j + 16 <= cols) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(xr + j));
+        w[0] = v.x, w[1] = v.y, w[2] = v.z, w[3] = v.w;
+      } else {
+        for (int e = 0; e < 16 && j + e < cols; e++) w[e >> 2] |= (uint32_t)xr[j + e] << (8 * (e & 3));
       }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        c += __popc(bytes_nonzero_01(w[q]));
+        bad |= w[q] & 0xfefefefeu;
+      }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     if (lane == 0) counts[r] = c;
   }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(non01, 1);
+  if (__any_sync(0xffffffffu, bad != 0) && lane == 0) atomicOr(non01, 1);
 }
 
 // CSR (values 1.0f) <- the nonzero bytes of a 0/1 byte matrix at the offsets
-// rp, increasing column; one warp per row, 4 bytes per lane.
+// rp, increasing column; one warp per row, 16 bytes per lane (as above).
 __global__ void dense_to_csr_u8_kernel(int rows, int cols, const uint8_t* __restrict__ X, long long ld,
                                        const int* __restrict__ rp, int* __restrict__ cj, float* __restrict__ cv) {
   const int lane = threadIdx.x & 31;
+  const bool vec = (ld % 16 == 0) && (reinterpret_cast<uintptr_t>(X) % 16 == 0);
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
     const uint8_t* xr = X + (long long)r * ld;
     int pos = rp[r];
-    for (int j0 = 0; j0 < cols; j0 += 128) {
-      const int j = j0 + 4 * lane;
-      bool f[4];
+    for (int j0 = 0; j0 < cols; j0 += 512) {
+      const int j = j0 + 16 * lane;
+      uint32_t w[4] = {0u, 0u, 0u, 0u};
+      if (j < cols) {
+        if (vec && j + 16 <= cols) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4*>(xr + j));
+          w[0] = v.x, w[1] = v.y, w[2] = v.z, w[3] = v.w;
+        } else {
+          for (int e = 0; e < 16 && j + e < cols; e++) w[e >> 2] |= (uint32_t)xr[j + e] << (8 * (e & 3));
+        }
+      }
       int c = 0;
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        f[e] = j + e < cols && xr[j + e] != 0;
-        c += f[e];
+      for (int q = 0; q < 4; q++) {
+        w[q] = bytes_nonzero_01(w[q]);
+        c += __popc(w[q]);
       }
+      if (__ballot_sync(0xffffffffu, c != 0) == 0u) continue;  // uniform: no entry in these 512 columns
       int incl = c;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -600,8 +619,8 @@ __global__ void dense_to_csr_u8_kernel(int rows, int cols, const uint8_t* __rest
       }
       int at = pos + incl - c;
 #pragma unroll
-      for (int e = 0; e < 4; e++)
-        if (f[e]) {
+      for (int e = 0; e < 16; e++)
+        if ((w[e >> 2] >> (8 * (e & 3))) & 1u) {
           cj[at] = j + e;
           cv[at] = 1.0f;
           at++;

@@ -242,10 +242,7 @@ __device__ __forceinline__ void tc_tile_epilogue(const TcEpilogue& ep, int M, in
             const uint32_t cw[8] = {c0v.x, c0v.y, c0v.z, c0v.w, c1v.x, c1v.y, c1v.z, c1v.w};
 #pragma unroll
             for (int q = 0; q < 8; q++) {
-              // normalise C's bytes to 0/1 before the OR
-              uint32_t cb = cw[q];
-              cb = ((cb & 0x7f7f7f7fu) + 0x7f7f7f7fu | cb) & 0x80808080u;
-              cb >>= 7;
+              const uint32_t cb = bytes_nonzero_01(cw[q]);  // C's bytes as 0/1 before the OR
               const uint32_t v = w[q] | cb;
               if (ep.changed && v != cb) changed = 1;
               w[q] = v;

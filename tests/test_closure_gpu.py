@@ -122,13 +122,14 @@ def _orand_dense_closure(X, max_iter=64):
     return X, it
 
 
-@pytest.mark.parametrize("case", ["er_deg2", "cycles", "non01"])
+@pytest.mark.parametrize("case", ["er_deg2", "cycles", "non01", "non01_255", "pitched"])
 def test_or_and_closure_sparse_opening(cuda, case):
     """From n = 8192 the or_and closure squares a sparse X as CSR SpGEMM
     steps before the INT8 tensor-core steps: same bits and step count as the
     dense loop ('cycles' converges while still sparse; 'non01' holds bytes
     other than 0 / 1, which the dense step rewrites, so the opening stands
-    aside)."""
+    aside; 'pitched' closes X in place inside a wider, unaligned buffer, where
+    the conversion to CSR reads bytes one at a time)."""
     n = 8192
     rng = np.random.default_rng(8192)
     X = torch.zeros((n, n), dtype=torch.uint8, device=cuda)
@@ -141,7 +142,13 @@ def test_or_and_closure_sparse_opening(cuda, case):
     X.fill_diagonal_(1)
     if case == "non01":
         X[5, 7] = 2
+    if case == "non01_255":
+        X[8000, 3] = 255
     want, it_want = _orand_dense_closure(X.clone())
+    if case == "pitched":
+        buf = torch.zeros((n, n + 5), dtype=torch.uint8, device=cuda)
+        buf[:, 1:n + 1] = X
+        X = buf[:, 1:n + 1]
     it = s2.closure("or_and", X)
     assert it == it_want
     assert torch.equal(X, want)
